@@ -1,0 +1,423 @@
+#!/usr/bin/env python3
+"""Throughput of the LCODE 3D xi step on B200: xi-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|mixed] [--grid 641]
+
+Workload (default): the production grid of the reference's example config,
+641 x 641 cells, h = 0.025 (window +-8), plasma coarseness 3 / fineness 2
+(42,025 coarse and 1,537,600 fine particles), xi_step = 0.005, cold uniform
+plasma, axisymmetric beam rho_b = A exp(-r^2/2) 0.5 (1 - cos(sqrt(pi/2) xi))
+with A = 0.5 (blowout regime). Synthetic inputs: the plasma and beam are
+generated, there is no dataset. The state is first advanced (untimed) into
+the beam so the timed steps see the nonlinear wake.
+
+One "step" is one full xi step (estimate, predictor, corrector, final move +
+deposit: 3 pushes, 3 depositions, 2 field solves of 6 fields).
+
+value: device-resident inputs (beam arrays already in HBM), context-owned
+state, each step timed with CUDA events on the launching stream; L2 is
+flushed (a 256 MiB write) between timed steps, outside the timed events.
+e2e: the same metric through the public drop-in API (lcode3d_b200.step) with
+the beam copied host->device from pinned memory and Ez(0,0) read back
+device->host every step, like the reference's CLI loop.
+
+--impl reference: the reference algorithm on the host cores (the oracle
+restatement in oracle/: numpy + scipy.fft, its particle kernels in C with
+OpenMP), a bounded number of steps of the same workload.
+
+Multi-GPU (torchrun, one process per GPU): a single simulation does not
+shard (each step has global spectral solves), so every rank runs an
+independent replica; value = all ranks' steps / max-over-ranks time.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'xi-steps/s'
+GRIDS = {
+    # N: (h, dxi, amplitude)
+    641: (0.025, 0.005, 0.5),
+    161: (0.05, 0.05, 0.05),
+}
+
+
+def make_config(N, precision):
+    import types
+    h, dxi, A = GRIDS[N]
+    c = types.SimpleNamespace(
+        grid_steps=N, grid_step_size=h, xi_step_size=dxi, xi_steps=3000,
+        diagnostics_each_N_steps=10 ** 9, field_solver_subtraction_trick=1,
+        field_solver_variant_A=True, reflect_padding_steps=5, plasma_padding_steps=10,
+        plasma_coarseness=3, plasma_fineness=2, gpu_index=0, lc3d_precision=precision)
+
+    def beam(xi_i, x, y):
+        xi = xi_i * dxi
+        if xi < 0 or xi > 2 * np.sqrt(2 * np.pi):
+            return 0
+        return A * np.exp(-(x ** 2 + y ** 2) / 2) * 0.5 * (1 - np.cos(np.sqrt(np.pi / 2) * xi))
+    c.beam = beam
+    return c
+
+
+def beam_np(cfg, xi_i, xs, ys):
+    N = cfg.grid_steps
+    return np.broadcast_to(np.asarray(cfg.beam(xi_i, xs, ys), dtype=np.float64), (N, N)).copy()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class Clocks:
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.Q}',
+                 '--format=csv,noheader,nounits', '-lms', '100'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith('active'):
+                    reasons.add(n)
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': mx,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def peaks():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get('hbm_gbs', 6650.0), 'measured (MEASURED_PEAKS.json)'
+    return 6650.0, 'fallback (6.65 TB/s)'
+
+
+def fp64_peak_tflops(torch):
+    """FP64 denominator measured in this run: cuBLAS DGEMM 8192^3 (best of
+    5), since the measured-peaks file holds no float64 figure."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device='cuda')
+    b = torch.randn(n, n, dtype=torch.float64, device='cuda')
+    torch.matmul(a, b)
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def transform_flops_per_launch(N):
+    """Algorithmic flops of one batched transform-GEMM launch: the 4 launches
+    of a solve apply L and R to each of the 6 fields (r x c with r, c in
+    {N, N-2}); each field costs 4 r c (r + c) flops over the 4 launches."""
+    M = N - 2
+    dims = [(N, M), (M, N), (M, M), (M, N), (N, M), (N, N)]
+    return sum(4 * r * c * (r + c) for r, c in dims) / 4
+
+
+def deposit_bytes_per_launch(N, Nc, Nf):
+    """Algorithmic bytes of one deposition (kernel + finalize): read the 7
+    coarse arrays and the 5 fine-lattice arrays, read ro_initial, write
+    ro, jx, jy, jz."""
+    return 8 * (7 * Nc * Nc + 5 * Nf + N * N + 4 * N * N)
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    import lcode3d_b200 as L
+    from lcode3d_b200 import _lib
+
+    dev = int(os.environ.get('LOCAL_RANK', 0))
+    torch.cuda.set_device(dev)
+    cfg = make_config(args.grid, args.precision)
+    N = cfg.grid_steps
+    xs, ys, const, virt, st = L.init(cfg)
+    s = L.solver_for(cfg)
+    s.set_virt(virt)
+    s.set_const(const)
+    L.lcode.check_errors = False
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    # advance (untimed) into the beam with the public API
+    t_pre = time.time()
+    for i in range(args.pre):
+        st = L.step(cfg, const, virt, st, beam_np(cfg, i, xs, ys))
+    torch.cuda.synchronize()
+    t_pre = time.time() - t_pre
+    x0 = args.pre
+    lib = _lib.lib
+    names = _lib.STATE_NAMES
+    ptrs = _lib.StatePtrs(*[getattr(st, n).data_ptr() for n in names])
+    _lib.check(lib.lc3d_set_state(s.ctx, ctypes.byref(ptrs), sp), 'set_state')
+    K, W = args.steps, args.warmup
+    beams = [torch.from_numpy(beam_np(cfg, x0 + i, xs, ys)).cuda() for i in range(W + K)]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
+    for i in range(W):
+        _lib.check(lib.lc3d_step(s.ctx, ctypes.c_void_p(beams[i].data_ptr()), sp), 'step')
+    torch.cuda.synchronize()
+    _lib.check(lib.lc3d_check_error(s.ctx, sp), 'warmup')
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    _lib.check(lib.lc3d_profile(s.ctx, 1), 'profile')
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(dev)
+    clocks.start()
+    for i in range(K):
+        flush.fill_(float(i))
+        ev[i][0].record(stream)
+        _lib.check(lib.lc3d_step(s.ctx, ctypes.c_void_p(beams[W + i].data_ptr()), sp), 'step')
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms_steps = [a.elapsed_time(b) for a, b in ev]
+    nst = len(_lib.STAGES)
+    launches = (ctypes.c_longlong * nst)()
+    kms = (ctypes.c_double * nst)()
+    timed = (ctypes.c_longlong * nst)()
+    rc = lib.lc3d_profile_read(s.ctx, launches, kms, timed)
+    lib.lc3d_profile(s.ctx, 0)
+    _lib.check(lib.lc3d_check_error(s.ctx, sp), 'timed steps')
+    total_ms = sum(ms_steps)
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t)
+    value = world * K / (total_ms * 1e-3)
+    stage = {n: {'launches': int(launches[k]), 'ms': kms[k], 'timed': int(timed[k])}
+             for k, n in enumerate(_lib.STAGES)}
+
+    # ---- e2e through the public API, host beam in pinned memory ----
+    st_e = st
+    pinned = [torch.from_numpy(beam_np(cfg, x0 + i, xs, ys)).pin_memory() for i in range(W + K)]
+    L.lcode.check_errors = False
+    for i in range(W):
+        st_e = L.step(cfg, const, virt, st_e, pinned[i])
+        float(st_e.Ez[N // 2, N // 2])
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for i in range(K):
+        st_e = L.step(cfg, const, virt, st_e, pinned[W + i])
+        float(st_e.Ez[N // 2, N // 2])   # D2H of the step's result
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t)
+    L.lcode.check_errors = True
+    s.check_device_flag('e2e')
+
+    if rank != 0:
+        return None
+    # ---- roofline of the dominant kernel ----
+    dom = max(stage, key=lambda n: stage[n]['ms'])
+    hbm, hbm_src = peaks()
+    roof = None
+    if dom == 'transform' and stage[dom]['timed']:
+        avg_ms = stage[dom]['ms'] / stage[dom]['timed']
+        fl = transform_flops_per_launch(N)
+        ach = fl / (avg_ms * 1e-3) / 1e12
+        pk = fp64_peak_tflops(torch)
+        roof = {'kernel': 'dgemm_kernel (FP64 DST/DCT transforms)', 'bound': 'fp64',
+                'achieved': ach, 'peak': pk, 'unit': 'TFLOP/s', 'frac': ach / pk,
+                'peak_source': 'measured in this run: cuBLAS DGEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)',
+                'algorithmic_per_launch': fl, 'avg_launch_ms': avg_ms, 'traffic': None}
+    else:
+        avg_ms = stage[dom]['ms'] / max(1, stage[dom]['timed'])
+        by = deposit_bytes_per_launch(N, s.Nc, s.Nf)
+        ach = by / (avg_ms * 1e-3) / 1e9
+        roof = {'kernel': dom, 'bound': 'hbm', 'achieved': ach, 'peak': hbm, 'unit': 'GB/s',
+                'frac': ach / hbm, 'peak_source': hbm_src, 'algorithmic_per_launch': by,
+                'avg_launch_ms': avg_ms, 'traffic': None}
+    tr = os.path.join(ROOT, 'profiles', 'traffic.json')
+    if os.path.exists(tr):
+        with open(tr) as f:
+            t = json.load(f).get(f'{args.grid}_{args.precision}', {})
+        if roof['kernel'].split(' ')[0] in t:
+            roof['traffic'] = t[roof['kernel'].split(' ')[0]]
+    out = {
+        'metric': METRIC, 'value': value, 'unit': 'xi-steps/s', 'n_gpus': world,
+        'steps': K, 'warmup': W, 'ms_per_step': total_ms / K, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64' if args.precision == 'fp64' else 'f64+bf16',
+        'data': 'synthetic (generated cold uniform plasma + axisymmetric beam; no dataset)',
+        'config': {'workload': f'LCODE 3D xi step, {N}x{N} grid, h={cfg.grid_step_size}, '
+                               f'xi_step={cfg.xi_step_size}, coarseness 3 / fineness 2, A={GRIDS[N][2]}, '
+                               f'{args.precision} field solvers',
+                   'grid_steps': N, 'coarse_particles': s.Nc ** 2, 'fine_particles': s.Nf ** 2,
+                   'precision': args.precision, 'start_xi_step': x0,
+                   'l2': 'flushed between timed steps (256 MiB write, outside the step events)',
+                   'parallelism': f'replicas x{world}' if world > 1 else 'single GPU'},
+        'e2e': {'value': world * K / (e2e_ms * 1e-3), 'unit': 'xi-steps/s',
+                'h2d_bytes_per_step': N * N * 8, 'd2h_bytes_per_step': 8,
+                'wall_ms': wall_ms, 'api': 'lcode3d_b200.step (drop-in for lcode.step)'},
+        'gpu_launches': int(sum(launches)),
+        'launches_per_step': sum(launches) / K,
+        'stages_ms_per_step': {n: stage[n]['ms'] / K for n in stage},
+        'roofline': roof,
+        'clocks': clk,
+        'pre_steps_seconds': t_pre,
+    }
+    return out
+
+
+# ---------------------------------------------------------------------------
+# CPU: the oracle (reference algorithm) on the host cores
+# ---------------------------------------------------------------------------
+
+def time_oracle(grid, steps, threads, start):
+    from oracle import lcode_oracle as O
+    O.use_c_kernels(threads)
+    O.FFT_WORKERS = threads
+    cfg = make_config(grid, 'fp64')
+    xs, ys, const, virt, st = O.init(cfg)
+    t0 = time.perf_counter()
+    for i in range(steps):
+        st = O.step(cfg, const, virt, st, beam_np(cfg, start + i, xs, ys))
+    return steps / (time.perf_counter() - t0)
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    threads = cpu_threads()
+    K = max(1, min(args.steps, args.ref_max_steps))
+    W = min(args.warmup, 1)
+    from oracle import lcode_oracle as O
+    if W:
+        time_oracle(args.grid, W, threads, 0)
+    v = time_oracle(args.grid, K, threads, 0)
+    cfg = make_config(args.grid, 'fp64')
+    N = cfg.grid_steps
+    return {
+        'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': 'xi-steps/s', 'n_gpus': 0,
+        'steps': K, 'warmup': W, 'ms_per_step': 1e3 / v, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+        'data': 'synthetic (generated cold uniform plasma + axisymmetric beam; no dataset)',
+        'config': {'workload': f'LCODE 3D xi step, {N}x{N} grid, h={cfg.grid_step_size}, '
+                               f'xi_step={cfg.xi_step_size}, coarseness 3 / fineness 2, A={GRIDS[N][2]}, '
+                               'fp64 field solvers', 'grid_steps': N},
+        'cpu_baseline': {'value': v, 'unit': 'xi-steps/s', 'cores': threads, 'kind': 'port',
+                         'sample': f'{K} xi steps of the {N}^2 workload from its initial state '
+                                   '(reference algorithm: numpy + scipy.fft, particle kernels in C/OpenMP)'},
+        'e2e': {'value': v, 'unit': 'xi-steps/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=100)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--precision', default='fp64', choices=['fp64', 'mixed'])
+    ap.add_argument('--grid', type=int, default=641, choices=sorted(GRIDS))
+    ap.add_argument('--pre', type=int, default=400, help='untimed steps into the beam')
+    ap.add_argument('--cpu-steps', type=int, default=16, help='oracle steps for cpu_baseline')
+    ap.add_argument('--ref-max-steps', type=int, default=40)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == 'ours':
+        args.warmup = 3
+
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    if args.impl == 'reference':
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+    out = run_ours(args, rank, world, dist)
+    if rank == 0:
+        threads = 1
+        v = time_oracle(args.grid, args.cpu_steps, threads, 0)
+        out['cpu_baseline'] = {
+            'value': v, 'unit': 'xi-steps/s', 'cores': threads, 'kind': 'port',
+            'sample': f'{args.cpu_steps} xi steps of the {args.grid}^2 workload from its initial state, '
+                      'oracle restatement of the reference (numpy + scipy.fft, particle kernels in C), 1 thread'}
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

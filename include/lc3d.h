@@ -1,0 +1,195 @@
+/*
+ * lc3d.h -- C ABI of the B200-native LCODE 3D xi-step solver (liblc3d.so).
+ *
+ * The reference (lotov/lcode3d) is one Python module, lcode.py; its public
+ * boundary is the module contract that its CLI loop (lcode.py:1032-1051) and
+ * embedding code use:
+ *     init(config)                                   lcode.py:936-975
+ *     step(config, const, virt_params, prev, beam_ro) lcode.py:828-931
+ * plus the per-stage functions that step() calls. Each entry point below
+ * replaces one of those functions (cited beside it); the Python package
+ * lcode3d_b200 binds them with ctypes and keeps the reference's names,
+ * argument meaning and attribute names on top.
+ *
+ * Conventions
+ *  - All array pointers are DEVICE pointers to float64 (int32 where noted),
+ *    C-contiguous, row-major with x as axis 0 (lcode.py:197, 951-953):
+ *    grids are N x N (N = grid_steps), coarse particle arrays Nc x Nc,
+ *    fine-lattice arrays have length Nf.
+ *  - Every call is stream-ordered on `stream` (a cudaStream_t; NULL = the
+ *    legacy default stream) and performs no implicit host synchronisation,
+ *    except lc3d_check_error / lc3d_ez_history which read device memory.
+ *  - A context owns all its device workspaces and its own copies of the
+ *    constant arrays (const, virt_params). One context per host thread.
+ *  - Return value: LC3D_OK (0) or one of the error codes below; the text of
+ *    a code is lc3d_strerror(code). A particle whose 3x3 stencil would leave
+ *    the grid is never written out of bounds: it is skipped, and the device
+ *    error flag is raised (read it with lc3d_check_error), where the
+ *    reference would corrupt memory (docs/overview/window_and_grids.rst:60).
+ */
+#ifndef LC3D_H
+#define LC3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LC3D_OK 0
+#define LC3D_ERR_PARAM 1        /* invalid parameter / config (the reference asserts) */
+#define LC3D_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define LC3D_ERR_WINDOW 3       /* device flag: a particle stencil left the grid */
+#define LC3D_ERR_NONFINITE 4    /* device flag: non-finite or out-of-range deposit */
+#define LC3D_ERR_STATE 5        /* call order: state / const not set */
+#define LC3D_ERR_SIZE 6         /* size beyond a documented maximum */
+
+/* Precision of the field solvers. */
+#define LC3D_PREC_FP64 0        /* float64 dense-transform (DGEMM-form) solvers */
+#define LC3D_PREC_MIXED 1       /* split-BF16 tcgen05 transforms, fp32 accumulate */
+
+/* Mirrors the reference config module attributes (config_example.py:1-30). */
+typedef struct lc3d_params {
+    int grid_steps;                       /* odd (lcode.py:941) */
+    double grid_step_size;
+    double xi_step_size;
+    int plasma_coarseness;
+    int plasma_fineness;
+    int reflect_padding_steps;            /* > plasma_coarseness + 1 (lcode.py:944) */
+    int plasma_padding_steps;
+    double field_solver_subtraction_trick; /* multiplies the *_avg terms (lcode.py:264-268) */
+    int field_solver_variant_A;
+    int precision;                        /* LC3D_PREC_* */
+} lc3d_params;
+
+/* The xi-step state, attribute names of lcode.py:926-929. */
+typedef struct lc3d_state_ptrs {
+    double *x_offt, *y_offt, *px, *py, *pz;   /* Nc x Nc */
+    double *Ex, *Ey, *Ez, *Bx, *By, *Bz;      /* N x N */
+    double *ro, *jx, *jy, *jz;                /* N x N */
+} lc3d_state_ptrs;
+
+/* const of lcode.py:964-965. */
+typedef struct lc3d_const_ptrs {
+    const double *m, *q, *x_init, *y_init;    /* Nc x Nc */
+    const double *ro_initial;                 /* N x N */
+} lc3d_const_ptrs;
+
+/* virt_params of lcode.py:566-570 (indices as int32). */
+typedef struct lc3d_virt_ptrs {
+    const double *influence_prev, *influence_next;   /* Nf */
+    const int32_t *indices_prev, *indices_next;      /* Nf */
+    const double *fine_grid;                         /* Nf */
+} lc3d_virt_ptrs;
+
+typedef struct lc3d_ctx lc3d_ctx;
+
+/* Derived sizes of a configuration without creating a context:
+ * Nc = coarse particles per side, Nf = fine particles per side,
+ * reflect_boundary as init() computes it (lcode.py:947-949, 454-487). */
+int lc3d_sizes(const lc3d_params* p, int* Nc, int* Nf, double* reflect_boundary);
+
+/* Create a context on `device` (replaces the per-config state that the
+ * reference keeps in cp.memoize caches, lcode.py:144, 215, 316). */
+int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out);
+int lc3d_destroy(lc3d_ctx* ctx);
+const char* lc3d_strerror(int code);
+
+/* Copy const and virt_params into the context (device to device). */
+int lc3d_set_const(lc3d_ctx* ctx, const lc3d_const_ptrs* c,
+                   const lc3d_virt_ptrs* v, void* stream);
+
+/* Context-owned state (double-buffered): copy in / copy out. */
+int lc3d_set_state(lc3d_ctx* ctx, const lc3d_state_ptrs* s, void* stream);
+int lc3d_get_state(lc3d_ctx* ctx, lc3d_state_ptrs* s, void* stream);
+
+/* One xi step on the context-owned state (lcode.py:828-931); beam_ro is an
+ * N x N device array. Graph-capturable. */
+int lc3d_step(lc3d_ctx* ctx, const double* beam_ro, void* stream);
+
+/* One xi step from caller-owned prev into caller-owned out arrays
+ * (lcode.py:828-931, the reference's ownership: prev is kept, out is new).
+ * `out` must not alias `prev`. */
+int lc3d_step_arrays(lc3d_ctx* ctx, const lc3d_state_ptrs* prev,
+                     const lc3d_state_ptrs* out, const double* beam_ro,
+                     void* stream);
+
+/* ---- per-stage entry points (the functions step() calls) ---- */
+
+/* move_estimate_wo_fields, lcode.py:369-391. */
+int lc3d_move_estimate_wo_fields(lc3d_ctx* ctx, const double* m,
+        const double* x_init, const double* y_init,
+        const double* prev_x_offt, const double* prev_y_offt,
+        const double* px, const double* py, const double* pz,
+        double* out_x_offt, double* out_y_offt, void* stream);
+
+/* move_smart / move_smart_kernel, lcode.py:704-823. */
+int lc3d_move_smart(lc3d_ctx* ctx, const double* m, const double* q,
+        const double* x_init, const double* y_init,
+        const double* x_prev_offt, const double* y_prev_offt,
+        const double* estimated_x_offt, const double* estimated_y_offt,
+        const double* px_prev, const double* py_prev, const double* pz_prev,
+        const double* Ex_avg, const double* Ey_avg, const double* Ez_avg,
+        const double* Bx_avg, const double* By_avg, const double* Bz_avg,
+        double* new_x_offt, double* new_y_offt,
+        double* new_px, double* new_py, double* new_pz, void* stream);
+
+/* deposit / deposit_kernel, lcode.py:626-689 (virt_params from the context;
+ * ro_initial may be NULL for the initial deposition, lcode.py:692-699).
+ * Deterministic: bit-identical results for identical inputs. */
+int lc3d_deposit(lc3d_ctx* ctx, const double* ro_initial,
+        const double* x_offt, const double* y_offt,
+        const double* m, const double* q,
+        const double* px, const double* py, const double* pz,
+        double* out_ro, double* out_jx, double* out_jy, double* out_jz,
+        void* stream);
+
+/* calculate_Ex_Ey_Bx_By, lcode.py:246-290. */
+int lc3d_calculate_Ex_Ey_Bx_By(lc3d_ctx* ctx,
+        const double* Ex_avg, const double* Ey_avg,
+        const double* Bx_avg, const double* By_avg,
+        const double* beam_ro, const double* ro, const double* jx,
+        const double* jy, const double* jz,
+        const double* jx_prev, const double* jy_prev,
+        double* Ex, double* Ey, double* Bx, double* By, void* stream);
+
+/* calculate_Ez, lcode.py:160-184. */
+int lc3d_calculate_Ez(lc3d_ctx* ctx, const double* jx, const double* jy,
+                      double* Ez, void* stream);
+
+/* calculate_Bz, lcode.py:333-364. */
+int lc3d_calculate_Bz(lc3d_ctx* ctx, const double* jx, const double* jy,
+                      double* Bz, void* stream);
+
+/* ---- launch accounting and kernel timing ---- */
+
+/* Stage categories of the launch counters and timers. */
+#define LC3D_STAGE_MOVE 0          /* move_smart_kernel / estimate */
+#define LC3D_STAGE_DEPOSIT 1       /* deposit_kernel (fine particles -> accumulators) */
+#define LC3D_STAGE_DEPOSIT_FIN 2   /* accumulators -> ro, jx, jy, jz */
+#define LC3D_STAGE_RHS 3           /* field-solver right-hand sides */
+#define LC3D_STAGE_TRANSFORM 4     /* DST/DCT transform GEMMs */
+#define LC3D_STAGE_FIELD_FIN 5     /* Variant A, Bz mean, half-step averages */
+#define LC3D_STAGE_OTHER 6
+#define LC3D_NSTAGES 7
+
+/* Enable (1) or disable (0) CUDA-event timing of every kernel launch of
+ * this context, and reset the counters. Not for use under stream capture.
+ * No reference counterpart (the reference has no instrumentation). */
+int lc3d_profile(lc3d_ctx* ctx, int enable);
+
+/* Synchronise the device and report, per stage, the kernel launches issued
+ * since the last reset (launches[]) and, with timing enabled, the summed
+ * kernel time in ms (ms[]) and the number of timed launches (timed[]).
+ * Arrays hold LC3D_NSTAGES entries; any may be NULL. Resets the counters. */
+int lc3d_profile_read(lc3d_ctx* ctx, long long* launches, double* ms, long long* timed);
+
+/* Read and clear the device error flag (synchronises `stream`); returns
+ * LC3D_OK, LC3D_ERR_WINDOW or LC3D_ERR_NONFINITE. */
+int lc3d_check_error(lc3d_ctx* ctx, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LC3D_H */

@@ -1,0 +1,494 @@
+// Spectral field solvers in dense-transform (GEMM) form, float64.
+//
+// Reference: lcode.py:124-184 (dst2d, dirichlet_matrix, calculate_Ez),
+// 187-290 (mix2d, mixed_matrix, dx_dy, calculate_Ex_Ey_Bx_By), 293-364
+// (dct2d, neumann_matrix, calculate_Bz).
+//
+// The reference builds DST-I / DCT-I out of padded real FFTs. Those
+// transforms are linear maps with fixed matrices, so every solve is
+//     F = L (Lambda o (L X R)) R
+// with X the right-hand side, L / R the transform along axis 0 / axis 1 and
+// Lambda the eigenvalue matrix (normalisation folded in):
+//     S2[k][n] = 2 sin(pi (k+1)(n+1) / (N-1))            (DST-I, M = N-2)
+//     C[k][n]  = c_n cos(pi k n / (N-1)), c_0 = c_{N-1} = 1, else 2   (DCT-I)
+//   Ey, Bx: X = rhs[1:-1, :]      L = S2, R = C^T, Lambda = mixed_matrix
+//   Ex, By: X = rhs[:, 1:-1]      L = C,  R = S2,  Lambda = mixed_matrix^T
+//           (the reference solves them transposed, lcode.py:287-288)
+//   Ez:     X = rhs_inner         L = S2, R = S2,  Lambda = dirichlet_matrix
+//   Bz:     X = rhs               L = C,  R = C^T, Lambda = neumann_matrix
+//           (dct2d is minus the DCT-I; the two signs cancel)
+// All six fields of a solve run as one batched GEMM per stage (4 stages).
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lc3d_internal.cuh"
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Right-hand sides, lcode.py:166-168, 234-268, 339-343.
+// ---------------------------------------------------------------------------
+struct RhsArgs {
+    SolveInputs in;
+    double st, h, dxi;
+    double* out[6];       // Ex Ey Ez Bx By Bz right-hand sides (N x N, may be NULL)
+    int N;
+};
+
+__device__ __forceinline__ double avg_in(const double* a, const double* a_prev, size_t k) {
+    return a_prev ? (a[k] + a_prev[k]) / 2 : a[k];
+}
+
+__global__ void __launch_bounds__(256) rhs_kernel(const __grid_constant__ RhsArgs a) {
+    const int N = a.N;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N * N) return;
+    const int i = k / N, j = k - i * N;
+    const bool interior = i >= 1 && i <= N - 2 && j >= 1 && j <= N - 2;
+    const SolveInputs& in = a.in;
+    const double h2 = a.h * 2;
+    if (a.out[0]) {   // the four transverse fields
+        double dro_dx = 0, dro_dy = 0, djz_dx = 0, djz_dy = 0;
+        if (interior) {
+            // (ro_in + beam_ro) and (jz_in + beam_ro) at the four neighbours
+            const size_t kp = k + N, km = k - N, lp = k + 1, lm = k - 1;
+            dro_dx = ((avg_in(in.ro, in.ro_prev, kp) + in.beam[kp]) -
+                      (avg_in(in.ro, in.ro_prev, km) + in.beam[km])) / h2;
+            dro_dy = ((avg_in(in.ro, in.ro_prev, lp) + in.beam[lp]) -
+                      (avg_in(in.ro, in.ro_prev, lm) + in.beam[lm])) / h2;
+            djz_dx = ((avg_in(in.jz, in.jz_prev, kp) + in.beam[kp]) -
+                      (avg_in(in.jz, in.jz_prev, km) + in.beam[km])) / h2;
+            djz_dy = ((avg_in(in.jz, in.jz_prev, lp) + in.beam[lp]) -
+                      (avg_in(in.jz, in.jz_prev, lm) + in.beam[lm])) / h2;
+        }
+        const double djx_dxi = (in.jx_prev[k] - in.jx[k]) / a.dxi;
+        const double djy_dxi = (in.jy_prev[k] - in.jy[k]) / a.dxi;
+        const double st = a.st;
+        a.out[0][k] = -((dro_dx - djx_dxi) - in.Ex_sub[k] * st);
+        a.out[1][k] = -((dro_dy - djy_dxi) - in.Ey_sub[k] * st);
+        a.out[3][k] = +((djz_dy - djy_dxi) + in.Bx_sub[k] * st);
+        a.out[4][k] = -((djz_dx - djx_dxi) - in.By_sub[k] * st);
+    }
+    if (a.out[2] || a.out[5]) {
+        double ez = 0, bz = 0;
+        if (interior) {
+            const double djx_dx = in.jx[k + N] - in.jx[k - N];
+            const double djy_dy = in.jy[k + 1] - in.jy[k - 1];
+            const double djx_dy = in.jx[k + 1] - in.jx[k - 1];
+            const double djy_dx = in.jy[k + N] - in.jy[k - N];
+            ez = -(djx_dx + djy_dy) / h2;
+            bz = -(djx_dy - djy_dx) / h2;
+        }
+        if (a.out[2]) a.out[2][k] = ez;
+        if (a.out[5]) a.out[5][k] = bz;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Batched float64 GEMM, C = A B (optionally C = Lambda o (A B)), row-major.
+// 64 x 64 tiles, k-step 16, 256 threads with 4 x 4 outputs each.
+// ---------------------------------------------------------------------------
+constexpr int MAX_PROBS = 6;
+
+struct GemmProb {
+    const double *A, *B, *L;
+    double* C;
+    int M, N, K, lda, ldb, ldc, ldl;
+    int tiles_n, tile_start;
+};
+
+struct GemmBatch {
+    GemmProb p[MAX_PROBS];
+    int count, total_tiles;
+};
+
+constexpr int GT = 64, GK = 16;
+
+__global__ void __launch_bounds__(256) dgemm_kernel(const __grid_constant__ GemmBatch b) {
+    __shared__ double As[2][GK][GT + 1];
+    __shared__ double Bs[2][GK][GT];
+    const int bid = blockIdx.x;
+    int pi = 0;
+#pragma unroll 1
+    for (int q = 1; q < b.count; ++q)
+        if (bid >= b.p[q].tile_start) pi = q;
+    const GemmProb& P = b.p[pi];
+    const int t = bid - P.tile_start;
+    const int tm = t / P.tiles_n, tn = t - tm * P.tiles_n;
+    const int row0 = tm * GT, col0 = tn * GT;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+
+    // load assignments
+    const int a_k = tid & 15, a_r = tid >> 4;        // rows a_r + 16 r
+    const int b_n = tid & 63, b_k = tid >> 6;        // k rows b_k + 4 r
+    double ra[4], rb[4];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int row = row0 + a_r + 16 * r, kk = k0 + a_k;
+            ra[r] = (row < P.M && kk < P.K) ? P.A[(size_t)row * P.lda + kk] : 0.0;
+            const int kb = k0 + b_k + 4 * r, col = col0 + b_n;
+            rb[r] = (kb < P.K && col < P.N) ? P.B[(size_t)kb * P.ldb + col] : 0.0;
+        }
+    };
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+
+    const int nk = (P.K + GK - 1) / GK;
+    load(0);
+    for (int kt = 0; kt < nk; ++kt) {
+        const int buf = kt & 1;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            As[buf][a_k][a_r + 16 * r] = ra[r];
+            Bs[buf][b_k + 4 * r][b_n] = rb[r];
+        }
+        __syncthreads();
+        if (kt + 1 < nk) load((kt + 1) * GK);
+#pragma unroll
+        for (int kk = 0; kk < GK; ++kk) {
+            double av[4], bv[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) av[i] = As[buf][kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) bv[j] = Bs[buf][kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int row = row0 + ty + 16 * i;
+        if (row >= P.M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int col = col0 + tx + 16 * j;
+            if (col >= P.N) continue;
+            double v = acc[i][j];
+            if (P.L) v *= P.L[(size_t)row * P.ldl + col];
+            P.C[(size_t)row * P.ldc + col] = v;
+        }
+    }
+}
+
+int launch_gemm(lc3d_ctx* c, GemmBatch& b, cudaStream_t s) {
+    int tiles = 0;
+    for (int q = 0; q < b.count; ++q) {
+        GemmProb& p = b.p[q];
+        p.tiles_n = (p.N + GT - 1) / GT;
+        p.tile_start = tiles;
+        tiles += ((p.M + GT - 1) / GT) * p.tiles_n;
+    }
+    b.total_tiles = tiles;
+    if (tiles == 0) return LC3D_OK;
+    ProfScope ps(c, LC3D_STAGE_TRANSFORM, s);
+    dgemm_kernel<<<tiles, 256, 0, s>>>(b);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic mean (fixed summation tree) and the step finalisation.
+// ---------------------------------------------------------------------------
+constexpr int RED_THREADS = 256;
+
+__device__ __forceinline__ double block_sum_fixed(double v, double* sh) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = RED_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    return sh[0];
+}
+
+__global__ void __launch_bounds__(RED_THREADS) partial_sum_kernel(const double* __restrict__ a, int n,
+                                                                  double* __restrict__ partial) {
+    __shared__ double sh[RED_THREADS];
+    double v = 0;
+    for (int k = blockIdx.x * RED_THREADS + threadIdx.x; k < n; k += gridDim.x * RED_THREADS) v += a[k];
+    double s = block_sum_fixed(v, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__device__ double mean_from_partials(const double* partial, int nblocks, double inv_n, double* sh) {
+    double v = 0;
+    for (int k = threadIdx.x; k < nblocks; k += RED_THREADS) v += partial[k];
+    return block_sum_fixed(v, sh) * inv_n;
+}
+
+struct FinalizeArgs {
+    const double* raw[6];
+    const double* prev[6];
+    double* out[6];
+    double* avg[6];
+    const double* partial;
+    int nblocks, n, variant_A, has_bz;
+    double inv_n;
+};
+
+__global__ void __launch_bounds__(RED_THREADS) finalize_step_kernel(const __grid_constant__ FinalizeArgs a) {
+    __shared__ double sh[RED_THREADS];
+    const double mean = a.has_bz ? mean_from_partials(a.partial, a.nblocks, a.inv_n, sh) : 0.0;
+    const int k = blockIdx.x * RED_THREADS + threadIdx.x;
+    if (k >= a.n) return;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        if (!a.raw[f]) continue;
+        double v = a.raw[f][k];
+        if (f == 5) v -= mean;
+        if (a.variant_A && f != 2 && f != 5) v = 2 * v - a.prev[f][k];
+        if (a.out[f]) a.out[f][k] = v;
+        a.avg[f][k] = (v + a.prev[f][k]) / 2;
+    }
+}
+
+__global__ void __launch_bounds__(RED_THREADS) subtract_mean_kernel(double* a, int n, const double* partial,
+                                                                    int nblocks, double inv_n) {
+    __shared__ double sh[RED_THREADS];
+    const double mean = mean_from_partials(partial, nblocks, inv_n, sh);
+    const int k = blockIdx.x * RED_THREADS + threadIdx.x;
+    if (k < n) a[k] -= mean;
+}
+
+// ---------------------------------------------------------------------------
+// Host: transform and eigenvalue matrices.
+// ---------------------------------------------------------------------------
+
+// sin(pi r / L) for integer r, with the argument reduced to [0, pi/2].
+double sin_pi_frac(long long r, long long L) {
+    r %= 2 * L;
+    if (r < 0) r += 2 * L;
+    double sign = 1;
+    if (r >= L) { r -= L; sign = -1; }
+    if (2 * r > L) r = L - r;
+    return sign * std::sin(M_PI * (double)r / (double)L);
+}
+
+// lam[k] = 4 / h**2 * sin(k pi / (2 (N - 1)))**2 as lcode.py:152-154 writes it
+double lam(int k, int N, double h) {
+    double s = std::sin(k * M_PI / (2.0 * (N - 1)));
+    return 4 / (h * h) * (s * s);
+}
+
+int upload(double** dst, const std::vector<double>& v) {
+    LC3D_CUDA_TRY(cudaMalloc(dst, v.size() * sizeof(double)));
+    LC3D_CUDA_TRY(cudaMemcpy(*dst, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return LC3D_OK;
+}
+
+}  // namespace
+
+int fields_init(lc3d_ctx* c) {
+    const int N = c->N, M = c->M;
+    const long long L = N - 1;
+    const double h = c->p.grid_step_size;
+    std::vector<double> S2((size_t)M * M), C((size_t)N * N), CT((size_t)N * N);
+    for (int k = 0; k < M; ++k)
+        for (int n = 0; n < M; ++n) S2[(size_t)k * M + n] = 2 * sin_pi_frac((long long)(k + 1) * (n + 1), L);
+    for (int k = 0; k < N; ++k)
+        for (int n = 0; n < N; ++n) {
+            // cos(pi r / L) = sin(pi (2 r + L) / (2 L)), r = k n mod 2L
+            const long long r = ((long long)k * n) % (2 * L);
+            const double cv = sin_pi_frac(2 * r + L, 2 * L);
+            const double w = (n == 0 || n == N - 1) ? 1.0 : 2.0;
+            C[(size_t)k * N + n] = w * cv;
+            CT[(size_t)n * N + k] = w * cv;
+        }
+    const double norm = 1.0 / ((2.0 * (N - 1)) * (2.0 * (N - 1)));
+    const double trick = c->p.field_solver_subtraction_trick != 0 ? 1.0 : 0.0;
+    std::vector<double> ld((size_t)M * M), lm((size_t)M * N), lmT((size_t)N * M), ln((size_t)N * N);
+    std::vector<double> lamk(N);
+    for (int k = 0; k < N; ++k) lamk[k] = lam(k, N, h);
+    for (int i = 0; i < M; ++i)
+        for (int j = 0; j < M; ++j) ld[(size_t)i * M + j] = (1 / (lamk[i + 1] + lamk[j + 1])) * norm;
+    for (int i = 0; i < M; ++i)
+        for (int j = 0; j < N; ++j) {
+            const double v = (1 / (lamk[i + 1] + lamk[j] + trick)) * norm;
+            lm[(size_t)i * N + j] = v;
+            lmT[(size_t)j * M + i] = v;
+        }
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j)
+            ln[(size_t)i * N + j] = (i == 0 && j == 0) ? 0.0 : (1 / (lamk[i] + lamk[j])) * norm;
+    LC3D_TRY(upload(&c->S2, S2));
+    LC3D_TRY(upload(&c->C, C));
+    LC3D_TRY(upload(&c->CT, CT));
+    LC3D_TRY(upload(&c->lam_dir, ld));
+    LC3D_TRY(upload(&c->lam_mix, lm));
+    LC3D_TRY(upload(&c->lam_mixT, lmT));
+    LC3D_TRY(upload(&c->lam_neu, ln));
+    const size_t plane = (size_t)N * N * sizeof(double);
+    for (int f = 0; f < 6; ++f) {
+        LC3D_CUDA_TRY(cudaMalloc(&c->rhs[f], plane));
+        LC3D_CUDA_TRY(cudaMalloc(&c->t1[f], plane));
+        LC3D_CUDA_TRY(cudaMalloc(&c->t2[f], plane));
+        LC3D_CUDA_TRY(cudaMalloc(&c->raw[f], plane));
+        LC3D_CUDA_TRY(cudaMemset(c->rhs[f], 0, plane));
+        LC3D_CUDA_TRY(cudaMemset(c->raw[f], 0, plane));
+    }
+    c->red_blocks = 160;
+    LC3D_CUDA_TRY(cudaMalloc(&c->red, c->red_blocks * sizeof(double)));
+    return LC3D_OK;
+}
+
+void fields_free(lc3d_ctx* c) {
+    double** ps[] = {&c->S2, &c->C, &c->CT, &c->lam_dir, &c->lam_mix, &c->lam_mixT, &c->lam_neu, &c->red};
+    for (double** p : ps) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    for (int f = 0; f < 6; ++f) {
+        double** q[] = {&c->rhs[f], &c->t1[f], &c->t2[f], &c->raw[f]};
+        for (double** p : q) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
+    }
+}
+
+namespace {
+
+struct FieldGeom {
+    int rows, cols;
+    size_t off;            // offset of X / output inside an N x N plane
+    const double *L, *R, *Lam;
+    int ldL, ldR, ldLam;
+};
+
+FieldGeom geom(const lc3d_ctx* c, int f) {
+    const int N = c->N, M = c->M;
+    FieldGeom g;
+    switch (f) {
+        case 0: case 4:   // Ex, By: solved transposed
+            g = {N, M, 1, c->C, c->S2, c->lam_mixT, N, M, M};
+            break;
+        case 1: case 3:   // Ey, Bx
+            g = {M, N, (size_t)N, c->S2, c->CT, c->lam_mix, M, N, N};
+            break;
+        case 2:           // Ez
+            g = {M, M, (size_t)N + 1, c->S2, c->S2, c->lam_dir, M, M, M};
+            break;
+        default:          // Bz
+            g = {N, N, 0, c->C, c->CT, c->lam_neu, N, N, N};
+            break;
+    }
+    return g;
+}
+
+}  // namespace
+
+int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutputs& o, cudaStream_t s) {
+    const int N = c->N;
+    const int n = N * N;
+    bool on[6] = {false, false, false, false, false, false};
+    if (which & LC3D_F_EXEYBXBY) on[0] = on[1] = on[3] = on[4] = true;
+    if (which & LC3D_F_EZ) on[2] = true;
+    if (which & LC3D_F_BZ) on[5] = true;
+
+    RhsArgs ra;
+    memset(&ra, 0, sizeof(ra));
+    ra.in = in;
+    ra.st = c->p.field_solver_subtraction_trick;
+    ra.h = c->p.grid_step_size;
+    ra.dxi = c->p.xi_step_size;
+    ra.N = N;
+    for (int f = 0; f < 6; ++f) ra.out[f] = on[f] ? c->rhs[f] : nullptr;
+    {
+        ProfScope ps(c, LC3D_STAGE_RHS, s);
+        rhs_kernel<<<(n + 255) / 256, 256, 0, s>>>(ra);
+        LC3D_CUDA_TRY(cudaGetLastError());
+    }
+
+    // destination of the raw solution
+    double* dst[6];
+    for (int f = 0; f < 6; ++f) {
+        dst[f] = nullptr;
+        if (!on[f]) continue;
+        if (o.mode == 0) {
+            dst[f] = o.out[f];
+            if (f != 5) LC3D_CUDA_TRY(cudaMemsetAsync(dst[f], 0, (size_t)n * sizeof(double), s));
+        } else {
+            dst[f] = c->raw[f];
+        }
+    }
+    // the four GEMM stages
+    for (int stage = 0; stage < 4; ++stage) {
+        GemmBatch b;
+        memset(&b, 0, sizeof(b));
+        for (int f = 0; f < 6; ++f) {
+            if (!on[f]) continue;
+            const FieldGeom g = geom(c, f);
+            GemmProb& p = b.p[b.count++];
+            switch (stage) {
+                case 0:   // t1 = X R
+                    p.A = c->rhs[f] + g.off; p.lda = N;
+                    p.B = g.R; p.ldb = g.ldR;
+                    p.C = c->t1[f]; p.ldc = N;
+                    p.M = g.rows; p.N = g.cols; p.K = g.cols;
+                    break;
+                case 1:   // t2 = Lambda o (L t1)
+                    p.A = g.L; p.lda = g.ldL;
+                    p.B = c->t1[f]; p.ldb = N;
+                    p.C = c->t2[f]; p.ldc = N;
+                    p.L = g.Lam; p.ldl = g.ldLam;
+                    p.M = g.rows; p.N = g.cols; p.K = g.rows;
+                    break;
+                case 2:   // t1 = t2 R
+                    p.A = c->t2[f]; p.lda = N;
+                    p.B = g.R; p.ldb = g.ldR;
+                    p.C = c->t1[f]; p.ldc = N;
+                    p.M = g.rows; p.N = g.cols; p.K = g.cols;
+                    break;
+                default:  // out = L t1
+                    p.A = g.L; p.lda = g.ldL;
+                    p.B = c->t1[f]; p.ldb = N;
+                    p.C = dst[f] + g.off; p.ldc = N;
+                    p.M = g.rows; p.N = g.cols; p.K = g.rows;
+                    break;
+            }
+        }
+        LC3D_TRY(launch_gemm(c, b, s));
+    }
+    const double inv_n = 1.0 / n;
+    if (on[5]) {
+        ProfScope ps(c, LC3D_STAGE_FIELD_FIN, s);
+        partial_sum_kernel<<<c->red_blocks, RED_THREADS, 0, s>>>(dst[5], n, c->red);
+        LC3D_CUDA_TRY(cudaGetLastError());
+    }
+    if (o.mode == 0) {
+        if (on[5]) {
+            ProfScope ps(c, LC3D_STAGE_FIELD_FIN, s);
+            subtract_mean_kernel<<<(n + RED_THREADS - 1) / RED_THREADS, RED_THREADS, 0, s>>>(
+                dst[5], n, c->red, c->red_blocks, inv_n);
+            LC3D_CUDA_TRY(cudaGetLastError());
+        }
+        return LC3D_OK;
+    }
+    FinalizeArgs fa;
+    memset(&fa, 0, sizeof(fa));
+    for (int f = 0; f < 6; ++f) {
+        if (!on[f]) continue;
+        fa.raw[f] = c->raw[f];
+        fa.prev[f] = o.prev[f];
+        fa.out[f] = o.out[f];
+        fa.avg[f] = o.avg[f];
+    }
+    fa.partial = c->red;
+    fa.nblocks = c->red_blocks;
+    fa.n = n;
+    fa.variant_A = c->p.field_solver_variant_A;
+    fa.has_bz = on[5];
+    fa.inv_n = inv_n;
+    ProfScope ps(c, LC3D_STAGE_FIELD_FIN, s);
+    finalize_step_kernel<<<(n + RED_THREADS - 1) / RED_THREADS, RED_THREADS, 0, s>>>(fa);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}

@@ -1,0 +1,165 @@
+// Internal declarations shared by the liblc3d translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/lc3d.h"
+
+// Device error flag bits (the host maps them to LC3D_ERR_*).
+#define LC3D_FLAG_WINDOW 1u
+#define LC3D_FLAG_NONFINITE 2u
+
+#define LC3D_CUDA_TRY(expr)                                                  \
+    do {                                                                     \
+        cudaError_t _e = (expr);                                             \
+        if (_e != cudaSuccess) {                                             \
+            lc3d_set_last_cuda_error(_e, #expr, __FILE__, __LINE__);         \
+            return LC3D_ERR_CUDA;                                            \
+        }                                                                    \
+    } while (0)
+
+#define LC3D_TRY(expr)                                                       \
+    do {                                                                     \
+        int _rc = (expr);                                                    \
+        if (_rc != LC3D_OK) return _rc;                                      \
+    } while (0)
+
+void lc3d_set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+
+// ---------------------------------------------------------------------------
+// Particle kernels (particles.cu)
+// ---------------------------------------------------------------------------
+
+struct MoveArgs {
+    const double *m, *q, *x_init, *y_init;
+    const double *x_prev, *y_prev;        // prev offsets
+    const double *est_x, *est_y;          // estimated offsets (NULL: estimate inline)
+    const double *px_prev, *py_prev, *pz_prev;
+    const double *F[6];                   // Ex Ey Ez Bx By Bz (averaged)
+    double *out_x, *out_y, *out_px, *out_py, *out_pz;
+    int n;                                // coarse particles
+    int N;                                // grid_steps
+    double h, dxi, rb;
+    unsigned* err;
+};
+
+struct EstimateArgs {
+    const double *m, *x_init, *y_init, *x_prev, *y_prev, *px, *py, *pz;
+    double *out_x, *out_y;
+    int n;
+    double dxi, rb;
+};
+
+struct DepositArgs {
+    const double *x_offt, *y_offt, *m, *q, *px, *py, *pz;   // coarse, Nc x Nc
+    const double *inf_prev, *inf_next, *fine_grid;            // Nf
+    const int32_t *idx_prev, *idx_next;                       // Nf
+    unsigned long long* acc;                                  // N*N*8 fixed-point words
+    int Nc, Nf, N;
+    double h, sf;
+    unsigned* err;
+};
+
+struct DepositFinalizeArgs {
+    unsigned long long* acc;
+    const double* ro_initial;             // may be NULL
+    double *ro, *jx, *jy, *jz;
+    int n;                                // N*N
+};
+
+int launch_move_estimate(const EstimateArgs& a, cudaStream_t s);
+int launch_move_smart(const MoveArgs& a, cudaStream_t s);
+int launch_deposit_main(const DepositArgs& a, cudaStream_t s);
+int launch_deposit_finalize(const DepositFinalizeArgs& f, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Launch accounting and optional per-launch CUDA-event timing (lc3d_api.cu).
+// Categories are the LC3D_STAGE_* values of include/lc3d.h.
+// ---------------------------------------------------------------------------
+struct lc3d_ctx;
+struct ProfScope {
+    lc3d_ctx* c;
+    int cat, slot;
+    cudaStream_t s;
+    ProfScope(lc3d_ctx* c, int cat, cudaStream_t s);
+    ~ProfScope();
+};
+
+// ---------------------------------------------------------------------------
+// Field solvers (fields.cu)
+// ---------------------------------------------------------------------------
+
+// Which fields a solve computes.
+#define LC3D_F_EXEYBXBY 1
+#define LC3D_F_EZ 2
+#define LC3D_F_BZ 4
+#define LC3D_F_ALL 7
+
+struct SolveInputs {
+    const double *ro, *ro_prev;           // ro_prev != NULL: ro_in = (ro + ro_prev) / 2
+    const double *jz, *jz_prev;           // likewise for jz
+    const double *jx, *jy, *jx_prev, *jy_prev, *beam;
+    const double *Ex_sub, *Ey_sub, *Bx_sub, *By_sub;   // subtraction-trick terms
+};
+
+// mode 0: raw fields into out[] (zero border, Bz mean removed), as the
+//         reference's calculate_* functions return them;
+// mode 1: step finalisation: Variant A (if set) against prev[], Bz mean
+//         removed, fields into out[] (optional, may be NULL) and the
+//         half-step averages (F + prev) / 2 into avg[].
+struct SolveOutputs {
+    int mode;
+    double* out[6];                       // Ex Ey Ez Bx By Bz
+    const double* prev[6];
+    double* avg[6];
+};
+
+int solve_fields(lc3d_ctx* ctx, int which, const SolveInputs& in,
+                 const SolveOutputs& o, cudaStream_t s);
+int fields_init(lc3d_ctx* ctx);           // transform matrices, workspaces
+void fields_free(lc3d_ctx* ctx);
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+
+struct lc3d_ctx {
+    lc3d_params p;
+    int device;
+    int N, M, Nc, Nf;                     // M = N - 2
+    double rb, sf;                        // reflect_boundary, 1/(c f)^2
+    // owned constants
+    double *m, *q, *x_init, *y_init, *ro_initial;
+    double *inf_prev, *inf_next, *fine_grid;
+    int32_t *idx_prev, *idx_next;
+    int const_set;
+    // owned state, double-buffered
+    lc3d_state_ptrs st[2];
+    int cur, state_set;
+    // step workspaces
+    double* pw[2][5];                     // predictor / corrector particles
+    double* dens[4];                      // ro jx jy jz of predictor / corrector
+    double* avg[6];                       // half-step averaged fields
+    unsigned long long* acc;              // deposit fixed-point accumulators
+    unsigned* err;                        // device error flag
+    double* zeros;                        // N x N zeros (absent beam)
+    // field-solver workspaces (fields.cu)
+    double *S2, *C, *CT;                  // 2*DST-I (M x M), DCT-I (N x N), its transpose
+    double *lam_dir, *lam_mix, *lam_mixT, *lam_neu;
+    double* rhs[6];                       // right-hand sides, N x N planes
+    double* t1[6];                        // transform scratch
+    double* t2[6];
+    double* raw[6];                       // raw solver output, zero border
+    double* red;                          // Bz mean partial sums
+    int red_blocks;
+    void* mixed;                          // mixed-precision solver state (fields_mixed.cu)
+    // launch accounting / profiling
+    long long launches[LC3D_NSTAGES];
+    int prof_on, prof_used, prof_cap, prof_overflow;
+    cudaEvent_t* prof_ev;                 // 2 per recorded launch
+    int* prof_cat;
+    double prof_ms[LC3D_NSTAGES];
+    long long prof_count[LC3D_NSTAGES];
+};

@@ -1,0 +1,457 @@
+"""Drop-in host interface of the B200 LCODE 3D xi-step solver.
+
+Mirrors the public functions of the reference ``lcode.py`` (same names,
+same arguments, same returned attribute names) so that the reference's CLI
+loop (lcode.py:1032-1051) or embedding code can switch to it:
+
+    init(config) -> (xs, ys, const, virt_params, state)        lcode.py:936-975
+    step(config, const, virt_params, prev, beam_ro) -> state    lcode.py:828-931
+
+plus the stage functions ``step`` is made of (``move_estimate_wo_fields``,
+``move_smart``, ``deposit``, ``initial_deposition``, ``calculate_Ex_Ey_Bx_By``,
+``calculate_Ez``, ``calculate_Bz``). Device arrays are torch CUDA float64
+tensors (cupy arrays in the reference); ``GPUArraysView`` copies to numpy on
+attribute access like the reference's. All device work runs in liblc3d.so
+(include/lc3d.h) on the current torch stream; there is no CPU fallback.
+
+Extra, optional config attributes (absent in the reference's config):
+``lc3d_precision`` = 'fp64' (default) or 'mixed'.
+"""
+import ctypes
+import math
+import os
+import sys
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import lib, check
+
+ELECTRON_CHARGE = -1
+ELECTRON_MASS = 1
+WARP_SIZE = 32
+
+#: read the device error flag after every step()/stage call (one host sync);
+#: the reference has no such check and silently corrupts memory instead
+check_errors = True
+
+
+# ---------------------------------------------------------------------------
+# Array groups (lcode.py:52-119)
+# ---------------------------------------------------------------------------
+
+def _device():
+    if not torch.cuda.is_available():
+        raise RuntimeError('lcode3d_b200 needs a CUDA device (B200, sm_100a); '
+                           'there is no CPU fallback')
+    return torch.device('cuda', torch.cuda.current_device())
+
+
+def to_device(a, dtype=None):
+    """Like ``cp.asarray``: a contiguous device tensor (float64 unless the
+    input is an integer array)."""
+    dev = _device()
+    if isinstance(a, torch.Tensor):
+        t = a
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(a)))
+    if dtype is None:
+        dtype = t.dtype if not t.dtype.is_floating_point else torch.float64
+        if dtype in (torch.int32, torch.int16, torch.int8, torch.uint8, torch.bool):
+            dtype = torch.int64
+    return t.to(device=dev, dtype=dtype).contiguous()
+
+
+class GPUArrays:
+    """Named group of device arrays (lcode.py:52-69)."""
+
+    def __init__(self, **kwargs):
+        for name, array in kwargs.items():
+            setattr(self, name, to_device(array))
+
+
+class GPUArraysView:
+    """Attribute access copies device -> host numpy; assignment copies
+    host -> device (lcode.py:73-119)."""
+
+    def __init__(self, gpu_arrays):
+        super().__setattr__('_arrs', gpu_arrays)
+
+    def __dir__(self):
+        return list(set(super().__dir__() + dir(self._arrs)))
+
+    def __getattr__(self, attrname):
+        return getattr(self._arrs, attrname).cpu().numpy()
+
+    def __setattr__(self, attrname, value):
+        t = getattr(self._arrs, attrname)
+        t.copy_(torch.as_tensor(np.asarray(value), dtype=t.dtype))
+
+
+# ---------------------------------------------------------------------------
+# Per-config solver context (replaces the cp.memoize caches of the
+# reference, lcode.py:144, 215, 316)
+# ---------------------------------------------------------------------------
+
+def _precision(config):
+    p = getattr(config, 'lc3d_precision', 'fp64')
+    if p in ('fp64', _lib.PREC_FP64):
+        return _lib.PREC_FP64
+    if p in ('mixed', _lib.PREC_MIXED):
+        return _lib.PREC_MIXED
+    raise ValueError(f'lc3d_precision must be "fp64" or "mixed", not {p!r}')
+
+
+def params_of(config):
+    p = _lib.Params()
+    p.grid_steps = int(config.grid_steps)
+    p.grid_step_size = float(config.grid_step_size)
+    p.xi_step_size = float(config.xi_step_size)
+    p.plasma_coarseness = int(config.plasma_coarseness)
+    p.plasma_fineness = int(config.plasma_fineness)
+    p.reflect_padding_steps = int(config.reflect_padding_steps)
+    p.plasma_padding_steps = int(config.plasma_padding_steps)
+    p.field_solver_subtraction_trick = float(config.field_solver_subtraction_trick)
+    p.field_solver_variant_A = int(bool(config.field_solver_variant_A))
+    p.precision = _precision(config)
+    return p
+
+
+def _key(p, device):
+    return tuple(getattr(p, f) for f, _ in p._fields_) + (device,)
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Solver:
+    """One liblc3d context: owns the device workspaces and copies of const
+    and virt_params for one configuration on one device."""
+
+    def __init__(self, params, device):
+        self.params = params
+        self.device = device
+        self.ctx = ctypes.c_void_p()
+        check(lib.lc3d_create(ctypes.byref(params), device, ctypes.byref(self.ctx)),
+              'lc3d_create')
+        nc, nf, rb = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(lib.lc3d_sizes(ctypes.byref(params), ctypes.byref(nc), ctypes.byref(nf),
+                             ctypes.byref(rb)), 'lc3d_sizes')
+        self.N, self.Nc, self.Nf, self.reflect_boundary = params.grid_steps, nc.value, nf.value, rb.value
+        self._const_key = None
+        self._virt_key = None
+        self._keep = ()
+
+    def __del__(self):
+        ctx = getattr(self, 'ctx', None)
+        if ctx and ctx.value and lib is not None:
+            lib.lc3d_destroy(ctx)
+            self.ctx = None
+
+    # -- constants ----------------------------------------------------------
+    def set_virt(self, virt):
+        key = tuple(getattr(virt, n).data_ptr() for n in _lib.VIRT_NAMES)
+        if key == self._virt_key:
+            return
+        ip = getattr(virt, 'indices_prev').to(torch.int32).contiguous()
+        inn = getattr(virt, 'indices_next').to(torch.int32).contiguous()
+        v = _lib.VirtPtrs(virt.influence_prev.data_ptr(), virt.influence_next.data_ptr(),
+                          ip.data_ptr(), inn.data_ptr(), virt.fine_grid.data_ptr())
+        check(lib.lc3d_set_const(self.ctx, None, ctypes.byref(v), _stream()), 'lc3d_set_const')
+        self._keep = (ip, inn)   # alive until the stream-ordered copy ran
+        torch.cuda.current_stream().synchronize()
+        self._virt_key = key
+
+    def set_const(self, const):
+        key = tuple(getattr(const, n).data_ptr() for n in _lib.CONST_NAMES)
+        if key == self._const_key:
+            return
+        c = _lib.ConstPtrs(*[getattr(const, n).data_ptr() for n in _lib.CONST_NAMES])
+        check(lib.lc3d_set_const(self.ctx, ctypes.byref(c), None, _stream()), 'lc3d_set_const')
+        self._const_key = key
+
+    def check_device_flag(self, where):
+        if check_errors:
+            check(lib.lc3d_check_error(self.ctx, _stream()), where)
+
+
+_solvers = {}
+
+
+def solver_for(config):
+    """The cached Solver of this configuration on the current device."""
+    p = params_of(config)
+    dev = _device().index
+    k = _key(p, dev)
+    s = _solvers.get(k)
+    if s is None:
+        s = _solvers[k] = Solver(p, dev)
+    return s
+
+
+def _grid(config):
+    N = config.grid_steps
+    return (N, N)
+
+
+def _zeros(shape):
+    return torch.zeros(shape, dtype=torch.float64, device=_device())
+
+
+def _empty(shape):
+    return torch.empty(shape, dtype=torch.float64, device=_device())
+
+
+def _f64(a, shape=None):
+    t = to_device(a, torch.float64)
+    if shape is not None and tuple(t.shape) != tuple(shape):
+        t = t.expand(shape).contiguous()
+    return t
+
+
+# ---------------------------------------------------------------------------
+# Field solvers (lcode.py:160-184, 246-290, 333-364)
+# ---------------------------------------------------------------------------
+
+def calculate_Ez(config, jx, jy):
+    """Ez from the Dirichlet Poisson problem (lcode.py:160-184)."""
+    s = solver_for(config)
+    jx, jy = _f64(jx), _f64(jy)
+    Ez = _empty(_grid(config))
+    check(lib.lc3d_calculate_Ez(s.ctx, _ptr(jx), _ptr(jy), _ptr(Ez), _stream()), 'calculate_Ez')
+    return Ez
+
+
+def calculate_Ex_Ey_Bx_By(config, Ex_avg, Ey_avg, Bx_avg, By_avg,
+                          beam_ro, ro, jx, jy, jz, jx_prev, jy_prev):
+    """Transverse fields from the Helmholtz (subtraction trick) or Laplace
+    problems with mixed boundary conditions (lcode.py:246-290)."""
+    s = solver_for(config)
+    g = _grid(config)
+    args = [_f64(a, g) for a in (Ex_avg, Ey_avg, Bx_avg, By_avg, beam_ro, ro, jx, jy, jz,
+                                 jx_prev, jy_prev)]
+    out = [_empty(g) for _ in range(4)]
+    check(lib.lc3d_calculate_Ex_Ey_Bx_By(s.ctx, *[_ptr(a) for a in args],
+                                         *[_ptr(o) for o in out], _stream()),
+          'calculate_Ex_Ey_Bx_By')
+    return tuple(out)
+
+
+def calculate_Bz(config, jx, jy):
+    """Bz from the Neumann Poisson problem, mean removed (lcode.py:333-364)."""
+    s = solver_for(config)
+    jx, jy = _f64(jx), _f64(jy)
+    Bz = _empty(_grid(config))
+    check(lib.lc3d_calculate_Bz(s.ctx, _ptr(jx), _ptr(jy), _ptr(Bz), _stream()), 'calculate_Bz')
+    return Bz
+
+
+# ---------------------------------------------------------------------------
+# Particles (lcode.py:369-391, 576-689, 692-699, 704-823)
+# ---------------------------------------------------------------------------
+
+def move_estimate_wo_fields(config, m, x_init, y_init, prev_x_offt, prev_y_offt, px, py, pz):
+    """Field-free drift with coordinate reflection (lcode.py:369-391)."""
+    s = solver_for(config)
+    shape = tuple(to_device(prev_x_offt).shape)
+    a = [_f64(v, shape) for v in (m, x_init, y_init, prev_x_offt, prev_y_offt, px, py, pz)]
+    ox, oy = _empty(shape), _empty(shape)
+    check(lib.lc3d_move_estimate_wo_fields(s.ctx, *[_ptr(v) for v in a], _ptr(ox), _ptr(oy),
+                                           _stream()), 'move_estimate_wo_fields')
+    return ox, oy
+
+
+def move_smart(config, m, q, x_init, y_init, x_prev_offt, y_prev_offt,
+               estimated_x_offt, estimated_y_offt, px_prev, py_prev, pz_prev,
+               Ex_avg, Ey_avg, Ez_avg, Bx_avg, By_avg, Bz_avg):
+    """Pusher with half-step TSC field interpolation (lcode.py:704-823)."""
+    s = solver_for(config)
+    shape = tuple(to_device(x_prev_offt).shape)
+    part = [_f64(v, shape) for v in (m, q, x_init, y_init, x_prev_offt, y_prev_offt,
+                                     estimated_x_offt, estimated_y_offt, px_prev, py_prev, pz_prev)]
+    g = _grid(config)
+    fields = [_f64(v, g) for v in (Ex_avg, Ey_avg, Ez_avg, Bx_avg, By_avg, Bz_avg)]
+    out = [_empty(shape) for _ in range(5)]
+    check(lib.lc3d_move_smart(s.ctx, *[_ptr(v) for v in part + fields],
+                              *[_ptr(o) for o in out], _stream()), 'move_smart')
+    s.check_device_flag('move_smart')
+    return tuple(out)
+
+
+def deposit(config, ro_initial, x_offt, y_offt, m, q, px, py, pz, virt_params):
+    """Coarse->fine interpolation and deterministic TSC deposition of rho,
+    jx, jy, jz, plus ro_initial (lcode.py:666-689)."""
+    s = solver_for(config)
+    s.set_virt(virt_params)
+    shape = tuple(to_device(x_offt).shape)
+    part = [_f64(v, shape) for v in (x_offt, y_offt, m, q, px, py, pz)]
+    g = _grid(config)
+    roi = None
+    if not (np.isscalar(ro_initial) and ro_initial == 0):
+        roi = _f64(ro_initial, g)
+    out = [_empty(g) for _ in range(4)]
+    check(lib.lc3d_deposit(s.ctx, _ptr(roi), *[_ptr(v) for v in part],
+                           *[_ptr(o) for o in out], _stream()), 'deposit')
+    s.check_device_flag('deposit')
+    return tuple(out)
+
+
+def initial_deposition(config, x_offt, y_offt, px, py, pz, m, q, virt_params):
+    """Ion background = minus the initial electron density (lcode.py:692-699)."""
+    ro_electrons_initial, _, _, _ = deposit(config, 0, x_offt, y_offt, m, q, px, py, pz,
+                                            virt_params)
+    return -ro_electrons_initial
+
+
+# ---------------------------------------------------------------------------
+# Plasma layout (lcode.py:454-573), host side: runs once per simulation
+# ---------------------------------------------------------------------------
+
+def make_coarse_plasma_grid(steps, step_size, coarseness=3):
+    """Coarse lattice, symmetric about 0 (lcode.py:454-465)."""
+    assert coarseness == int(coarseness)
+    half = np.arange(steps // (coarseness * 2)) * (step_size * coarseness)
+    grid = np.concatenate([-half[:0:-1], half])
+    assert np.array_equal(grid, -grid[::-1])
+    return grid
+
+
+def make_fine_plasma_grid(steps, step_size, fineness=2):
+    """Fine lattice avoiding cell edges (lcode.py:468-487)."""
+    assert fineness == int(fineness)
+    d = step_size / fineness
+    if fineness % 2:
+        half = np.arange(steps // 2 * fineness) * d
+        grid = np.concatenate([-half[:0:-1], half])
+    else:
+        half = (.5 + np.arange(steps // 2 * fineness)) * d
+        grid = np.concatenate([-half[::-1], half])
+    assert np.array_equal(grid, -grid[::-1])
+    return grid
+
+
+def make_plasma(steps, cell_size, coarseness=3, fineness=2):
+    """Coarse particles and the coarse->fine interpolation parameters
+    (lcode.py:490-573)."""
+    coarse = make_coarse_plasma_grid(steps, cell_size, coarseness)
+    fine = make_fine_plasma_grid(steps, cell_size, fineness)
+    Nc = len(coarse)
+    zeros = np.zeros((Nc, Nc))
+    x_init = np.broadcast_to(coarse[:, None], (Nc, Nc))
+    y_init = np.broadcast_to(coarse[None, :], (Nc, Nc))
+    m = np.full((Nc, Nc), float(ELECTRON_MASS * coarseness ** 2))
+    q = np.full((Nc, Nc), float(ELECTRON_CHARGE * coarseness ** 2))
+    pos = np.searchsorted(coarse, fine)
+    nxt = np.clip(pos, 0, Nc - 1)
+    prv = np.clip(pos - 1, 0, Nc - 1)
+    inf_prev = (coarse[nxt] - fine) / (cell_size * coarseness)
+    inf_next = (fine - coarse[prv]) / (cell_size * coarseness)
+    inf_prev[nxt == 0] = 0
+    inf_next[nxt == 0] = 1
+    inf_next[prv == Nc - 1] = 0
+    inf_prev[prv == Nc - 1] = 1
+    virt = GPUArrays(influence_prev=inf_prev, influence_next=inf_next,
+                     indices_prev=prv, indices_next=nxt, fine_grid=fine)
+    dev = [to_device(a) for a in (x_init, y_init, zeros, zeros, zeros, zeros, zeros, m, q)]
+    return (*dev, virt)
+
+
+# ---------------------------------------------------------------------------
+# The xi step and init (lcode.py:828-975)
+# ---------------------------------------------------------------------------
+
+def _beam(config, beam_ro):
+    if isinstance(beam_ro, (int, float)) and beam_ro == 0:
+        return None
+    return _f64(beam_ro, _grid(config))
+
+
+def step(config, const, virt_params, prev, beam_ro):
+    """One xi step: estimate, predictor, corrector, final move and deposit
+    (lcode.py:828-931). Returns a new GPUArrays; ``prev`` is not modified."""
+    s = solver_for(config)
+    s.set_virt(virt_params)
+    s.set_const(const)
+    beam = _beam(config, beam_ro)
+    shape_p = tuple(prev.x_offt.shape)
+    g = _grid(config)
+    prev_t = [_f64(getattr(prev, n), shape_p if k < 5 else g) for k, n in enumerate(_lib.STATE_NAMES)]
+    out = {n: _empty(shape_p if k < 5 else g) for k, n in enumerate(_lib.STATE_NAMES)}
+    sp = _lib.StatePtrs(*[t.data_ptr() for t in prev_t])
+    so = _lib.StatePtrs(*[out[n].data_ptr() for n in _lib.STATE_NAMES])
+    check(lib.lc3d_step_arrays(s.ctx, ctypes.byref(sp), ctypes.byref(so), _ptr(beam), _stream()),
+          'step')
+    s.check_device_flag('step')
+    new = GPUArrays.__new__(GPUArrays)
+    for n in _lib.STATE_NAMES:
+        setattr(new, n, out[n])
+    return new
+
+
+def init(config):
+    """Check the config, set config.reflect_boundary, lay out the plasma and
+    deposit the ion background (lcode.py:936-975)."""
+    assert config.grid_steps % 2 == 1
+    assert config.reflect_padding_steps > config.plasma_coarseness + 1
+    config.reflect_boundary = config.grid_step_size * (
+        config.grid_steps / 2 - config.reflect_padding_steps)
+    N = config.grid_steps
+    grid = (np.arange(N) - N // 2) * config.grid_step_size
+    xs, ys = grid[:, None], grid[None, :]
+    x_init, y_init, x_offt, y_offt, px, py, pz, m, q, virt_params = make_plasma(
+        N - config.plasma_padding_steps * 2, config.grid_step_size,
+        coarseness=config.plasma_coarseness, fineness=config.plasma_fineness)
+    ro_initial = initial_deposition(config, x_offt, y_offt, px, py, pz, m, q, virt_params)
+    const = GPUArrays(m=m, q=q, x_init=x_init, y_init=y_init, ro_initial=ro_initial)
+    z = lambda: _zeros((N, N))
+    state = GPUArrays(x_offt=x_offt, y_offt=y_offt, px=px, py=py, pz=pz,
+                      Ex=z(), Ey=z(), Ez=z(), Bx=z(), By=z(), Bz=z(),
+                      ro=z(), jx=z(), jy=z(), jz=z())
+    return xs, ys, const, virt_params, state
+
+
+# ---------------------------------------------------------------------------
+# CLI loop (lcode.py:1032-1051) with the on-axis Ez report of
+# lcode.py:992-1002, 1016-1026 (PNG slices and the zn figure are omitted)
+# ---------------------------------------------------------------------------
+
+def diags_peak_msg(Ez_00_history):
+    """Last on-axis Ez peak and its drift from the first peak
+    (lcode.py:992-1002)."""
+    a = np.asarray(Ez_00_history)
+    if a.size < 3:
+        return '...'
+    inner = a[1:-1]
+    peaks = np.nonzero((inner > a[:-2]) & (inner > a[2:]))[0] + 1
+    if not peaks.size:
+        return '...'
+    v = a[peaks]
+    dev = 100 * (v / v[0] - 1)
+    return f'{v[-1]:0.4e} {dev[-1]:+0.2f}%'
+
+
+def main():
+    import config
+    with torch.cuda.device(getattr(config, 'gpu_index', 0)):
+        xs, ys, const, virt_params, state = init(config)
+        Ez_00_history = []
+        N = config.grid_steps
+        for xi_i in range(config.xi_steps):
+            beam_ro = config.beam(xi_i, xs, ys)
+            state = step(config, const, virt_params, state, beam_ro)
+            ez = float(state.Ez[N // 2, N // 2])
+            Ez_00_history.append(ez)
+            if xi_i % config.diagnostics_each_N_steps == 0 or xi_i == config.xi_steps - 1:
+                xi = -xi_i * config.xi_step_size
+                print(f'xi={xi:+.4f} {ez:+.4e}|{diags_peak_msg(Ez_00_history)}')
+                sys.stdout.flush()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,244 @@
+"""Parity of the CUDA path (liblc3d.so through its C ABI) with the reference's
+golden vectors and with the CPU oracle. Tolerances are max|a-b| / max|b|
+per array; the float64 path is held to <= 1e-10 (the reference's own
+deposition is order-dependent at ~1e-12, its FFTs at ~1e-15)."""
+import ctypes
+import os
+import types
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip('torch')
+
+from conftest import GOLDEN  # noqa: E402
+from make_golden import beam_array, make_config  # noqa: E402
+from oracle import lcode_oracle as O  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+STATE = ('x_offt', 'y_offt', 'px', 'py', 'pz', 'Ex', 'Ey', 'Ez', 'Bx', 'By',
+         'Bz', 'ro', 'jx', 'jy', 'jz')
+TOL = 1e-10
+
+
+def rel(a, b):
+    if isinstance(a, torch.Tensor):
+        a = a.cpu().numpy()
+    return O.relative_error(a, b)
+
+
+@pytest.fixture(scope='module')
+def L():
+    if not torch.cuda.is_available():
+        pytest.skip('no GPU')
+    import lcode3d_b200 as L
+    L.lcode.check_errors = True
+    return L
+
+
+@pytest.fixture(scope='module')
+def stages(L):
+    g = np.load(os.path.join(GOLDEN, 'stages_n41.npz'))
+    cfg = make_config(41, 0.1, 0.05, 10, amplitude=0.3)
+    xs, ys, const, virt, _ = L.init(cfg)
+    prev = types.SimpleNamespace(**{k[5:]: torch.from_numpy(g[k]).cuda()
+                                    for k in g.files if k.startswith('prev_')})
+    return g, cfg, const, virt, prev
+
+
+def test_init(L, stages):
+    g, cfg, const, virt, _ = stages
+    assert cfg.reflect_boundary == float(g['reflect_boundary'])
+    for k in ('m', 'q', 'x_init', 'y_init'):
+        np.testing.assert_array_equal(getattr(const, k).cpu().numpy(), g['const_' + k])
+    assert rel(const.ro_initial, g['const_ro_initial']) < 1e-15
+    for k in ('influence_prev', 'influence_next', 'indices_prev', 'indices_next', 'fine_grid'):
+        np.testing.assert_array_equal(getattr(virt, k).cpu().numpy(), g['virt_' + k])
+
+
+def test_stage_functions(L, stages):
+    g, cfg, c, virt, P = stages
+    ex, ey = L.move_estimate_wo_fields(cfg, c.m, c.x_init, c.y_init, P.x_offt, P.y_offt,
+                                       P.px, P.py, P.pz)
+    assert rel(ex, g['est_x_offt']) < 1e-15 and rel(ey, g['est_y_offt']) < 1e-15
+    mv = L.move_smart(cfg, c.m, c.q, c.x_init, c.y_init, P.x_offt, P.y_offt, ex, ey,
+                      P.px, P.py, P.pz, P.Ex, P.Ey, P.Ez, P.Bx, P.By, P.Bz)
+    for k, v in zip(('x_offt', 'y_offt', 'px', 'py', 'pz'), mv):
+        assert rel(v, g['move_' + k]) < 1e-13, k
+    gm = [torch.from_numpy(g['move_' + k]).cuda() for k in ('x_offt', 'y_offt', 'px', 'py', 'pz')]
+    dep = L.deposit(cfg, c.ro_initial, gm[0], gm[1], c.m, c.q, gm[2], gm[3], gm[4], virt)
+    for k, v in zip(('ro', 'jx', 'jy', 'jz'), dep):
+        assert rel(v, g['dep_' + k]) < 1e-13, k
+    d = {k: torch.from_numpy(g['dep_' + k]).cuda() for k in ('ro', 'jx', 'jy', 'jz')}
+    beam = torch.from_numpy(g['beam_ro']).cuda()
+    F = L.calculate_Ex_Ey_Bx_By(cfg, P.Ex, P.Ey, P.Bx, P.By, beam, d['ro'], d['jx'], d['jy'],
+                                d['jz'], P.jx, P.jy)
+    for k, v in zip(('Ex', 'Ey', 'Bx', 'By'), F):
+        assert rel(v, g['fld_' + k]) < 1e-12, k
+    assert rel(L.calculate_Ez(cfg, d['jx'], d['jy']), g['fld_Ez']) < 1e-12
+    assert rel(L.calculate_Bz(cfg, d['jx'], d['jy']), g['fld_Bz']) < 1e-12
+    cfg0 = make_config(41, 0.1, 0.05, 10, amplitude=0.3)
+    cfg0.field_solver_subtraction_trick = 0
+    L.init(cfg0)
+    F0 = L.calculate_Ex_Ey_Bx_By(cfg0, P.Ex, P.Ey, P.Bx, P.By, beam, d['ro'], d['jx'], d['jy'],
+                                 d['jz'], P.jx, P.jy)
+    for k, v in zip(('Ex', 'Ey', 'Bx', 'By'), F0):
+        assert rel(v, g['fld0_' + k]) < 1e-12, k
+
+
+@pytest.mark.parametrize('variant_A', [True, False])
+def test_step_stages_fixture(L, stages, variant_A):
+    g, _, c, virt, P = stages
+    cfg = make_config(41, 0.1, 0.05, 10, amplitude=0.3)
+    cfg.field_solver_variant_A = variant_A
+    L.init(cfg)
+    new = L.step(cfg, c, virt, P, torch.from_numpy(g['beam_ro']).cuda())
+    pre = 'step_' if variant_A else 'stepB_'
+    for k in STATE:
+        assert rel(getattr(new, k), g[pre + k]) < 1e-12, k
+
+
+def test_run_n161_300_steps(L):
+    """161^2, h=0.05, dxi=0.05, A=0.05: all 300 steps through the drop-in
+    step(); the on-axis Ez history and the final state against the
+    reference."""
+    g = np.load(os.path.join(GOLDEN, 'run_n161.npz'))
+    cfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    xs, ys, const, virt, st = L.init(cfg)
+    ez = []
+    for i in range(300):
+        st = L.step(cfg, const, virt, st, beam_array(cfg, i, xs, ys))
+        ez.append(float(st.Ez[80, 80]))
+        if i + 1 in (1, 100):
+            for k in ('Ex', 'Ey', 'Ez', 'Bz', 'ro', 'jz'):
+                assert rel(getattr(st, k), g[f's{i + 1}_{k}']) < TOL, (i, k)
+    assert rel(np.array(ez), g['Ez00']) < TOL
+    for k in ('Ex', 'Ey', 'Ez', 'Bz', 'ro', 'jz', 'x_offt', 'y_offt', 'px', 'py', 'pz'):
+        assert rel(getattr(st, k), g['final_' + k]) < TOL, k
+
+
+def test_run_n641_head(L):
+    """641^2, h=0.025, dxi=0.005, A=0.5 (the production grid): the first 30
+    steps against the reference's axis/diagonal rows and sums."""
+    g = np.load(os.path.join(GOLDEN, 'run_n641_head.npz'))
+    cfg = make_config(641, 0.025, 0.005, 3000, amplitude=0.5)
+    xs, ys, const, virt, st = L.init(cfg)
+    assert abs(float(const.ro_initial.sum()) - float(g['ro_initial_sum'])) < 1e-8
+    steps = int(g['steps'])
+    ez = []
+    for i in range(steps):
+        st = L.step(cfg, const, virt, st, beam_array(cfg, i, xs, ys))
+        ez.append(float(st.Ez[320, 320]))
+    assert rel(np.array(ez), g['Ez00']) < TOL
+    for k in STATE[5:]:
+        a = getattr(st, k).cpu().numpy()
+        scale = float(g['maxabs_' + k])
+        assert np.abs(a[320] - g['axis_' + k]).max() <= TOL * scale, k
+        assert np.abs(np.diagonal(a) - g['diag_' + k]).max() <= TOL * scale, k
+
+
+def _displaced_state(cfg, const, rng, amp):
+    """A strongly displaced plasma (offsets of several cells, random
+    momenta), kept inside the reflect boundary, to exercise the deposit
+    paths for particles outside a CTA's shared-memory window."""
+    x0 = const.x_init.cpu().numpy()
+    y0 = const.y_init.cpu().numpy()
+    rb = cfg.reflect_boundary * 0.97
+    x = np.clip(x0 + rng.normal(0, amp, x0.shape), -rb, rb)
+    y = np.clip(y0 + rng.normal(0, amp, y0.shape), -rb, rb)
+    p = [rng.normal(0, 0.3, x0.shape) for _ in range(3)]
+    return x - x0, y - y0, p
+
+
+def test_deposit_displaced_vs_oracle(L):
+    cfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    xs, ys, const, virt, st = L.init(cfg)
+    ocfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    oxs, oys, oconst, ovirt, ost = O.init(ocfg)
+    rng = np.random.default_rng(7)
+    for amp in (0.02, 0.3, 1.5):
+        xo, yo, (px, py, pz) = _displaced_state(cfg, const, rng, amp)
+        t = [torch.from_numpy(a).cuda() for a in (xo, yo, px, py, pz)]
+        dep = L.deposit(cfg, const.ro_initial, t[0], t[1], const.m, const.q, t[2], t[3], t[4], virt)
+        exp = O.deposit(ocfg, oconst.ro_initial, xo, yo, oconst.m, oconst.q, px, py, pz, ovirt)
+        for k, a, b in zip(('ro', 'jx', 'jy', 'jz'), dep, exp):
+            assert rel(a, b) < 1e-13, (amp, k)
+
+
+def test_move_smart_vs_oracle(L):
+    cfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    xs, ys, const, virt, st = L.init(cfg)
+    ocfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    _, _, oc, _, _ = O.init(ocfg)
+    rng = np.random.default_rng(11)
+    xo, yo, (px, py, pz) = _displaced_state(cfg, const, rng, 0.5)
+    ex = xo + rng.normal(0, 0.01, xo.shape)
+    ey = yo + rng.normal(0, 0.01, yo.shape)
+    N = 161
+    F = [rng.normal(0, 0.1, (N, N)) for _ in range(6)]
+    args = (xo, yo, ex, ey, px, py, pz, *F)
+    t = [torch.from_numpy(a).cuda() for a in args]
+    got = L.move_smart(cfg, const.m, const.q, const.x_init, const.y_init, *t)
+    exp = O.move_smart(ocfg, oc.m, oc.q, oc.x_init, oc.y_init, *args)
+    for k, a, b in zip(('x_offt', 'y_offt', 'px', 'py', 'pz'), got, exp):
+        assert rel(a, b) < 1e-13, k
+
+
+def test_deposit_deterministic(L):
+    """Bit-identical deposition on repeated calls (the reference's float64
+    atomics are order-dependent)."""
+    cfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    xs, ys, const, virt, st = L.init(cfg)
+    rng = np.random.default_rng(5)
+    xo, yo, (px, py, pz) = _displaced_state(cfg, const, rng, 0.8)
+    t = [torch.from_numpy(a).cuda() for a in (xo, yo, px, py, pz)]
+    a = L.deposit(cfg, const.ro_initial, t[0], t[1], const.m, const.q, t[2], t[3], t[4], virt)
+    for _ in range(3):
+        b = L.deposit(cfg, const.ro_initial, t[0], t[1], const.m, const.q, t[2], t[3], t[4], virt)
+        for x, y in zip(a, b):
+            assert torch.equal(x, y)
+
+
+def test_step_deterministic_and_ctx_state(L):
+    """step() twice from the same prev is bit-identical, and the
+    context-owned state path (lc3d_set_state / lc3d_step / lc3d_get_state)
+    gives the same arrays as lc3d_step_arrays."""
+    from lcode3d_b200 import _lib
+    cfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    xs, ys, const, virt, st = L.init(cfg)
+    for i in range(60):
+        st = L.step(cfg, const, virt, st, beam_array(cfg, i, xs, ys))
+    beam = torch.from_numpy(beam_array(cfg, 60, xs, ys)).cuda()
+    a = L.step(cfg, const, virt, st, beam)
+    b = L.step(cfg, const, virt, st, beam)
+    for k in STATE:
+        assert torch.equal(getattr(a, k), getattr(b, k)), k
+    s = L.solver_for(cfg)
+    lib = _lib.lib
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    sp = _lib.StatePtrs(*[getattr(st, k).data_ptr() for k in STATE])
+    _lib.check(lib.lc3d_set_state(s.ctx, ctypes.byref(sp), stream), 'set_state')
+    _lib.check(lib.lc3d_step(s.ctx, ctypes.c_void_p(beam.data_ptr()), stream), 'step')
+    out = {k: torch.empty_like(getattr(st, k)) for k in STATE}
+    so = _lib.StatePtrs(*[out[k].data_ptr() for k in STATE])
+    _lib.check(lib.lc3d_get_state(s.ctx, ctypes.byref(so), stream), 'get_state')
+    torch.cuda.synchronize()
+    for k in STATE:
+        assert torch.equal(out[k], getattr(a, k)), k
+
+
+def test_out_of_window_particle_is_flagged(L):
+    """A particle pushed beyond the grid is not written out of bounds: the
+    kernel's own bounds check skips it and raises the error flag, which
+    step() reports; the context stays usable."""
+    from lcode3d_b200._lib import LC3DError, ERR_WINDOW
+    cfg = make_config(41, 0.1, 0.05, 10, amplitude=0.3)
+    xs, ys, const, virt, st = L.init(cfg)
+    bad = L.GPUArrays(**{k: getattr(st, k).clone() for k in STATE})
+    bad.x_offt[0, 0] = -100.0   # far outside the 41-cell grid
+    with pytest.raises(LC3DError) as e:
+        L.step(cfg, const, virt, bad, 0)
+    assert e.value.code == ERR_WINDOW
+    new = L.step(cfg, const, virt, st, 0)
+    assert torch.isfinite(new.ro).all()
