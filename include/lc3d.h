@@ -49,6 +49,11 @@ extern "C" {
 #define LC3D_PREC_FP64 0        /* float64 dense-transform (DGEMM-form) solvers */
 #define LC3D_PREC_MIXED 1       /* split-BF16 tcgen05 transforms, fp32 accumulate */
 
+/* Float64 transform method (lc3d_params.fp64_transform). */
+#define LC3D_FP64_AUTO 0        /* FFT when 2(N-1) factors into 2, 3, 5, 7; else dense */
+#define LC3D_FP64_FFT 1         /* shared-memory FFT DST-I / DCT-I */
+#define LC3D_FP64_DENSE 2       /* dense transform matrices (DGEMM form) */
+
 /* Mirrors the reference config module attributes (config_example.py:1-30). */
 typedef struct lc3d_params {
     int grid_steps;                       /* odd (lcode.py:941) */
@@ -61,6 +66,7 @@ typedef struct lc3d_params {
     double field_solver_subtraction_trick; /* multiplies the *_avg terms (lcode.py:264-268) */
     int field_solver_variant_A;
     int precision;                        /* LC3D_PREC_* */
+    int fp64_transform;                   /* LC3D_FP64_* */
 } lc3d_params;
 
 /* The xi-step state, attribute names of lcode.py:926-929. */

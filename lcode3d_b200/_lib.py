@@ -13,6 +13,7 @@ c_int, c_double, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
 OK, ERR_PARAM, ERR_CUDA, ERR_WINDOW, ERR_NONFINITE, ERR_STATE, ERR_SIZE = range(7)
 PREC_FP64, PREC_MIXED = 0, 1
+FP64_AUTO, FP64_FFT, FP64_DENSE = 0, 1, 2
 
 
 class Params(ctypes.Structure):
@@ -25,7 +26,8 @@ class Params(ctypes.Structure):
                 ('plasma_padding_steps', c_int),
                 ('field_solver_subtraction_trick', c_double),
                 ('field_solver_variant_A', c_int),
-                ('precision', c_int)]
+                ('precision', c_int),
+                ('fp64_transform', c_int)]
 
 
 STATE_NAMES = ('x_offt', 'y_offt', 'px', 'py', 'pz', 'Ex', 'Ey', 'Ez',
@@ -62,7 +64,7 @@ SIGNATURES = [
     ('lc3d_step_arrays', c_int, [P, ctypes.POINTER(StatePtrs), ctypes.POINTER(StatePtrs), P, P]),
     ('lc3d_move_estimate_wo_fields', c_int, [P] * 12),
     ('lc3d_move_smart', c_int, [P] * 24),
-    ('lc3d_deposit', c_int, [P] * 15),
+    ('lc3d_deposit', c_int, [P] * 14),
     ('lc3d_calculate_Ex_Ey_Bx_By', c_int, [P] * 17),
     ('lc3d_calculate_Ez', c_int, [P] * 5),
     ('lc3d_calculate_Bz', c_int, [P] * 5),

@@ -361,6 +361,7 @@ struct FieldGeom {
     size_t off;            // offset of X / output inside an N x N plane
     const double *L, *R, *Lam;
     int ldL, ldR, ldLam;
+    int type0, type1;      // axis-0 / axis-1 transform: 0 DCT-I, 1 DST-I
 };
 
 FieldGeom geom(const lc3d_ctx* c, int f) {
@@ -368,16 +369,16 @@ FieldGeom geom(const lc3d_ctx* c, int f) {
     FieldGeom g;
     switch (f) {
         case 0: case 4:   // Ex, By: solved transposed
-            g = {N, M, 1, c->C, c->S2, c->lam_mixT, N, M, M};
+            g = {N, M, 1, c->C, c->S2, c->lam_mixT, N, M, M, 0, 1};
             break;
         case 1: case 3:   // Ey, Bx
-            g = {M, N, (size_t)N, c->S2, c->CT, c->lam_mix, M, N, N};
+            g = {M, N, (size_t)N, c->S2, c->CT, c->lam_mix, M, N, N, 1, 0};
             break;
         case 2:           // Ez
-            g = {M, M, (size_t)N + 1, c->S2, c->S2, c->lam_dir, M, M, M};
+            g = {M, M, (size_t)N + 1, c->S2, c->S2, c->lam_dir, M, M, M, 1, 1};
             break;
         default:          // Bz
-            g = {N, N, 0, c->C, c->CT, c->lam_neu, N, N, N};
+            g = {N, N, 0, c->C, c->CT, c->lam_neu, N, N, N, 0, 0};
             break;
     }
     return g;
@@ -419,43 +420,67 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
             dst[f] = c->raw[f];
         }
     }
-    // the four GEMM stages
-    for (int stage = 0; stage < 4; ++stage) {
-        GemmBatch b;
-        memset(&b, 0, sizeof(b));
-        for (int f = 0; f < 6; ++f) {
-            if (!on[f]) continue;
-            const FieldGeom g = geom(c, f);
-            GemmProb& p = b.p[b.count++];
-            switch (stage) {
-                case 0:   // t1 = X R
-                    p.A = c->rhs[f] + g.off; p.lda = N;
-                    p.B = g.R; p.ldb = g.ldR;
-                    p.C = c->t1[f]; p.ldc = N;
-                    p.M = g.rows; p.N = g.cols; p.K = g.cols;
-                    break;
-                case 1:   // t2 = Lambda o (L t1)
-                    p.A = g.L; p.lda = g.ldL;
-                    p.B = c->t1[f]; p.ldb = N;
-                    p.C = c->t2[f]; p.ldc = N;
-                    p.L = g.Lam; p.ldl = g.ldLam;
-                    p.M = g.rows; p.N = g.cols; p.K = g.rows;
-                    break;
-                case 2:   // t1 = t2 R
-                    p.A = c->t2[f]; p.lda = N;
-                    p.B = g.R; p.ldb = g.ldR;
-                    p.C = c->t1[f]; p.ldc = N;
-                    p.M = g.rows; p.N = g.cols; p.K = g.cols;
-                    break;
-                default:  // out = L t1
-                    p.A = g.L; p.lda = g.ldL;
-                    p.B = c->t1[f]; p.ldb = N;
-                    p.C = dst[f] + g.off; p.ldc = N;
-                    p.M = g.rows; p.N = g.cols; p.K = g.rows;
-                    break;
+    if (c->use_fft) {
+        // four FFT row passes, each writing its output transposed
+        for (int stage = 0; stage < 4; ++stage) {
+            FftRowsDesc d[6];
+            int cnt = 0;
+            for (int f = 0; f < 6; ++f) {
+                if (!on[f]) continue;
+                const FieldGeom g = geom(c, f);
+                FftRowsDesc& e = d[cnt++];
+                memset(&e, 0, sizeof(e));
+                e.ld_in = N;
+                e.ld_out = N;
+                switch (stage) {
+                    case 0: e.in = c->rhs[f] + g.off; e.rows = g.rows; e.type = g.type1; e.out = c->t1[f]; break;
+                    case 1: e.in = c->t1[f]; e.rows = g.cols; e.type = g.type0; e.out = c->t2[f];
+                            e.lam = g.Lam; e.ld_lam = g.ldLam; break;
+                    case 2: e.in = c->t2[f]; e.rows = g.rows; e.type = g.type1; e.out = c->t1[f]; break;
+                    default: e.in = c->t1[f]; e.rows = g.cols; e.type = g.type0; e.out = dst[f] + g.off; break;
+                }
             }
+            LC3D_TRY(fft_rows(c, d, cnt, s));
         }
-        LC3D_TRY(launch_gemm(c, b, s));
+    } else {
+        // the four GEMM stages
+        for (int stage = 0; stage < 4; ++stage) {
+            GemmBatch b;
+            memset(&b, 0, sizeof(b));
+            for (int f = 0; f < 6; ++f) {
+                if (!on[f]) continue;
+                const FieldGeom g = geom(c, f);
+                GemmProb& p = b.p[b.count++];
+                switch (stage) {
+                    case 0:   // t1 = X R
+                        p.A = c->rhs[f] + g.off; p.lda = N;
+                        p.B = g.R; p.ldb = g.ldR;
+                        p.C = c->t1[f]; p.ldc = N;
+                        p.M = g.rows; p.N = g.cols; p.K = g.cols;
+                        break;
+                    case 1:   // t2 = Lambda o (L t1)
+                        p.A = g.L; p.lda = g.ldL;
+                        p.B = c->t1[f]; p.ldb = N;
+                        p.C = c->t2[f]; p.ldc = N;
+                        p.L = g.Lam; p.ldl = g.ldLam;
+                        p.M = g.rows; p.N = g.cols; p.K = g.rows;
+                        break;
+                    case 2:   // t1 = t2 R
+                        p.A = c->t2[f]; p.lda = N;
+                        p.B = g.R; p.ldb = g.ldR;
+                        p.C = c->t1[f]; p.ldc = N;
+                        p.M = g.rows; p.N = g.cols; p.K = g.cols;
+                        break;
+                    default:  // out = L t1
+                        p.A = g.L; p.lda = g.ldL;
+                        p.B = c->t1[f]; p.ldb = N;
+                        p.C = dst[f] + g.off; p.ldc = N;
+                        p.M = g.rows; p.N = g.cols; p.K = g.rows;
+                        break;
+                }
+            }
+            LC3D_TRY(launch_gemm(c, b, s));
+        }
     }
     const double inv_n = 1.0 / n;
     if (on[5]) {

@@ -1,0 +1,257 @@
+// Float64 DST-I / DCT-I row transforms through a shared-memory FFT.
+//
+// The reference realises its transforms with padded real FFTs
+// (lcode.py:124-141 dst2d, 190-212 mix2d, 295-313 dct2d). Here every 1-D
+// transform is one length-P complex FFT, P = 2 (N - 1), of the symmetric
+// (DCT-I) or antisymmetric (DST-I) extension of a row, with TWO rows packed
+// as real and imaginary parts:
+//     DCT-I: Z = Y_a + i Y_b, Y real         -> X_a = Re Z[k],  X_b = Im Z[k]
+//     DST-I: Z = -i X_a + X_b (Y imaginary)   -> X_a = -Im Z[k+1], X_b = Re Z[k+1]
+// (unnormalised, the conventions of scipy's dct/dst type 1, so DST-I = S2 x
+// and DCT-I = C x of the dense-transform form). The FFT is a Stockham
+// autosort FFT with mixed radices 4, 2, 3, 5, 7, ping-ponging between two
+// shared-memory buffers. Every launch transforms rows and writes its output
+// TRANSPOSED (out[k][r]), optionally scaled by Lambda[k][r]; the 2-D solve
+// F = L (Lambda o (L X R)) R is then four such passes:
+//     A: rows of X by the axis-1 transform          -> T1^T
+//     B: rows of T1^T by the axis-0 transform, x Lambda -> Z
+//     C: rows of Z by the axis-1 transform          -> T3^T
+//     D: rows of T3^T by the axis-0 transform       -> F
+// One launch covers all fields of a solve.
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lc3d_internal.cuh"
+
+namespace {
+
+constexpr int FFT_THREADS = 256;
+constexpr int FFT_PER_CTA = 2;           // complex FFTs per CTA (4 rows)
+constexpr int ROWS_PER_CTA = 2 * FFT_PER_CTA;
+constexpr int MAX_RADICES = 24;
+
+struct FftField {
+    const double* in;
+    int ld_in, rows, type;               // type: 0 DCT-I (n = N), 1 DST-I (n = N - 2)
+    double* out;
+    int ld_out;
+    const double* lam;
+    int ld_lam;
+    int cta_start;
+};
+
+struct FftBatch {
+    FftField f[6];
+    int count, P, N;
+    int nrad;
+    int rad[MAX_RADICES];
+    const double2* tw;                   // tw[m] = exp(-2 pi i m / P)
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+
+// Small DFTs in registers, forward sign.
+template <int R>
+__device__ __forceinline__ void dft(double2 (&v)[R], const double2* __restrict__ tw, int P) {
+    double2 o[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+        double2 s = v[0];
+#pragma unroll
+        for (int r = 1; r < R; ++r) s = cadd(s, cmul(v[r], __ldg(tw + ((r * m) % R) * (P / R))));
+        o[m] = s;
+    }
+#pragma unroll
+    for (int m = 0; m < R; ++m) v[m] = o[m];
+}
+
+template <>
+__device__ __forceinline__ void dft<2>(double2 (&v)[2], const double2*, int) {
+    const double2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+}
+
+template <>
+__device__ __forceinline__ void dft<4>(double2 (&v)[4], const double2*, int) {
+    const double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    const double2 a2 = cadd(v[1], v[3]), d = csub(v[1], v[3]);
+    const double2 a3 = make_double2(d.y, -d.x);   // -i (v1 - v3)
+    v[0] = cadd(a0, a2);
+    v[2] = csub(a0, a2);
+    v[1] = cadd(a1, a3);
+    v[3] = csub(a1, a3);
+}
+
+// One Stockham butterfly: inputs a[j + r P/R], twiddled by
+// exp(-2 pi i r k / (Ns R)), outputs b[(j / Ns) Ns R + k + r Ns].
+template <int R>
+__device__ __forceinline__ void butterfly(const double2* a, double2* b, int j, int Ns, int P,
+                                          const double2* __restrict__ tw) {
+    const int k = j % Ns, stride = P / R, tstep = P / (Ns * R);
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = a[j + r * stride];
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(tw + r * k * tstep));
+    dft<R>(v, tw, P);
+    const int d = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) b[d + r * Ns] = v[r];
+}
+
+template <int R>
+__device__ __forceinline__ void fft_pass(const double2* A, double2* B, int Ns, int P, const double2* tw) {
+    const int nb = P / R;
+    for (int t = threadIdx.x; t < FFT_PER_CTA * nb; t += FFT_THREADS) {
+        const int q = t / nb, j = t - q * nb;
+        butterfly<R>(A + q * P, B + q * P, j, Ns, P, tw);
+    }
+}
+
+__global__ void __launch_bounds__(FFT_THREADS) fft_rows_kernel(const __grid_constant__ FftBatch b) {
+    extern __shared__ double2 sm[];      // [2 buffers][FFT_PER_CTA][P]
+    int fi = 0;
+#pragma unroll 1
+    for (int q = 1; q < b.count; ++q)
+        if ((int)blockIdx.x >= b.f[q].cta_start) fi = q;
+    const FftField& F = b.f[fi];
+    const int P = b.P, L = P / 2;
+    const int r0 = ((int)blockIdx.x - F.cta_start) * ROWS_PER_CTA;
+    const int n = F.type ? b.N - 2 : b.N;     // input / output length
+    double2* A = sm;
+    double2* B = sm + FFT_PER_CTA * P;
+
+    // symmetric / antisymmetric extensions, two rows per complex FFT
+    for (int t = threadIdx.x; t < FFT_PER_CTA * P; t += FFT_THREADS) {
+        const int q = t / P, m = t - q * P;
+        double v[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int row = r0 + 2 * q + h;
+            double x = 0;
+            if (row < F.rows) {
+                const double* rp = F.in + (size_t)row * F.ld_in;
+                if (F.type == 0) {
+                    x = rp[m <= L ? m : P - m];
+                } else if (m != 0 && m != L) {
+                    x = m < L ? rp[m - 1] : -rp[P - m - 1];
+                }
+            }
+            v[h] = x;
+        }
+        A[t] = make_double2(v[0], v[1]);
+    }
+    __syncthreads();
+    int Ns = 1;
+    for (int p = 0; p < b.nrad; ++p) {
+        const int R = b.rad[p];
+        switch (R) {
+            case 4: fft_pass<4>(A, B, Ns, P, b.tw); break;
+            case 2: fft_pass<2>(A, B, Ns, P, b.tw); break;
+            case 3: fft_pass<3>(A, B, Ns, P, b.tw); break;
+            case 5: fft_pass<5>(A, B, Ns, P, b.tw); break;
+            default: fft_pass<7>(A, B, Ns, P, b.tw); break;
+        }
+        __syncthreads();
+        double2* t = A;
+        A = B;
+        B = t;
+        Ns *= R;
+    }
+    // transposed output, 4 consecutive rows per output index k
+    const int off = F.type;   // DST-I outputs are Z[1 .. L-1]
+    for (int t = threadIdx.x; t < n * ROWS_PER_CTA; t += FFT_THREADS) {
+        const int k = t / ROWS_PER_CTA, rr = t - k * ROWS_PER_CTA;
+        const int row = r0 + rr;
+        if (row >= F.rows) continue;
+        const double2 z = A[(rr >> 1) * P + k + off];
+        double x;
+        if (F.type == 0)
+            x = (rr & 1) ? z.y : z.x;
+        else
+            x = (rr & 1) ? z.x : -z.y;
+        if (F.lam) x *= F.lam[(size_t)k * F.ld_lam + row];
+        F.out[(size_t)k * F.ld_out + row] = x;
+    }
+}
+
+double sin_pi_frac(long long r, long long L) {
+    r %= 2 * L;
+    if (r < 0) r += 2 * L;
+    double sign = 1;
+    if (r >= L) { r -= L; sign = -1; }
+    if (2 * r > L) r = L - r;
+    return sign * std::sin(M_PI * (double)r / (double)L);
+}
+
+}  // namespace
+
+// Radix plan for a length-P FFT: factors 4, 2, 3, 5, 7 (largest powers of 4
+// first). Returns the number of passes, or 0 if P has another prime factor.
+int fft_plan(int P, int* rad) {
+    int n = 0;
+    int r = P;
+    while (r % 4 == 0 && n < MAX_RADICES) { rad[n++] = 4; r /= 4; }
+    const int others[] = {2, 3, 5, 7};
+    for (int f : others)
+        while (r % f == 0 && n < MAX_RADICES) { rad[n++] = f; r /= f; }
+    return (r == 1) ? n : 0;
+}
+
+size_t fft_smem_bytes(int P) { return (size_t)2 * FFT_PER_CTA * P * sizeof(double2); }
+
+int fft_init(lc3d_ctx* c) {
+    const int P = 2 * (c->N - 1);
+    int rad[MAX_RADICES];
+    c->fft_ok = fft_plan(P, rad) > 0 && fft_smem_bytes(P) <= 200 * 1024;
+    if (!c->fft_ok) return LC3D_OK;
+    LC3D_TRY(fft_prepare(P));
+    std::vector<double> tw(2 * (size_t)P);
+    for (int m = 0; m < P; ++m) {
+        // exp(-2 pi i m / P) = cos(2 pi m / P) - i sin(2 pi m / P)
+        tw[2 * m] = sin_pi_frac(4LL * m + P, 2LL * P);      // cos(pi (2m) / P)
+        tw[2 * m + 1] = -sin_pi_frac(2LL * m, (long long)P);
+    }
+    LC3D_CUDA_TRY(cudaMalloc(&c->fft_tw, tw.size() * sizeof(double)));
+    LC3D_CUDA_TRY(cudaMemcpy(c->fft_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return LC3D_OK;
+}
+
+int fft_prepare(int P) {
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)fft_smem_bytes(P)));
+    return LC3D_OK;
+}
+
+// One transform pass over up to 6 fields: desc[f] = {in, ld_in, rows, type,
+// out, ld_out, lam, ld_lam}; rows of `in` are transformed and written
+// transposed into `out`.
+int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, cudaStream_t s) {
+    FftBatch b;
+    memset(&b, 0, sizeof(b));
+    b.P = 2 * (c->N - 1);
+    b.N = c->N;
+    b.nrad = fft_plan(b.P, b.rad);
+    b.tw = reinterpret_cast<const double2*>(c->fft_tw);
+    int ctas = 0;
+    for (int q = 0; q < count; ++q) {
+        FftField& f = b.f[b.count++];
+        f.in = desc[q].in; f.ld_in = desc[q].ld_in; f.rows = desc[q].rows; f.type = desc[q].type;
+        f.out = desc[q].out; f.ld_out = desc[q].ld_out; f.lam = desc[q].lam; f.ld_lam = desc[q].ld_lam;
+        f.cta_start = ctas;
+        ctas += (f.rows + ROWS_PER_CTA - 1) / ROWS_PER_CTA;
+    }
+    if (!ctas) return LC3D_OK;
+    const size_t smem = fft_smem_bytes(b.P);
+    ProfScope ps(c, LC3D_STAGE_TRANSFORM, s);
+    fft_rows_kernel<<<ctas, FFT_THREADS, smem, s>>>(b);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}

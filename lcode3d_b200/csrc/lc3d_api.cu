@@ -58,6 +58,7 @@ int check_params(const lc3d_params* p, int* Nc, int* Nf, double* rb) {
     if (c < 1 || f < 1) return LC3D_ERR_PARAM;
     if (!(p->reflect_padding_steps > c + 1)) return LC3D_ERR_PARAM;       // lcode.py:944
     if (p->precision != LC3D_PREC_FP64 && p->precision != LC3D_PREC_MIXED) return LC3D_ERR_PARAM;
+    if (p->fp64_transform < LC3D_FP64_AUTO || p->fp64_transform > LC3D_FP64_DENSE) return LC3D_ERR_PARAM;
     const int steps = N - 2 * p->plasma_padding_steps;                   // lcode.py:956
     if (steps < 2) return LC3D_ERR_PARAM;
     const int R = steps / (2 * c);                                        // lcode.py:461
@@ -233,6 +234,7 @@ void destroy(lc3d_ctx* c) {
     if (c->acc) cudaFree(c->acc);
     if (c->err) cudaFree(c->err);
     if (c->zeros) cudaFree(c->zeros);
+    if (c->fft_tw) cudaFree(c->fft_tw);
     if (c->prof_ev) {
         for (int k = 0; k < 2 * c->prof_cap; ++k) cudaEventDestroy(c->prof_ev[k]);
         free(c->prof_ev);
@@ -310,7 +312,13 @@ int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out) {
     LC3D_STEP(dalloc(&c->acc, ng * 8));
     LC3D_STEP(dalloc(&c->err, (size_t)1));
     LC3D_STEP(dalloc(&c->zeros, ng));
+    LC3D_STEP(particles_prepare());
     LC3D_STEP(fields_init(c));
+    LC3D_STEP(fft_init(c));
+    if (rc == LC3D_OK) {
+        if (p->fp64_transform == LC3D_FP64_FFT && !c->fft_ok) rc = LC3D_ERR_PARAM;
+        c->use_fft = c->fft_ok && p->fp64_transform != LC3D_FP64_DENSE;
+    }
 #undef LC3D_STEP
     if (rc == LC3D_OK && cudaDeviceSynchronize() != cudaSuccess) rc = LC3D_ERR_CUDA;
     if (rc != LC3D_OK) {

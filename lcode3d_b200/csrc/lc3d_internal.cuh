@@ -118,6 +118,24 @@ struct SolveOutputs {
 
 int solve_fields(lc3d_ctx* ctx, int which, const SolveInputs& in,
                  const SolveOutputs& o, cudaStream_t s);
+
+// FFT row transforms (fields_fft.cu): rows of `in` (length N for DCT-I,
+// N - 2 for DST-I) are transformed and written transposed, out[k][r],
+// optionally multiplied by lam[k][r].
+struct FftRowsDesc {
+    const double* in;
+    int ld_in, rows, type;                // type: 0 DCT-I, 1 DST-I
+    double* out;
+    int ld_out;
+    const double* lam;
+    int ld_lam;
+};
+int fft_init(lc3d_ctx* ctx);
+int fft_rows(lc3d_ctx* ctx, const FftRowsDesc* desc, int count, cudaStream_t s);
+int fft_plan(int P, int* rad);
+// one-time per-device kernel attributes (shared-memory opt-ins)
+int particles_prepare();
+int fft_prepare(int P);
 int fields_init(lc3d_ctx* ctx);           // transform matrices, workspaces
 void fields_free(lc3d_ctx* ctx);
 
@@ -154,6 +172,8 @@ struct lc3d_ctx {
     double* raw[6];                       // raw solver output, zero border
     double* red;                          // Bz mean partial sums
     int red_blocks;
+    int fft_ok, use_fft;                  // FFT transforms available / selected
+    double* fft_tw;                       // FFT twiddles, P complex
     void* mixed;                          // mixed-precision solver state (fields_mixed.cu)
     // launch accounting / profiling
     long long launches[LC3D_NSTAGES];

@@ -31,22 +31,33 @@ struct Tsc {
     double wxM, wx0, wxP, wyM, wy0, wyP;
 };
 
-__device__ __forceinline__ Tsc tsc_weights(double x, double y, int N, double h) {
-    Tsc t;
+// Centre cell (i, j) and offset from the cell centre, lcode.py:404-406.
+__device__ __forceinline__ void tsc_cell(double x, double y, int N, double h, int& i, int& j, double& xl,
+                                         double& yl) {
     double x_h = x / h + .5, y_h = y / h + .5;
     double fx = floor(x_h), fy = floor(y_h);
+    xl = x_h - fx - .5;
+    yl = y_h - fy - .5;
     // out-of-range positions map to an invalid index without UB in the cast
     fx = fmin(fmax(fx, -1.0e6), 1.0e6);
     fy = fmin(fmax(fy, -1.0e6), 1.0e6);
-    t.i = (int)fx + N / 2;
-    t.j = (int)fy + N / 2;
-    double xl = x_h - fx - .5, yl = y_h - fy - .5;
-    t.wx0 = .75 - xl * xl;
-    t.wy0 = .75 - yl * yl;
-    t.wxP = (.5 + xl) * (.5 + xl) / 2;
-    t.wyP = (.5 + yl) * (.5 + yl) / 2;
-    t.wxM = (.5 - xl) * (.5 - xl) / 2;
-    t.wyM = (.5 - yl) * (.5 - yl) / 2;
+    i = (int)fx + N / 2;
+    j = (int)fy + N / 2;
+}
+
+// Quadratic-spline weights along one axis, lcode.py:410-412.
+__device__ __forceinline__ void tsc_axis(double l, double& wM, double& w0, double& wP) {
+    w0 = .75 - l * l;
+    wP = (.5 + l) * (.5 + l) / 2;
+    wM = (.5 - l) * (.5 - l) / 2;
+}
+
+__device__ __forceinline__ Tsc tsc_weights(double x, double y, int N, double h) {
+    Tsc t;
+    double xl, yl;
+    tsc_cell(x, y, N, h, t.i, t.j, xl, yl);
+    tsc_axis(xl, t.wxM, t.wx0, t.wxP);
+    tsc_axis(yl, t.wyM, t.wy0, t.wyP);
     return t;
 }
 
@@ -186,9 +197,12 @@ __device__ __forceinline__ double fx_value(long long hi, long long lo) {
            (double)lo * 0x1p-76;
 }
 
-constexpr int DEP_T = 16;      // fine particles per CTA side
-constexpr int DEP_W = 24;      // shared window side (cells)
-constexpr int DEP_WORDS = 8;   // 4 fields x (hi, lo)
+constexpr int DEP_B = 16;                 // threads per CTA side
+constexpr int DEP_T = 2 * DEP_B;          // fine particles per CTA side (2 x 2 per thread)
+constexpr int DEP_W = 32;                 // shared window side (cells)
+constexpr int DEP_WIN = DEP_W * DEP_W;
+constexpr int DEP_WORDS = 8;              // 4 fields x (hi, lo), one plane each
+constexpr size_t DEP_SMEM = (size_t)DEP_WORDS * DEP_WIN * sizeof(unsigned long long);
 
 // One fine particle: coarse->fine mix (lcode.py:591-621) and the deposit
 // quantities (lcode.py:651-655).
@@ -221,101 +235,189 @@ __device__ __forceinline__ FineParticle fine_particle(const DepositArgs& a, int 
     return p;
 }
 
-__global__ void __launch_bounds__(256) deposit_kernel(DepositArgs a) {
-    __shared__ unsigned long long win[DEP_W * DEP_W * DEP_WORDS];
-    __shared__ int s_imin, s_imax, s_jmin, s_jmax;
+// What the deposition keeps of a fine particle: centre cell, offsets from
+// the cell centre, and the four deposited values.
+struct Dep {
+    int i, j;
+    double xl, yl;
+    double v[4];
+};
 
-    const int tid = threadIdx.y * DEP_T + threadIdx.x;
-    const int fi = blockIdx.y * DEP_T + threadIdx.y;
-    const int fj = blockIdx.x * DEP_T + threadIdx.x;
-    const bool in_lattice = fi < a.Nf && fj < a.Nf;
+__device__ __forceinline__ double pick4(const double (&v)[4], int f) {
+    return f == 0 ? v[0] : f == 1 ? v[1] : f == 2 ? v[2] : v[3];
+}
+
+__device__ __forceinline__ void fx_add(unsigned long long* hi_plane, unsigned long long* lo_plane, size_t cell,
+                                       double c) {
+    long long hi, lo;
+    fx_split(c, hi, lo);
+    atomicAdd(hi_plane + cell, (unsigned long long)hi);
+    atomicAdd(lo_plane + cell, (unsigned long long)lo);
+}
+
+// Deposition of a 32 x 32 patch of the fine lattice by 16 x 16 threads.
+// Each thread owns a 2 x 2 block of fine particles (initially one cell).
+// When the block's centre cells span at most 2 x 2 cells -- the common case,
+// neighbouring fine particles are interpolated from the same coarse
+// particles and move together -- the thread sums its particles' TSC
+// stencils in a fixed order into a 4 x 4 float64 register patch per field
+// and adds the patch through the exact fixed-point split into the CTA's
+// shared window: 4x fewer integer atomics than per-particle scatter, and no
+// two lanes of a warp hit the same cell. Otherwise each particle is added
+// on its own, into the window or (outside it) straight into the global
+// accumulators. All additions are integer, so the result is independent
+// of the order.
+__global__ void __launch_bounds__(256, 1) deposit_kernel(DepositArgs a) {
+    extern __shared__ unsigned long long win[];   // [DEP_WORDS][DEP_WIN]
+    __shared__ int s_bb[4];                        // imin imax jmin jmax
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DEP_B + tx;
     const int N = a.N;
-
+    const size_t NN = (size_t)N * N;
     if (tid == 0) {
-        s_imin = s_jmin = 1 << 30;
-        s_imax = s_jmax = -(1 << 30);
+        s_bb[0] = s_bb[2] = 1 << 30;
+        s_bb[1] = s_bb[3] = -(1 << 30);
     }
-    for (int w = tid; w < DEP_W * DEP_W * DEP_WORDS; w += 256) win[w] = 0ull;
+    for (int w = tid; w < DEP_WORDS * DEP_WIN; w += 256) win[w] = 0ull;
 
-    FineParticle p;
-    Tsc t;
-    bool valid = false;
-    if (in_lattice) {
-        p = fine_particle(a, fi, fj);
-        t = tsc_weights(p.x, p.y, N, a.h);
-        valid = tsc_in_grid(t, N);
-        if (!valid) atomicOr(a.err, LC3D_FLAG_WINDOW);
-        const double vmax = fmax(fmax(fabs(p.dro), fabs(p.djx)), fmax(fabs(p.djy), fabs(p.djz)));
-        if (valid && !(vmax < FX_MAX)) {   // also catches NaN
-            atomicOr(a.err, LC3D_FLAG_NONFINITE);
-            valid = false;
+    Dep P[4];
+    bool ok[4];
+    int imin = 1 << 30, imax = -(1 << 30), jmin = 1 << 30, jmax = -(1 << 30);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int fi = blockIdx.y * DEP_T + 2 * ty + (p >> 1);
+        const int fj = blockIdx.x * DEP_T + 2 * tx + (p & 1);
+        ok[p] = false;
+        if (fi < a.Nf && fj < a.Nf) {
+            const FineParticle f = fine_particle(a, fi, fj);
+            tsc_cell(f.x, f.y, N, a.h, P[p].i, P[p].j, P[p].xl, P[p].yl);
+            P[p].v[0] = f.dro;
+            P[p].v[1] = f.djx;
+            P[p].v[2] = f.djy;
+            P[p].v[3] = f.djz;
+            const double vmax = fmax(fmax(fabs(f.dro), fabs(f.djx)), fmax(fabs(f.djy), fabs(f.djz)));
+            const bool in_grid = P[p].i >= 1 && P[p].i <= N - 2 && P[p].j >= 1 && P[p].j <= N - 2;
+            if (!in_grid) {
+                atomicOr(a.err, LC3D_FLAG_WINDOW);
+            } else if (!(vmax < FX_MAX)) {   // also catches NaN
+                atomicOr(a.err, LC3D_FLAG_NONFINITE);
+            } else {
+                ok[p] = true;
+                imin = min(imin, P[p].i);
+                imax = max(imax, P[p].i);
+                jmin = min(jmin, P[p].j);
+                jmax = max(jmax, P[p].j);
+            }
         }
     }
-    __syncthreads();
-    if (valid) {
-        atomicMin(&s_imin, t.i);
-        atomicMax(&s_imax, t.i);
-        atomicMin(&s_jmin, t.j);
-        atomicMax(&s_jmax, t.j);
+    const int ti0 = imin, ti1 = imax, tj0 = jmin, tj1 = jmax;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        imin = min(imin, __shfl_xor_sync(0xffffffffu, imin, o));
+        imax = max(imax, __shfl_xor_sync(0xffffffffu, imax, o));
+        jmin = min(jmin, __shfl_xor_sync(0xffffffffu, jmin, o));
+        jmax = max(jmax, __shfl_xor_sync(0xffffffffu, jmax, o));
     }
     __syncthreads();
-    const int oi = s_imin - 1, oj = s_jmin - 1;   // window origin (cells)
-    if (valid) {
-        const double wx[3] = {t.wxM, t.wx0, t.wxP};
-        const double wy[3] = {t.wyM, t.wy0, t.wyP};
-        const double val[4] = {p.dro, p.djx, p.djy, p.djz};
-        const int li = t.i - oi, lj = t.j - oj;   // stencil centre in the window
-        const bool inside = li + 1 < DEP_W && lj + 1 < DEP_W;
+    if ((tid & 31) == 0 && imin <= imax) {
+        atomicMin(&s_bb[0], imin);
+        atomicMax(&s_bb[1], imax);
+        atomicMin(&s_bb[2], jmin);
+        atomicMax(&s_bb[3], jmax);
+    }
+    __syncthreads();
+    const int oi = s_bb[0] - 1, oj = s_bb[2] - 1;   // window origin (cells)
+
+    const bool patch = ti0 <= ti1 && ti1 - ti0 <= 1 && tj1 - tj0 <= 1 && ti0 + 2 - oi < DEP_W &&
+                       tj0 + 2 - oj < DEP_W;
+    if (patch) {
+        const int r0 = ti0 - 1 - oi, c0 = tj0 - 1 - oj;
+#pragma unroll 1
+        for (int f = 0; f < 4; ++f) {
+            double acc[16];
 #pragma unroll
-        for (int di = 0; di < 3; ++di) {
+            for (int k = 0; k < 16; ++k) acc[k] = 0.0;
 #pragma unroll
-            for (int dj = 0; dj < 3; ++dj) {
-                const double w = wx[di] * wy[dj];
+            for (int p = 0; p < 4; ++p) {
+                if (!ok[p]) continue;
+                double wxM, wx0, wxP, wyM, wy0, wyP;
+                tsc_axis(P[p].xl, wxM, wx0, wxP);
+                tsc_axis(P[p].yl, wyM, wy0, wyP);
+                const bool si = P[p].i != ti0, sj = P[p].j != tj0;
+                const double wx4[4] = {si ? 0.0 : wxM, si ? wxM : wx0, si ? wx0 : wxP, si ? wxP : 0.0};
+                const double wy4[4] = {sj ? 0.0 : wyM, sj ? wyM : wy0, sj ? wy0 : wyP, sj ? wyP : 0.0};
+                const double v = pick4(P[p].v, f);
 #pragma unroll
-                for (int f = 0; f < 4; ++f) {
-                    long long hi, lo;
-                    fx_split(val[f] * w, hi, lo);
-                    if (inside) {
-                        unsigned long long* c =
-                            &win[((li + di - 1) * DEP_W + (lj + dj - 1)) * DEP_WORDS + 2 * f];
-                        atomicAdd(c, (unsigned long long)hi);
-                        atomicAdd(c + 1, (unsigned long long)lo);
-                    } else {
-                        unsigned long long* c =
-                            a.acc + ((size_t)(t.i + di - 1) * N + (t.j + dj - 1)) * DEP_WORDS + 2 * f;
-                        atomicAdd(c, (unsigned long long)hi);
-                        atomicAdd(c + 1, (unsigned long long)lo);
+                for (int r = 0; r < 4; ++r)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) acc[r * 4 + c] += v * (wx4[r] * wy4[c]);
+            }
+            unsigned long long* hp = win + (2 * f) * DEP_WIN;
+            unsigned long long* lp = hp + DEP_WIN;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    if (acc[r * 4 + c] != 0.0) fx_add(hp, lp, (r0 + r) * DEP_W + (c0 + c), acc[r * 4 + c]);
+        }
+    } else {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (!ok[p]) continue;
+            double wx[3], wy[3];
+            tsc_axis(P[p].xl, wx[0], wx[1], wx[2]);
+            tsc_axis(P[p].yl, wy[0], wy[1], wy[2]);
+            const int li = P[p].i - oi, lj = P[p].j - oj;
+            const bool inside = li + 1 < DEP_W && lj + 1 < DEP_W;
+#pragma unroll 1
+            for (int f = 0; f < 4; ++f) {
+                const double v = pick4(P[p].v, f);
+#pragma unroll
+                for (int di = 0; di < 3; ++di)
+#pragma unroll
+                    for (int dj = 0; dj < 3; ++dj) {
+                        const double c = v * (wx[di] * wy[dj]);
+                        if (inside)
+                            fx_add(win + (2 * f) * DEP_WIN, win + (2 * f + 1) * DEP_WIN,
+                                   (li + di - 1) * DEP_W + (lj + dj - 1), c);
+                        else
+                            fx_add(a.acc + (2 * f) * NN, a.acc + (2 * f + 1) * NN,
+                                   (size_t)(P[p].i + di - 1) * N + (P[p].j + dj - 1), c);
                     }
-                }
             }
         }
     }
     __syncthreads();
     // flush the touched part of the window
-    const int ni = min(s_imax + 2 - oi, DEP_W), nj = min(s_jmax + 2 - oj, DEP_W);
-    if (s_imin <= s_imax) {
-        const int rowlen = nj * DEP_WORDS;
-        for (int w = tid; w < ni * rowlen; w += 256) {
-            const int r = w / rowlen, c = w - r * rowlen;
-            const unsigned long long v = win[r * DEP_W * DEP_WORDS + c];
-            if (v) atomicAdd(a.acc + ((size_t)(oi + r) * N + oj) * DEP_WORDS + c, v);
+    if (s_bb[0] <= s_bb[1]) {
+        const int ni = min(s_bb[1] + 2 - oi, DEP_W), nj = min(s_bb[3] + 2 - oj, DEP_W);
+        const int plane = ni * nj;
+        for (int w = tid; w < DEP_WORDS * plane; w += 256) {
+            const int word = w / plane, rem = w - word * plane;
+            const int r = rem / nj, c = rem - r * nj;
+            const unsigned long long v = win[word * DEP_WIN + r * DEP_W + c];
+            if (v) atomicAdd(a.acc + word * NN + (size_t)(oi + r) * N + (oj + c), v);
         }
     }
 }
 
 __global__ void __launch_bounds__(256) deposit_finalize_kernel(DepositFinalizeArgs f) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= f.n) return;
-    ulonglong2* w = reinterpret_cast<ulonglong2*>(f.acc + (size_t)k * DEP_WORDS);
-    ulonglong2 a0 = w[0], a1 = w[1], a2 = w[2], a3 = w[3];
-    const ulonglong2 z = make_ulonglong2(0ull, 0ull);
-    w[0] = z; w[1] = z; w[2] = z; w[3] = z;
-    double ro = fx_value((long long)a0.x, (long long)a0.y);
-    if (f.ro_initial) ro += f.ro_initial[k];
-    f.ro[k] = ro;
-    f.jx[k] = fx_value((long long)a1.x, (long long)a1.y);
-    f.jy[k] = fx_value((long long)a2.x, (long long)a2.y);
-    f.jz[k] = fx_value((long long)a3.x, (long long)a3.y);
+    const size_t NN = (size_t)f.n;
+    unsigned long long* acc = f.acc;
+    double out[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const unsigned long long hi = acc[(2 * q) * NN + k], lo = acc[(2 * q + 1) * NN + k];
+        acc[(2 * q) * NN + k] = 0ull;
+        acc[(2 * q + 1) * NN + k] = 0ull;
+        out[q] = fx_value((long long)hi, (long long)lo);
+    }
+    if (f.ro_initial) out[0] += f.ro_initial[k];
+    f.ro[k] = out[0];
+    f.jx[k] = out[1];
+    f.jy[k] = out[2];
+    f.jz[k] = out[3];
 }
 
 }  // namespace
@@ -334,10 +436,15 @@ int launch_move_smart(const MoveArgs& a, cudaStream_t s) {
     return LC3D_OK;
 }
 
+int particles_prepare() {
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DEP_SMEM));
+    return LC3D_OK;
+}
+
 int launch_deposit_main(const DepositArgs& a, cudaStream_t s) {
     if (a.Nf <= 0) return LC3D_OK;
     dim3 grid((a.Nf + DEP_T - 1) / DEP_T, (a.Nf + DEP_T - 1) / DEP_T);
-    deposit_kernel<<<grid, dim3(DEP_T, DEP_T), 0, s>>>(a);
+    deposit_kernel<<<grid, dim3(DEP_B, DEP_B), DEP_SMEM, s>>>(a);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }

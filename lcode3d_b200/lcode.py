@@ -15,7 +15,9 @@ attribute access like the reference's. All device work runs in liblc3d.so
 (include/lc3d.h) on the current torch stream; there is no CPU fallback.
 
 Extra, optional config attributes (absent in the reference's config):
-``lc3d_precision`` = 'fp64' (default) or 'mixed'.
+``lc3d_precision`` = 'fp64' (default) or 'mixed';
+``lc3d_fp64_transform`` = 'auto' (default: FFT where 2(N-1) factors into
+2, 3, 5, 7), 'fft' or 'dense' (DGEMM-form transform matrices).
 """
 import ctypes
 import math
@@ -103,6 +105,14 @@ def _precision(config):
     raise ValueError(f'lc3d_precision must be "fp64" or "mixed", not {p!r}')
 
 
+def _fp64_transform(config):
+    t = getattr(config, 'lc3d_fp64_transform', 'auto')
+    table = {'auto': _lib.FP64_AUTO, 'fft': _lib.FP64_FFT, 'dense': _lib.FP64_DENSE}
+    if t not in table:
+        raise ValueError(f'lc3d_fp64_transform must be one of {sorted(table)}, not {t!r}')
+    return table[t]
+
+
 def params_of(config):
     p = _lib.Params()
     p.grid_steps = int(config.grid_steps)
@@ -115,6 +125,7 @@ def params_of(config):
     p.field_solver_subtraction_trick = float(config.field_solver_subtraction_trick)
     p.field_solver_variant_A = int(bool(config.field_solver_variant_A))
     p.precision = _precision(config)
+    p.fp64_transform = _fp64_transform(config)
     return p
 
 

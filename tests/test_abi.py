@@ -58,6 +58,7 @@ def _params(N=161, h=0.05, c=3, f=2, rpad=5, ppad=10):
     p.plasma_coarseness, p.plasma_fineness = c, f
     p.reflect_padding_steps, p.plasma_padding_steps = rpad, ppad
     p.field_solver_subtraction_trick, p.field_solver_variant_A, p.precision = 1.0, 1, 0
+    p.fp64_transform = 0
     return p
 
 
@@ -122,3 +123,36 @@ def test_python_interface_needs_gpu():
     from make_golden import make_config
     with pytest.raises(RuntimeError, match='CUDA'):
         L.init(make_config(41, 0.1, 0.05, 10, amplitude=0.3))
+
+
+def declared_arity():
+    """{function: number of parameters} from the prototypes in include/*.h."""
+    out = {}
+    for h in HEADERS:
+        src = re.sub(r'/\*.*?\*/', '', open(h).read(), flags=re.S)
+        for m in re.finditer(r'\b(lc3d_\w+)\s*\(([^;{]*?)\)\s*;', src):
+            args = m.group(2).strip()
+            out[m.group(1)] = 0 if args in ('', 'void') else args.count(',') + 1
+    return out
+
+
+def test_binding_arity_matches_header():
+    """Every ctypes binding declares as many arguments as the C prototype."""
+    from lcode3d_b200 import _lib
+    ar = declared_arity()
+    for name, _, argtypes in _lib.SIGNATURES:
+        assert ar[name] == len(argtypes), (name, ar[name], len(argtypes))
+
+
+def test_oracle_binding_arity():
+    """The oracle's ctypes declarations match its C prototypes."""
+    src = open(os.path.join(ROOT, 'oracle', 'lc3d_oracle.c')).read()
+    from oracle import lcode_oracle as O
+    O.use_c_kernels(1)
+    try:
+        for name in ('oracle_move_smart', 'oracle_deposit'):
+            m = re.search(r'\bint ' + name + r'\(([^{]*?)\)\s*\{', src, flags=re.S)
+            n = m.group(1).count(',') + 1
+            assert len(getattr(O._C, name).argtypes) == n, name
+    finally:
+        O.use_numpy_kernels()

@@ -87,6 +87,52 @@ def test_stage_functions(L, stages):
         assert rel(v, g['fld0_' + k]) < 1e-12, k
 
 
+@pytest.mark.parametrize('transform', ['dense', 'fft'])
+def test_stage_field_solvers_both_transforms(L, stages, transform):
+    """Both float64 transform methods (dense DGEMM form and shared-memory
+    FFT) against the reference's field solvers."""
+    g, _, c, virt, P = stages
+    cfg = make_config(41, 0.1, 0.05, 10, amplitude=0.3)
+    cfg.lc3d_fp64_transform = transform
+    L.init(cfg)
+    d = {k: torch.from_numpy(g['dep_' + k]).cuda() for k in ('ro', 'jx', 'jy', 'jz')}
+    beam = torch.from_numpy(g['beam_ro']).cuda()
+    F = L.calculate_Ex_Ey_Bx_By(cfg, P.Ex, P.Ey, P.Bx, P.By, beam, d['ro'], d['jx'], d['jy'],
+                                d['jz'], P.jx, P.jy)
+    for k, v in zip(('Ex', 'Ey', 'Bx', 'By'), F):
+        assert rel(v, g['fld_' + k]) < 1e-12, k
+    assert rel(L.calculate_Ez(cfg, d['jx'], d['jy']), g['fld_Ez']) < 1e-12
+    assert rel(L.calculate_Bz(cfg, d['jx'], d['jy']), g['fld_Bz']) < 1e-12
+    new = L.step(cfg, c, virt, P, beam)
+    for k in STATE:
+        assert rel(getattr(new, k), g['step_' + k]) < 1e-12, k
+
+
+@pytest.mark.parametrize('N', [161, 321, 481, 641])
+def test_fft_vs_dense_vs_oracle(L, N):
+    """The FFT and dense transforms agree with each other and with the
+    oracle's scipy.fft solvers on random right-hand sides, at every grid
+    size of the batched scan (161, 321, 481, 641)."""
+    rng = np.random.default_rng(N)
+    h = 16 / (N - 1)
+    ins = [rng.normal(size=(N, N)) for _ in range(11)]
+    ins_t = [torch.from_numpy(a).cuda() for a in ins]
+    res = {}
+    for t in ('fft', 'dense'):
+        cfg = make_config(N, h, 0.01, 10, amplitude=0.1)
+        cfg.lc3d_fp64_transform = t
+        F = L.calculate_Ex_Ey_Bx_By(cfg, *ins_t)
+        Ez = L.calculate_Ez(cfg, ins_t[6], ins_t[7])
+        Bz = L.calculate_Bz(cfg, ins_t[6], ins_t[7])
+        res[t] = [x.cpu().numpy() for x in (*F, Ez, Bz)]
+    ocfg = make_config(N, h, 0.01, 10, amplitude=0.1)
+    exp = list(O.calculate_Ex_Ey_Bx_By(ocfg, *ins)) + [O.calculate_Ez(ocfg, ins[6], ins[7]),
+                                                       O.calculate_Bz(ocfg, ins[6], ins[7])]
+    for k, name in enumerate(('Ex', 'Ey', 'Bx', 'By', 'Ez', 'Bz')):
+        assert rel(res['fft'][k], res['dense'][k]) < 1e-12, name
+        assert rel(res['fft'][k], exp[k]) < 1e-12, name
+
+
 @pytest.mark.parametrize('variant_A', [True, False])
 def test_step_stages_fixture(L, stages, variant_A):
     g, _, c, virt, P = stages
@@ -131,9 +177,15 @@ def test_run_n641_head(L):
         st = L.step(cfg, const, virt, st, beam_array(cfg, i, xs, ys))
         ez.append(float(st.Ez[320, 320]))
     assert rel(np.array(ez), g['Ez00']) < TOL
+    # ro is the small difference of the electron density and the ion
+    # background (both ~1 per cell early in the run), so its rounding noise
+    # is measured against the background density
+    ro_scale = float(const.ro_initial.abs().max())
     for k in STATE[5:]:
         a = getattr(st, k).cpu().numpy()
         scale = float(g['maxabs_' + k])
+        if k == 'ro':
+            scale = max(scale, ro_scale)
         assert np.abs(a[320] - g['axis_' + k]).max() <= TOL * scale, k
         assert np.abs(np.diagonal(a) - g['diag_' + k]).max() <= TOL * scale, k
 
