@@ -174,6 +174,16 @@ def transform_flops_per_launch(N):
     return sum(4 * r * c * (r + c) for r, c in dims) / 4
 
 
+def fft_bytes_per_launch(N):
+    """Algorithmic bytes of one FFT row pass over the 6 fields of a solve:
+    every field's r x c array is read once and written once (8 bytes per
+    element); one of the 4 passes also reads the eigenvalue matrix, counted
+    as a quarter per launch."""
+    M = N - 2
+    dims = [(N, M), (M, N), (M, M), (M, N), (N, M), (N, N)]
+    return sum(8 * r * c * (2 + 0.25) for r, c in dims)
+
+
 def deposit_bytes_per_launch(N, Nc, Nf):
     """Algorithmic bytes of one deposition (kernel + finalize): read the 7
     coarse arrays and the 5 fine-lattice arrays, read ro_initial, write
@@ -189,6 +199,7 @@ def run_ours(args, rank, world, dist):
     dev = int(os.environ.get('LOCAL_RANK', 0))
     torch.cuda.set_device(dev)
     cfg = make_config(args.grid, args.precision)
+    cfg.lc3d_fp64_transform = args.fp64_transform
     N = cfg.grid_steps
     xs, ys, const, virt, st = L.init(cfg)
     s = L.solver_for(cfg)
@@ -282,7 +293,16 @@ def run_ours(args, rank, world, dist):
     dom = max(stage, key=lambda n: stage[n]['ms'])
     hbm, hbm_src = peaks()
     roof = None
-    if dom == 'transform' and stage[dom]['timed']:
+    use_fft = args.fp64_transform != 'dense'
+    if dom == 'transform' and stage[dom]['timed'] and use_fft:
+        avg_ms = stage[dom]['ms'] / stage[dom]['timed']
+        by = fft_bytes_per_launch(N)
+        ach = by / (avg_ms * 1e-3) / 1e9
+        roof = {'kernel': 'fft_rows_kernel (FP64 DST/DCT row-FFT pass, 6 fields)', 'bound': 'hbm',
+                'achieved': ach, 'peak': hbm, 'unit': 'GB/s', 'frac': ach / hbm,
+                'peak_source': hbm_src, 'algorithmic_per_launch': by, 'avg_launch_ms': avg_ms,
+                'traffic': None}
+    elif dom == 'transform' and stage[dom]['timed']:
         avg_ms = stage[dom]['ms'] / stage[dom]['timed']
         fl = transform_flops_per_launch(N)
         ach = fl / (avg_ms * 1e-3) / 1e12
@@ -313,7 +333,8 @@ def run_ours(args, rank, world, dist):
                                f'xi_step={cfg.xi_step_size}, coarseness 3 / fineness 2, A={GRIDS[N][2]}, '
                                f'{args.precision} field solvers',
                    'grid_steps': N, 'coarse_particles': s.Nc ** 2, 'fine_particles': s.Nf ** 2,
-                   'precision': args.precision, 'start_xi_step': x0,
+                   'precision': args.precision, 'fp64_transform': args.fp64_transform,
+                   'start_xi_step': x0,
                    'l2': 'flushed between timed steps (256 MiB write, outside the step events)',
                    'parallelism': f'replicas x{world}' if world > 1 else 'single GPU'},
         'e2e': {'value': world * K / (e2e_ms * 1e-3), 'unit': 'xi-steps/s',
@@ -384,6 +405,7 @@ def main():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--precision', default='fp64', choices=['fp64', 'mixed'])
+    ap.add_argument('--fp64-transform', default='auto', choices=['auto', 'fft', 'dense'])
     ap.add_argument('--grid', type=int, default=641, choices=sorted(GRIDS))
     ap.add_argument('--pre', type=int, default=400, help='untimed steps into the beam')
     ap.add_argument('--cpu-steps', type=int, default=16, help='oracle steps for cpu_baseline')

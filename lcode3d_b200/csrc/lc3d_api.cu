@@ -135,11 +135,13 @@ int deposit_into(lc3d_ctx* c, const double* ro_initial, const double* x, const d
     a.inf_prev = c->inf_prev; a.inf_next = c->inf_next; a.fine_grid = c->fine_grid;
     a.idx_prev = c->idx_prev; a.idx_next = c->idx_next;
     a.acc = c->acc;
+    a.plane = c->acc_plane;
     a.Nc = c->Nc; a.Nf = c->Nf; a.N = c->N;
     a.h = c->p.grid_step_size; a.sf = c->sf;
     a.err = c->err;
     DepositFinalizeArgs f;
     f.acc = c->acc;
+    f.plane = c->acc_plane;
     f.ro_initial = ro_initial;
     f.ro = ro; f.jx = jx; f.jy = jy; f.jz = jz;
     f.n = c->N * c->N;
@@ -309,7 +311,8 @@ int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out) {
         for (int k = 0; k < 5; ++k) LC3D_STEP(dalloc(&c->pw[a][k], np));
     for (int k = 0; k < 4; ++k) LC3D_STEP(dalloc(&c->dens[k], ng));
     for (int k = 0; k < 6; ++k) LC3D_STEP(dalloc(&c->avg[k], ng));
-    LC3D_STEP(dalloc(&c->acc, ng * 8));
+    c->acc_plane = (ng + 31) / 32 * 32;
+    LC3D_STEP(dalloc(&c->acc, c->acc_plane * 8));
     LC3D_STEP(dalloc(&c->err, (size_t)1));
     LC3D_STEP(dalloc(&c->zeros, ng));
     LC3D_STEP(particles_prepare());

@@ -56,7 +56,8 @@ struct DepositArgs {
     const double *x_offt, *y_offt, *m, *q, *px, *py, *pz;   // coarse, Nc x Nc
     const double *inf_prev, *inf_next, *fine_grid;            // Nf
     const int32_t *idx_prev, *idx_next;                       // Nf
-    unsigned long long* acc;                                  // N*N*8 fixed-point words
+    unsigned long long* acc;                                  // 8 planes of fixed-point words
+    size_t plane;                                             // plane stride (>= N*N, 256-byte multiple)
     int Nc, Nf, N;
     double h, sf;
     unsigned* err;
@@ -64,6 +65,7 @@ struct DepositArgs {
 
 struct DepositFinalizeArgs {
     unsigned long long* acc;
+    size_t plane;
     const double* ro_initial;             // may be NULL
     double *ro, *jx, *jy, *jz;
     int n;                                // N*N
@@ -160,7 +162,8 @@ struct lc3d_ctx {
     double* pw[2][5];                     // predictor / corrector particles
     double* dens[4];                      // ro jx jy jz of predictor / corrector
     double* avg[6];                       // half-step averaged fields
-    unsigned long long* acc;              // deposit fixed-point accumulators
+    unsigned long long* acc;              // deposit fixed-point accumulators, 8 planes
+    size_t acc_plane;                     // plane stride in words
     unsigned* err;                        // device error flag
     double* zeros;                        // N x N zeros (absent beam)
     // field-solver workspaces (fields.cu)

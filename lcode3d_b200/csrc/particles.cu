@@ -197,12 +197,14 @@ __device__ __forceinline__ double fx_value(long long hi, long long lo) {
            (double)lo * 0x1p-76;
 }
 
-constexpr int DEP_B = 16;                 // threads per CTA side
-constexpr int DEP_T = 2 * DEP_B;          // fine particles per CTA side (2 x 2 per thread)
+constexpr int DEP_T = 32;                 // fine particles per CTA side
+constexpr int DEP_THREADS = DEP_T * DEP_T; // phase 1: one fine particle per thread
 constexpr int DEP_W = 32;                 // shared window side (cells)
 constexpr int DEP_WIN = DEP_W * DEP_W;
 constexpr int DEP_WORDS = 8;              // 4 fields x (hi, lo), one plane each
-constexpr size_t DEP_SMEM = (size_t)DEP_WORDS * DEP_WIN * sizeof(unsigned long long);
+// shared memory: window planes + per-particle staging (cell, xl, yl, 4 values)
+constexpr size_t DEP_SMEM = (size_t)DEP_WORDS * DEP_WIN * sizeof(unsigned long long) +
+                            (size_t)DEP_THREADS * (6 * sizeof(double) + sizeof(int));
 
 // One fine particle: coarse->fine mix (lcode.py:591-621) and the deposit
 // quantities (lcode.py:651-655).
@@ -235,18 +237,6 @@ __device__ __forceinline__ FineParticle fine_particle(const DepositArgs& a, int 
     return p;
 }
 
-// What the deposition keeps of a fine particle: centre cell, offsets from
-// the cell centre, and the four deposited values.
-struct Dep {
-    int i, j;
-    double xl, yl;
-    double v[4];
-};
-
-__device__ __forceinline__ double pick4(const double (&v)[4], int f) {
-    return f == 0 ? v[0] : f == 1 ? v[1] : f == 2 ? v[2] : v[3];
-}
-
 __device__ __forceinline__ void fx_add(unsigned long long* hi_plane, unsigned long long* lo_plane, size_t cell,
                                        double c) {
     long long hi, lo;
@@ -255,84 +245,109 @@ __device__ __forceinline__ void fx_add(unsigned long long* hi_plane, unsigned lo
     atomicAdd(lo_plane + cell, (unsigned long long)lo);
 }
 
-// Deposition of a 32 x 32 patch of the fine lattice by 16 x 16 threads.
-// Each thread owns a 2 x 2 block of fine particles (initially one cell).
-// When the block's centre cells span at most 2 x 2 cells -- the common case,
-// neighbouring fine particles are interpolated from the same coarse
-// particles and move together -- the thread sums its particles' TSC
-// stencils in a fixed order into a 4 x 4 float64 register patch per field
-// and adds the patch through the exact fixed-point split into the CTA's
-// shared window: 4x fewer integer atomics than per-particle scatter, and no
-// two lanes of a warp hit the same cell. Otherwise each particle is added
-// on its own, into the window or (outside it) straight into the global
-// accumulators. All additions are integer, so the result is independent
-// of the order.
-__global__ void __launch_bounds__(256, 1) deposit_kernel(DepositArgs a) {
-    extern __shared__ unsigned long long win[];   // [DEP_WORDS][DEP_WIN]
-    __shared__ int s_bb[4];                        // imin imax jmin jmax
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DEP_B + tx;
+// Deposition of a 32 x 32 patch of the fine lattice by one CTA of 1024
+// threads, in three phases.
+//  1. One thread per fine particle: coarse->fine interpolation, deposit
+//     values and TSC cell, staged in shared memory; CTA bounding box of the
+//     particles' cells (the window is placed on it).
+//  2. One thread per (2 x 2 block of fine particles, field): when the
+//     block's centre cells span at most 2 x 2 cells -- the common case,
+//     neighbouring fine particles are interpolated from the same coarse
+//     particles and move together -- the block's four TSC stencils are
+//     summed in a fixed order into a 4 x 4 float64 register patch and added
+//     through the exact fixed-point split into the shared window (lanes of
+//     a warp own different blocks, so they hit different cells). Otherwise
+//     each particle is added on its own, into the window or, outside it,
+//     straight into the global accumulators.
+//  3. The touched part of the window is added to the global accumulators.
+// All additions are integer, so the result does not depend on their order.
+__global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) {
+    extern __shared__ unsigned long long smem_u64[];
+    unsigned long long* win = smem_u64;                                   // [DEP_WORDS][DEP_WIN]
+    double* s_xl = reinterpret_cast<double*>(win + DEP_WORDS * DEP_WIN);  // [DEP_THREADS]
+    double* s_yl = s_xl + DEP_THREADS;
+    double* s_v = s_yl + DEP_THREADS;                                     // [4][DEP_THREADS]
+    int* s_cell = reinterpret_cast<int*>(s_v + 4 * DEP_THREADS);         // i << 16 | j, or -1
+    __shared__ int s_bb[4];                                               // imin imax jmin jmax
+    const int t = threadIdx.x;
     const int N = a.N;
-    const size_t NN = (size_t)N * N;
-    if (tid == 0) {
+    const size_t NN = a.plane;
+    if (t == 0) {
         s_bb[0] = s_bb[2] = 1 << 30;
         s_bb[1] = s_bb[3] = -(1 << 30);
     }
-    for (int w = tid; w < DEP_WORDS * DEP_WIN; w += 256) win[w] = 0ull;
+    for (int w = t; w < DEP_WORDS * DEP_WIN; w += DEP_THREADS) win[w] = 0ull;
 
-    Dep P[4];
-    bool ok[4];
-    int imin = 1 << 30, imax = -(1 << 30), jmin = 1 << 30, jmax = -(1 << 30);
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-        const int fi = blockIdx.y * DEP_T + 2 * ty + (p >> 1);
-        const int fj = blockIdx.x * DEP_T + 2 * tx + (p & 1);
-        ok[p] = false;
+    // ---- phase 1: one fine particle per thread ----
+    {
+        const int fi = blockIdx.y * DEP_T + (t >> 5), fj = blockIdx.x * DEP_T + (t & 31);
+        int cell = -1, i = 1 << 30, j = 1 << 30;
         if (fi < a.Nf && fj < a.Nf) {
             const FineParticle f = fine_particle(a, fi, fj);
-            tsc_cell(f.x, f.y, N, a.h, P[p].i, P[p].j, P[p].xl, P[p].yl);
-            P[p].v[0] = f.dro;
-            P[p].v[1] = f.djx;
-            P[p].v[2] = f.djy;
-            P[p].v[3] = f.djz;
+            double xl, yl;
+            tsc_cell(f.x, f.y, N, a.h, i, j, xl, yl);
             const double vmax = fmax(fmax(fabs(f.dro), fabs(f.djx)), fmax(fabs(f.djy), fabs(f.djz)));
-            const bool in_grid = P[p].i >= 1 && P[p].i <= N - 2 && P[p].j >= 1 && P[p].j <= N - 2;
-            if (!in_grid) {
+            if (!(i >= 1 && i <= N - 2 && j >= 1 && j <= N - 2)) {
                 atomicOr(a.err, LC3D_FLAG_WINDOW);
             } else if (!(vmax < FX_MAX)) {   // also catches NaN
                 atomicOr(a.err, LC3D_FLAG_NONFINITE);
             } else {
-                ok[p] = true;
-                imin = min(imin, P[p].i);
-                imax = max(imax, P[p].i);
-                jmin = min(jmin, P[p].j);
-                jmax = max(jmax, P[p].j);
+                cell = (i << 16) | j;
             }
+            s_xl[t] = xl;
+            s_yl[t] = yl;
+            s_v[t] = f.dro;
+            s_v[DEP_THREADS + t] = f.djx;
+            s_v[2 * DEP_THREADS + t] = f.djy;
+            s_v[3 * DEP_THREADS + t] = f.djz;
         }
-    }
-    const int ti0 = imin, ti1 = imax, tj0 = jmin, tj1 = jmax;
+        s_cell[t] = cell;
+        int imin = cell >= 0 ? i : 1 << 30, imax = cell >= 0 ? i : -(1 << 30);
+        int jmin = cell >= 0 ? j : 1 << 30, jmax = cell >= 0 ? j : -(1 << 30);
 #pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        imin = min(imin, __shfl_xor_sync(0xffffffffu, imin, o));
-        imax = max(imax, __shfl_xor_sync(0xffffffffu, imax, o));
-        jmin = min(jmin, __shfl_xor_sync(0xffffffffu, jmin, o));
-        jmax = max(jmax, __shfl_xor_sync(0xffffffffu, jmax, o));
-    }
-    __syncthreads();
-    if ((tid & 31) == 0 && imin <= imax) {
-        atomicMin(&s_bb[0], imin);
-        atomicMax(&s_bb[1], imax);
-        atomicMin(&s_bb[2], jmin);
-        atomicMax(&s_bb[3], jmax);
+        for (int o = 16; o; o >>= 1) {
+            imin = min(imin, __shfl_xor_sync(0xffffffffu, imin, o));
+            imax = max(imax, __shfl_xor_sync(0xffffffffu, imax, o));
+            jmin = min(jmin, __shfl_xor_sync(0xffffffffu, jmin, o));
+            jmax = max(jmax, __shfl_xor_sync(0xffffffffu, jmax, o));
+        }
+        __syncthreads();   // s_bb initialised, window zeroed
+        if ((t & 31) == 0 && imin <= imax) {
+            atomicMin(&s_bb[0], imin);
+            atomicMax(&s_bb[1], imax);
+            atomicMin(&s_bb[2], jmin);
+            atomicMax(&s_bb[3], jmax);
+        }
     }
     __syncthreads();
     const int oi = s_bb[0] - 1, oj = s_bb[2] - 1;   // window origin (cells)
 
-    const bool patch = ti0 <= ti1 && ti1 - ti0 <= 1 && tj1 - tj0 <= 1 && ti0 + 2 - oi < DEP_W &&
-                       tj0 + 2 - oj < DEP_W;
-    if (patch) {
-        const int r0 = ti0 - 1 - oi, c0 = tj0 - 1 - oj;
-#pragma unroll 1
-        for (int f = 0; f < 4; ++f) {
+    // ---- phase 2: one (2 x 2 block, field) per thread ----
+    {
+        const int f = t >> 8, blk = t & 255;
+        const int p0 = (blk >> 4) * 2 * DEP_T + (blk & 15) * 2;   // top-left particle of the block
+        const int pidx[4] = {p0, p0 + 1, p0 + DEP_T, p0 + DEP_T + 1};
+        int ci[4], cj[4];
+        bool ok[4];
+        int i0 = 1 << 30, i1 = -(1 << 30), j0 = 1 << 30, j1 = -(1 << 30);
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int c = s_cell[pidx[p]];
+            ok[p] = c >= 0;
+            ci[p] = c >> 16;
+            cj[p] = c & 0xffff;
+            if (ok[p]) {
+                i0 = min(i0, ci[p]);
+                i1 = max(i1, ci[p]);
+                j0 = min(j0, cj[p]);
+                j1 = max(j1, cj[p]);
+            }
+        }
+        unsigned long long* hp = win + (2 * f) * DEP_WIN;
+        unsigned long long* lp = hp + DEP_WIN;
+        const double* vf = s_v + f * DEP_THREADS;
+        const bool patch = i0 <= i1 && i1 - i0 <= 1 && j1 - j0 <= 1 && i0 + 2 - oi < DEP_W && j0 + 2 - oj < DEP_W;
+        if (patch) {
             double acc[16];
 #pragma unroll
             for (int k = 0; k < 16; ++k) acc[k] = 0.0;
@@ -340,58 +355,55 @@ __global__ void __launch_bounds__(256, 1) deposit_kernel(DepositArgs a) {
             for (int p = 0; p < 4; ++p) {
                 if (!ok[p]) continue;
                 double wxM, wx0, wxP, wyM, wy0, wyP;
-                tsc_axis(P[p].xl, wxM, wx0, wxP);
-                tsc_axis(P[p].yl, wyM, wy0, wyP);
-                const bool si = P[p].i != ti0, sj = P[p].j != tj0;
+                tsc_axis(s_xl[pidx[p]], wxM, wx0, wxP);
+                tsc_axis(s_yl[pidx[p]], wyM, wy0, wyP);
+                const bool si = ci[p] != i0, sj = cj[p] != j0;
                 const double wx4[4] = {si ? 0.0 : wxM, si ? wxM : wx0, si ? wx0 : wxP, si ? wxP : 0.0};
                 const double wy4[4] = {sj ? 0.0 : wyM, sj ? wyM : wy0, sj ? wy0 : wyP, sj ? wyP : 0.0};
-                const double v = pick4(P[p].v, f);
+                const double v = vf[pidx[p]];
 #pragma unroll
                 for (int r = 0; r < 4; ++r)
 #pragma unroll
                     for (int c = 0; c < 4; ++c) acc[r * 4 + c] += v * (wx4[r] * wy4[c]);
             }
-            unsigned long long* hp = win + (2 * f) * DEP_WIN;
-            unsigned long long* lp = hp + DEP_WIN;
+            const int r0 = i0 - 1 - oi, c0 = j0 - 1 - oj;
 #pragma unroll
             for (int r = 0; r < 4; ++r)
 #pragma unroll
                 for (int c = 0; c < 4; ++c)
                     if (acc[r * 4 + c] != 0.0) fx_add(hp, lp, (r0 + r) * DEP_W + (c0 + c), acc[r * 4 + c]);
-        }
-    } else {
-#pragma unroll
-        for (int p = 0; p < 4; ++p) {
-            if (!ok[p]) continue;
-            double wx[3], wy[3];
-            tsc_axis(P[p].xl, wx[0], wx[1], wx[2]);
-            tsc_axis(P[p].yl, wy[0], wy[1], wy[2]);
-            const int li = P[p].i - oi, lj = P[p].j - oj;
-            const bool inside = li + 1 < DEP_W && lj + 1 < DEP_W;
+        } else {
 #pragma unroll 1
-            for (int f = 0; f < 4; ++f) {
-                const double v = pick4(P[p].v, f);
+            for (int p = 0; p < 4; ++p) {
+                const int c = s_cell[pidx[p]];
+                if (c < 0) continue;
+                const int pi = c >> 16, pj = c & 0xffff;
+                double wx[3], wy[3];
+                tsc_axis(s_xl[pidx[p]], wx[0], wx[1], wx[2]);
+                tsc_axis(s_yl[pidx[p]], wy[0], wy[1], wy[2]);
+                const double v = vf[pidx[p]];
+                const int li = pi - oi, lj = pj - oj;
+                const bool inside = li + 1 < DEP_W && lj + 1 < DEP_W;
 #pragma unroll
                 for (int di = 0; di < 3; ++di)
 #pragma unroll
                     for (int dj = 0; dj < 3; ++dj) {
-                        const double c = v * (wx[di] * wy[dj]);
+                        const double cv = v * (wx[di] * wy[dj]);
                         if (inside)
-                            fx_add(win + (2 * f) * DEP_WIN, win + (2 * f + 1) * DEP_WIN,
-                                   (li + di - 1) * DEP_W + (lj + dj - 1), c);
+                            fx_add(hp, lp, (li + di - 1) * DEP_W + (lj + dj - 1), cv);
                         else
                             fx_add(a.acc + (2 * f) * NN, a.acc + (2 * f + 1) * NN,
-                                   (size_t)(P[p].i + di - 1) * N + (P[p].j + dj - 1), c);
+                                   (size_t)(pi + di - 1) * N + (pj + dj - 1), cv);
                     }
             }
         }
     }
     __syncthreads();
-    // flush the touched part of the window
+    // ---- phase 3: flush the touched part of the window ----
     if (s_bb[0] <= s_bb[1]) {
         const int ni = min(s_bb[1] + 2 - oi, DEP_W), nj = min(s_bb[3] + 2 - oj, DEP_W);
         const int plane = ni * nj;
-        for (int w = tid; w < DEP_WORDS * plane; w += 256) {
+        for (int w = t; w < DEP_WORDS * plane; w += DEP_THREADS) {
             const int word = w / plane, rem = w - word * plane;
             const int r = rem / nj, c = rem - r * nj;
             const unsigned long long v = win[word * DEP_WIN + r * DEP_W + c];
@@ -400,24 +412,43 @@ __global__ void __launch_bounds__(256, 1) deposit_kernel(DepositArgs a) {
     }
 }
 
+// Accumulators -> float64 (+ ion background), two cells per thread with
+// 16-byte loads; the accumulators are cleared for the next deposition.
 __global__ void __launch_bounds__(256) deposit_finalize_kernel(DepositFinalizeArgs f) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     if (k >= f.n) return;
-    const size_t NN = (size_t)f.n;
-    unsigned long long* acc = f.acc;
-    double out[4];
+    const size_t P = f.plane;
+    double out[4][2];
+    if (k + 1 < f.n) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const unsigned long long hi = acc[(2 * q) * NN + k], lo = acc[(2 * q + 1) * NN + k];
-        acc[(2 * q) * NN + k] = 0ull;
-        acc[(2 * q + 1) * NN + k] = 0ull;
-        out[q] = fx_value((long long)hi, (long long)lo);
+        for (int q = 0; q < 4; ++q) {
+            ulonglong2* hp = reinterpret_cast<ulonglong2*>(f.acc + (2 * q) * P + k);
+            ulonglong2* lp = reinterpret_cast<ulonglong2*>(f.acc + (2 * q + 1) * P + k);
+            const ulonglong2 h = *hp, l = *lp;
+            *hp = make_ulonglong2(0ull, 0ull);
+            *lp = make_ulonglong2(0ull, 0ull);
+            out[q][0] = fx_value((long long)h.x, (long long)l.x);
+            out[q][1] = fx_value((long long)h.y, (long long)l.y);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            unsigned long long* hp = f.acc + (2 * q) * P + k;
+            unsigned long long* lp = f.acc + (2 * q + 1) * P + k;
+            out[q][0] = fx_value((long long)*hp, (long long)*lp);
+            *hp = 0ull;
+            *lp = 0ull;
+        }
     }
-    if (f.ro_initial) out[0] += f.ro_initial[k];
-    f.ro[k] = out[0];
-    f.jx[k] = out[1];
-    f.jy[k] = out[2];
-    f.jz[k] = out[3];
+    const int nk = (k + 1 < f.n) ? 2 : 1;
+    for (int e = 0; e < nk; ++e) {
+        double ro = out[0][e];
+        if (f.ro_initial) ro += f.ro_initial[k + e];
+        f.ro[k + e] = ro;
+        f.jx[k + e] = out[1][e];
+        f.jy[k + e] = out[2][e];
+        f.jz[k + e] = out[3][e];
+    }
 }
 
 }  // namespace
@@ -444,13 +475,13 @@ int particles_prepare() {
 int launch_deposit_main(const DepositArgs& a, cudaStream_t s) {
     if (a.Nf <= 0) return LC3D_OK;
     dim3 grid((a.Nf + DEP_T - 1) / DEP_T, (a.Nf + DEP_T - 1) / DEP_T);
-    deposit_kernel<<<grid, dim3(DEP_B, DEP_B), DEP_SMEM, s>>>(a);
+    deposit_kernel<<<grid, DEP_THREADS, DEP_SMEM, s>>>(a);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
 
 int launch_deposit_finalize(const DepositFinalizeArgs& f, cudaStream_t s) {
-    deposit_finalize_kernel<<<(f.n + 255) / 256, 256, 0, s>>>(f);
+    deposit_finalize_kernel<<<((f.n + 1) / 2 + 255) / 256, 256, 0, s>>>(f);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
