@@ -201,9 +201,9 @@ constexpr int DEP_T = 32;                 // fine particles per CTA side
 constexpr int DEP_THREADS = DEP_T * DEP_T; // phase 1: one fine particle per thread
 constexpr int DEP_W = 32;                 // shared window side (cells)
 constexpr int DEP_WIN = DEP_W * DEP_W;
-constexpr int DEP_WORDS = 8;              // 4 fields x (hi, lo), one plane each
-// shared memory: window planes + per-particle staging (cell, xl, yl, 4 values)
-constexpr size_t DEP_SMEM = (size_t)DEP_WORDS * DEP_WIN * sizeof(unsigned long long) +
+// shared memory: float64 window (4 fields), anchor claims, per-particle
+// staging (cell, xl, yl, 4 values)
+constexpr size_t DEP_SMEM = (size_t)4 * DEP_WIN * sizeof(double) + (size_t)DEP_WIN * sizeof(int) +
                             (size_t)DEP_THREADS * (6 * sizeof(double) + sizeof(int));
 
 // One fine particle: coarse->fine mix (lcode.py:591-621) and the deposit
@@ -246,29 +246,34 @@ __device__ __forceinline__ void fx_add(unsigned long long* hi_plane, unsigned lo
 }
 
 // Deposition of a 32 x 32 patch of the fine lattice by one CTA of 1024
-// threads, in three phases.
+// threads. Deterministic: every float64 sum below has a fixed order, and the
+// sums that cross CTAs are exact integer (fixed-point) sums.
 //  1. One thread per fine particle: coarse->fine interpolation, deposit
-//     values and TSC cell, staged in shared memory; CTA bounding box of the
-//     particles' cells (the window is placed on it).
-//  2. One thread per (2 x 2 block of fine particles, field): when the
-//     block's centre cells span at most 2 x 2 cells -- the common case,
-//     neighbouring fine particles are interpolated from the same coarse
-//     particles and move together -- the block's four TSC stencils are
-//     summed in a fixed order into a 4 x 4 float64 register patch and added
-//     through the exact fixed-point split into the shared window (lanes of
-//     a warp own different blocks, so they hit different cells). Otherwise
-//     each particle is added on its own, into the window or, outside it,
-//     straight into the global accumulators.
-//  3. The touched part of the window is added to the global accumulators.
-// All additions are integer, so the result does not depend on their order.
+//     values and TSC cell, staged in shared memory; the CTA's bounding box
+//     of cells places a 32 x 32-cell float64 window.
+//  2. One thread per (2 x 2 block of fine particles, field). If the block's
+//     centre cells span at most 2 x 2 cells -- neighbouring fine particles
+//     are interpolated from the same coarse particles and move together --
+//     its four TSC stencils are summed in a fixed order into a 4 x 4 float64
+//     register patch. Blocks claim their patch anchor cell (atomicMax of
+//     the block index: the winner does not depend on timing); winners add
+//     their patches to the window in 16 barrier-separated steps, one patch
+//     entry per step, so in each step every window cell has at most one
+//     writer and its summation order is fixed. Losing blocks (two blocks on
+//     one anchor, < 1% of blocks in the 641^2 blowout run) and blocks that
+//     span more cells or leave the window add their contributions straight
+//     to the global accumulators through the exact fixed-point split.
+//  3. Each touched window cell is split once into fixed point and added to
+//     the global accumulators.
 __global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) {
-    extern __shared__ unsigned long long smem_u64[];
-    unsigned long long* win = smem_u64;                                   // [DEP_WORDS][DEP_WIN]
-    double* s_xl = reinterpret_cast<double*>(win + DEP_WORDS * DEP_WIN);  // [DEP_THREADS]
+    extern __shared__ double smem_f64[];
+    double* fwin = smem_f64;                                   // [4][DEP_WIN]
+    double* s_xl = fwin + 4 * DEP_WIN;                         // [DEP_THREADS]
     double* s_yl = s_xl + DEP_THREADS;
-    double* s_v = s_yl + DEP_THREADS;                                     // [4][DEP_THREADS]
-    int* s_cell = reinterpret_cast<int*>(s_v + 4 * DEP_THREADS);         // i << 16 | j, or -1
-    __shared__ int s_bb[4];                                               // imin imax jmin jmax
+    double* s_v = s_yl + DEP_THREADS;                          // [4][DEP_THREADS]
+    int* s_cell = reinterpret_cast<int*>(s_v + 4 * DEP_THREADS);   // i << 16 | j, or -1
+    int* s_claim = s_cell + DEP_THREADS;                       // [DEP_WIN]
+    __shared__ int s_bb[4];                                    // imin imax jmin jmax
     const int t = threadIdx.x;
     const int N = a.N;
     const size_t NN = a.plane;
@@ -276,7 +281,8 @@ __global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) 
         s_bb[0] = s_bb[2] = 1 << 30;
         s_bb[1] = s_bb[3] = -(1 << 30);
     }
-    for (int w = t; w < DEP_WORDS * DEP_WIN; w += DEP_THREADS) win[w] = 0ull;
+    for (int w = t; w < 4 * DEP_WIN; w += DEP_THREADS) fwin[w] = 0.0;
+    for (int w = t; w < DEP_WIN; w += DEP_THREADS) s_claim[w] = -1;
 
     // ---- phase 1: one fine particle per thread ----
     {
@@ -311,7 +317,7 @@ __global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) 
             jmin = min(jmin, __shfl_xor_sync(0xffffffffu, jmin, o));
             jmax = max(jmax, __shfl_xor_sync(0xffffffffu, jmax, o));
         }
-        __syncthreads();   // s_bb initialised, window zeroed
+        __syncthreads();   // s_bb initialised, window and claims cleared
         if ((t & 31) == 0 && imin <= imax) {
             atomicMin(&s_bb[0], imin);
             atomicMax(&s_bb[1], imax);
@@ -323,91 +329,94 @@ __global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) 
     const int oi = s_bb[0] - 1, oj = s_bb[2] - 1;   // window origin (cells)
 
     // ---- phase 2: one (2 x 2 block, field) per thread ----
-    {
-        const int f = t >> 8, blk = t & 255;
-        const int p0 = (blk >> 4) * 2 * DEP_T + (blk & 15) * 2;   // top-left particle of the block
-        const int pidx[4] = {p0, p0 + 1, p0 + DEP_T, p0 + DEP_T + 1};
-        int ci[4], cj[4];
-        bool ok[4];
-        int i0 = 1 << 30, i1 = -(1 << 30), j0 = 1 << 30, j1 = -(1 << 30);
+    const int f = t >> 8, blk = t & 255;
+    const int p0 = (blk >> 4) * 2 * DEP_T + (blk & 15) * 2;   // top-left particle of the block
+    const int pidx[4] = {p0, p0 + 1, p0 + DEP_T, p0 + DEP_T + 1};
+    int ci[4], cj[4];
+    bool ok[4];
+    int i0 = 1 << 30, i1 = -(1 << 30), j0 = 1 << 30, j1 = -(1 << 30);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int c = s_cell[pidx[p]];
+        ok[p] = c >= 0;
+        ci[p] = c >> 16;
+        cj[p] = c & 0xffff;
+        if (ok[p]) {
+            i0 = min(i0, ci[p]);
+            i1 = max(i1, ci[p]);
+            j0 = min(j0, cj[p]);
+            j1 = max(j1, cj[p]);
+        }
+    }
+    const bool patch = i0 <= i1 && i1 - i0 <= 1 && j1 - j0 <= 1 && i0 + 2 - oi < DEP_W && j0 + 2 - oj < DEP_W;
+    const int r0 = i0 - 1 - oi, c0 = j0 - 1 - oj;   // window coordinates of the patch corner
+    if (patch && f == 0) atomicMax(&s_claim[r0 * DEP_W + c0], blk);
+    __syncthreads();
+    const bool winner = patch && s_claim[r0 * DEP_W + c0] == blk;
+    unsigned long long* ghi = a.acc + (2 * f) * NN;
+    unsigned long long* glo = ghi + NN;
+    const double* vf = s_v + f * DEP_THREADS;
+    double acc[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) acc[k] = 0.0;
+    if (patch) {
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
-            const int c = s_cell[pidx[p]];
-            ok[p] = c >= 0;
-            ci[p] = c >> 16;
-            cj[p] = c & 0xffff;
-            if (ok[p]) {
-                i0 = min(i0, ci[p]);
-                i1 = max(i1, ci[p]);
-                j0 = min(j0, cj[p]);
-                j1 = max(j1, cj[p]);
-            }
+            if (!ok[p]) continue;
+            double wxM, wx0, wxP, wyM, wy0, wyP;
+            tsc_axis(s_xl[pidx[p]], wxM, wx0, wxP);
+            tsc_axis(s_yl[pidx[p]], wyM, wy0, wyP);
+            const bool si = ci[p] != i0, sj = cj[p] != j0;
+            const double wx4[4] = {si ? 0.0 : wxM, si ? wxM : wx0, si ? wx0 : wxP, si ? wxP : 0.0};
+            const double wy4[4] = {sj ? 0.0 : wyM, sj ? wyM : wy0, sj ? wy0 : wyP, sj ? wyP : 0.0};
+            const double v = vf[pidx[p]];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r * 4 + c] += v * (wx4[r] * wy4[c]);
         }
-        unsigned long long* hp = win + (2 * f) * DEP_WIN;
-        unsigned long long* lp = hp + DEP_WIN;
-        const double* vf = s_v + f * DEP_THREADS;
-        const bool patch = i0 <= i1 && i1 - i0 <= 1 && j1 - j0 <= 1 && i0 + 2 - oi < DEP_W && j0 + 2 - oj < DEP_W;
-        if (patch) {
-            double acc[16];
-#pragma unroll
-            for (int k = 0; k < 16; ++k) acc[k] = 0.0;
-#pragma unroll
-            for (int p = 0; p < 4; ++p) {
-                if (!ok[p]) continue;
-                double wxM, wx0, wxP, wyM, wy0, wyP;
-                tsc_axis(s_xl[pidx[p]], wxM, wx0, wxP);
-                tsc_axis(s_yl[pidx[p]], wyM, wy0, wyP);
-                const bool si = ci[p] != i0, sj = cj[p] != j0;
-                const double wx4[4] = {si ? 0.0 : wxM, si ? wxM : wx0, si ? wx0 : wxP, si ? wxP : 0.0};
-                const double wy4[4] = {sj ? 0.0 : wyM, sj ? wyM : wy0, sj ? wy0 : wyP, sj ? wyP : 0.0};
-                const double v = vf[pidx[p]];
-#pragma unroll
-                for (int r = 0; r < 4; ++r)
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) acc[r * 4 + c] += v * (wx4[r] * wy4[c]);
-            }
-            const int r0 = i0 - 1 - oi, c0 = j0 - 1 - oj;
+        if (!winner) {
 #pragma unroll
             for (int r = 0; r < 4; ++r)
 #pragma unroll
                 for (int c = 0; c < 4; ++c)
-                    if (acc[r * 4 + c] != 0.0) fx_add(hp, lp, (r0 + r) * DEP_W + (c0 + c), acc[r * 4 + c]);
-        } else {
+                    if (acc[r * 4 + c] != 0.0) fx_add(ghi, glo, (size_t)(i0 - 1 + r) * N + (j0 - 1 + c), acc[r * 4 + c]);
+        }
+    } else {
 #pragma unroll 1
-            for (int p = 0; p < 4; ++p) {
-                const int c = s_cell[pidx[p]];
-                if (c < 0) continue;
-                const int pi = c >> 16, pj = c & 0xffff;
-                double wx[3], wy[3];
-                tsc_axis(s_xl[pidx[p]], wx[0], wx[1], wx[2]);
-                tsc_axis(s_yl[pidx[p]], wy[0], wy[1], wy[2]);
-                const double v = vf[pidx[p]];
-                const int li = pi - oi, lj = pj - oj;
-                const bool inside = li + 1 < DEP_W && lj + 1 < DEP_W;
+        for (int p = 0; p < 4; ++p) {
+            const int c = s_cell[pidx[p]];
+            if (c < 0) continue;
+            const int pi = c >> 16, pj = c & 0xffff;
+            double wx[3], wy[3];
+            tsc_axis(s_xl[pidx[p]], wx[0], wx[1], wx[2]);
+            tsc_axis(s_yl[pidx[p]], wy[0], wy[1], wy[2]);
+            const double v = vf[pidx[p]];
 #pragma unroll
-                for (int di = 0; di < 3; ++di)
+            for (int di = 0; di < 3; ++di)
 #pragma unroll
-                    for (int dj = 0; dj < 3; ++dj) {
-                        const double cv = v * (wx[di] * wy[dj]);
-                        if (inside)
-                            fx_add(hp, lp, (li + di - 1) * DEP_W + (lj + dj - 1), cv);
-                        else
-                            fx_add(a.acc + (2 * f) * NN, a.acc + (2 * f + 1) * NN,
-                                   (size_t)(pi + di - 1) * N + (pj + dj - 1), cv);
-                    }
-            }
+                for (int dj = 0; dj < 3; ++dj)
+                    fx_add(ghi, glo, (size_t)(pi + di - 1) * N + (pj + dj - 1), v * (wx[di] * wy[dj]));
         }
     }
-    __syncthreads();
-    // ---- phase 3: flush the touched part of the window ----
+    // winners add their patches, one entry per barrier-separated step
+    double* fw = fwin + f * DEP_WIN + (winner ? r0 * DEP_W + c0 : 0);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        if (winner && acc[k] != 0.0) fw[(k >> 2) * DEP_W + (k & 3)] += acc[k];
+        __syncthreads();
+    }
+
+    // ---- phase 3: split each touched window cell once, add to global ----
     if (s_bb[0] <= s_bb[1]) {
         const int ni = min(s_bb[1] + 2 - oi, DEP_W), nj = min(s_bb[3] + 2 - oj, DEP_W);
         const int plane = ni * nj;
-        for (int w = t; w < DEP_WORDS * plane; w += DEP_THREADS) {
-            const int word = w / plane, rem = w - word * plane;
+        for (int w = t; w < 4 * plane; w += DEP_THREADS) {
+            const int q = w / plane, rem = w - q * plane;
             const int r = rem / nj, c = rem - r * nj;
-            const unsigned long long v = win[word * DEP_WIN + r * DEP_W + c];
-            if (v) atomicAdd(a.acc + word * NN + (size_t)(oi + r) * N + (oj + c), v);
+            const double v = fwin[q * DEP_WIN + r * DEP_W + c];
+            if (v != 0.0)
+                fx_add(a.acc + (2 * q) * NN, a.acc + (2 * q + 1) * NN, (size_t)(oi + r) * N + (oj + c), v);
         }
     }
 }
