@@ -8,9 +8,9 @@
 //     DCT-I: Z = Y_a + i Y_b, Y real         -> X_a = Re Z[k],  X_b = Im Z[k]
 //     DST-I: Z = -i X_a + X_b (Y imaginary)   -> X_a = -Im Z[k+1], X_b = Re Z[k+1]
 // (unnormalised, the conventions of scipy's dct/dst type 1, so DST-I = S2 x
-// and DCT-I = C x of the dense-transform form). The FFT is a Stockham
-// autosort FFT with mixed radices 4, 2, 3, 5, 7, ping-ponging between two
-// shared-memory buffers. Every launch transforms rows and writes its output
+// and DCT-I = C x of the dense-transform form). The FFT is an
+// in-place decimation-in-frequency FFT with mixed radices 4, 2, 3, 5 in
+// shared memory, read out in digit-reversed order. Every launch transforms rows and writes its output
 // TRANSPOSED (out[k][r]), optionally scaled by Lambda[k][r]; the 2-D solve
 // F = L (Lambda o (L X R)) R is then four such passes:
 //     A: rows of X by the axis-1 transform          -> T1^T
@@ -78,6 +78,44 @@ __device__ __forceinline__ void dft<2>(double2 (&v)[2], const double2*, int) {
     v[1] = csub(a, b);
 }
 
+// x -> -i x and x -> +i x
+__device__ __forceinline__ double2 mul_mi(double2 a) { return make_double2(a.y, -a.x); }
+__device__ __forceinline__ double2 mul_pi(double2 a) { return make_double2(-a.y, a.x); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+// 3-point DFT: W = exp(-2 pi i / 3) = (c, -s) read from the twiddle table.
+template <>
+__device__ __forceinline__ void dft<3>(double2 (&v)[3], const double2* tw, int P) {
+    const double2 w = __ldg(tw + P / 3);
+    const double2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+    const double2 a = cadd(v[0], cscale(t1, w.x));
+    const double2 bb = cscale(t2, -w.y);
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(a, mul_mi(bb));
+    v[2] = csub(a, mul_mi(bb));
+}
+
+// 5-point DFT with W = (c1, -s1), W^2 = (c2, -s2) from the twiddle table:
+// X1,4 = v0 + c1 t1 + c2 t2 -+ i (s1 t3 + s2 t4),
+// X2,3 = v0 + c2 t1 + c1 t2 -+ i (s2 t3 - s1 t4),
+// t1 = v1 + v4, t2 = v2 + v3, t3 = v1 - v4, t4 = v2 - v3.
+template <>
+__device__ __forceinline__ void dft<5>(double2 (&v)[5], const double2* tw, int P) {
+    const double2 w1 = __ldg(tw + P / 5), w2 = __ldg(tw + 2 * (P / 5));
+    const double c1 = w1.x, s1 = -w1.y, c2 = w2.x, s2 = -w2.y;
+    const double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    const double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    const double2 a1 = cadd(v[0], cadd(cscale(t1, c1), cscale(t2, c2)));
+    const double2 a2 = cadd(v[0], cadd(cscale(t1, c2), cscale(t2, c1)));
+    const double2 b1 = cadd(cscale(t3, s1), cscale(t4, s2));
+    const double2 b2 = csub(cscale(t3, s2), cscale(t4, s1));
+    v[0] = cadd(v[0], cadd(t1, t2));
+    v[1] = cadd(a1, mul_mi(b1));
+    v[4] = csub(a1, mul_mi(b1));
+    v[2] = cadd(a2, mul_mi(b2));
+    v[3] = csub(a2, mul_mi(b2));
+}
+
 template <>
 __device__ __forceinline__ void dft<4>(double2 (&v)[4], const double2*, int) {
     const double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
@@ -89,34 +127,37 @@ __device__ __forceinline__ void dft<4>(double2 (&v)[4], const double2*, int) {
     v[3] = csub(a1, a3);
 }
 
-// One Stockham butterfly: inputs a[j + r P/R], twiddled by
-// exp(-2 pi i r k / (Ns R)), outputs b[(j / Ns) Ns R + k + r Ns].
+// One in-place decimation-in-frequency butterfly of radix R inside a
+// sub-transform of length Lr = R * span: the R inputs A[base + r span] are
+// transformed and output m is scaled by exp(-2 pi i m k / Lr), k the
+// position inside the span, and written back in place. After all passes
+// frequency k = m0 + R0 (m1 + R1 (m2 + ...)) sits at sum_s m_s P / (R0..Rs).
 template <int R>
-__device__ __forceinline__ void butterfly(const double2* a, double2* b, int j, int Ns, int P,
-                                          const double2* __restrict__ tw) {
-    const int k = j % Ns, stride = P / R, tstep = P / (Ns * R);
+__device__ __forceinline__ void dif_butterfly(double2* A, int b, int span, int P, const double2* __restrict__ tw) {
+    const int g = b / span, k = b - g * span;
+    const int base = g * span * R + k;
     double2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = a[j + r * stride];
-#pragma unroll
-    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(tw + r * k * tstep));
+    for (int r = 0; r < R; ++r) v[r] = A[base + r * span];
     dft<R>(v, tw, P);
-    const int d = (j / Ns) * Ns * R + k;
+    const int tstep = P / (span * R);
 #pragma unroll
-    for (int r = 0; r < R; ++r) b[d + r * Ns] = v[r];
+    for (int m = 1; m < R; ++m) v[m] = cmul(v[m], __ldg(tw + m * k * tstep));
+#pragma unroll
+    for (int m = 0; m < R; ++m) A[base + m * span] = v[m];
 }
 
 template <int R>
-__device__ __forceinline__ void fft_pass(const double2* A, double2* B, int Ns, int P, const double2* tw) {
+__device__ __forceinline__ void fft_pass(double2* A, int span, int P, const double2* tw) {
     const int nb = P / R;
     for (int t = threadIdx.x; t < FFT_PER_CTA * nb; t += FFT_THREADS) {
         const int q = t / nb, j = t - q * nb;
-        butterfly<R>(A + q * P, B + q * P, j, Ns, P, tw);
+        dif_butterfly<R>(A + q * P, j, span, P, tw);
     }
 }
 
-__global__ void __launch_bounds__(FFT_THREADS) fft_rows_kernel(const __grid_constant__ FftBatch b) {
-    extern __shared__ double2 sm[];      // [2 buffers][FFT_PER_CTA][P]
+__global__ void __launch_bounds__(FFT_THREADS, 3) fft_rows_kernel(const __grid_constant__ FftBatch b) {
+    extern __shared__ double2 sm[];      // [FFT_PER_CTA][P], transformed in place
     int fi = 0;
 #pragma unroll 1
     for (int q = 1; q < b.count; ++q)
@@ -126,7 +167,6 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_rows_kernel(const __grid_cons
     const int r0 = ((int)blockIdx.x - F.cta_start) * ROWS_PER_CTA;
     const int n = F.type ? b.N - 2 : b.N;     // input / output length
     double2* A = sm;
-    double2* B = sm + FFT_PER_CTA * P;
 
     // symmetric / antisymmetric extensions, two rows per complex FFT
     for (int t = threadIdx.x; t < FFT_PER_CTA * P; t += FFT_THREADS) {
@@ -139,9 +179,9 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_rows_kernel(const __grid_cons
             if (row < F.rows) {
                 const double* rp = F.in + (size_t)row * F.ld_in;
                 if (F.type == 0) {
-                    x = rp[m <= L ? m : P - m];
+                    x = __ldg(rp + (m <= L ? m : P - m));
                 } else if (m != 0 && m != L) {
-                    x = m < L ? rp[m - 1] : -rp[P - m - 1];
+                    x = m < L ? __ldg(rp + m - 1) : -__ldg(rp + P - m - 1);
                 }
             }
             v[h] = x;
@@ -149,29 +189,34 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_rows_kernel(const __grid_cons
         A[t] = make_double2(v[0], v[1]);
     }
     __syncthreads();
-    int Ns = 1;
+    int span = P;
     for (int p = 0; p < b.nrad; ++p) {
         const int R = b.rad[p];
+        span /= R;
         switch (R) {
-            case 4: fft_pass<4>(A, B, Ns, P, b.tw); break;
-            case 2: fft_pass<2>(A, B, Ns, P, b.tw); break;
-            case 3: fft_pass<3>(A, B, Ns, P, b.tw); break;
-            case 5: fft_pass<5>(A, B, Ns, P, b.tw); break;
-            default: fft_pass<7>(A, B, Ns, P, b.tw); break;
+            case 4: fft_pass<4>(A, span, P, b.tw); break;
+            case 2: fft_pass<2>(A, span, P, b.tw); break;
+            case 3: fft_pass<3>(A, span, P, b.tw); break;
+            default: fft_pass<5>(A, span, P, b.tw); break;
         }
         __syncthreads();
-        double2* t = A;
-        A = B;
-        B = t;
-        Ns *= R;
     }
-    // transposed output, 4 consecutive rows per output index k
+    // transposed output, 4 consecutive rows per output index k; frequency
+    // kk sits at its digit-reversed position
     const int off = F.type;   // DST-I outputs are Z[1 .. L-1]
     for (int t = threadIdx.x; t < n * ROWS_PER_CTA; t += FFT_THREADS) {
         const int k = t / ROWS_PER_CTA, rr = t - k * ROWS_PER_CTA;
         const int row = r0 + rr;
         if (row >= F.rows) continue;
-        const double2 z = A[(rr >> 1) * P + k + off];
+        int kk = k + off, pos = 0, rem = P;
+        for (int p = 0; p < b.nrad; ++p) {
+            const int R = b.rad[p];
+            const int m = kk % R;
+            kk /= R;
+            rem /= R;
+            pos += m * rem;
+        }
+        const double2 z = A[(rr >> 1) * P + pos];
         double x;
         if (F.type == 0)
             x = (rr & 1) ? z.y : z.x;
@@ -193,19 +238,20 @@ double sin_pi_frac(long long r, long long L) {
 
 }  // namespace
 
-// Radix plan for a length-P FFT: factors 4, 2, 3, 5, 7 (largest powers of 4
-// first). Returns the number of passes, or 0 if P has another prime factor.
+// Radix plan for a length-P FFT: factors 4, 2, 3, 5 (powers of 4 first).
+// Returns the number of passes, or 0 if P has another prime factor (the
+// dense transform form is used then).
 int fft_plan(int P, int* rad) {
     int n = 0;
     int r = P;
     while (r % 4 == 0 && n < MAX_RADICES) { rad[n++] = 4; r /= 4; }
-    const int others[] = {2, 3, 5, 7};
+    const int others[] = {2, 3, 5};
     for (int f : others)
         while (r % f == 0 && n < MAX_RADICES) { rad[n++] = f; r /= f; }
     return (r == 1) ? n : 0;
 }
 
-size_t fft_smem_bytes(int P) { return (size_t)2 * FFT_PER_CTA * P * sizeof(double2); }
+size_t fft_smem_bytes(int P) { return (size_t)FFT_PER_CTA * P * sizeof(double2); }
 
 int fft_init(lc3d_ctx* c) {
     const int P = 2 * (c->N - 1);
