@@ -48,6 +48,7 @@ struct FftBatch {
     int nrad;
     int rad[MAX_RADICES];
     const double2* tw;                   // tw[m] = exp(-2 pi i m / P)
+    const int* pos;                      // position of frequency k after the DIF passes
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -133,8 +134,11 @@ __device__ __forceinline__ void dft<4>(double2 (&v)[4], const double2*, int) {
 // position inside the span, and written back in place. After all passes
 // frequency k = m0 + R0 (m1 + R1 (m2 + ...)) sits at sum_s m_s P / (R0..Rs).
 template <int R>
-__device__ __forceinline__ void dif_butterfly(double2* A, int b, int span, int P, const double2* __restrict__ tw) {
-    const int g = b / span, k = b - g * span;
+__device__ __forceinline__ void dif_butterfly(double2* A, int b, int span, float inv_span, int P,
+                                              const double2* __restrict__ tw) {
+    // g = b / span: (b + 0.5) / span lies at least 0.5 / span from an
+    // integer, far more than the float rounding for b, span < 2^16
+    const int g = __float2int_rz(((float)b + 0.5f) * inv_span), k = b - g * span;
     const int base = g * span * R + k;
     double2 v[R];
 #pragma unroll
@@ -149,10 +153,12 @@ __device__ __forceinline__ void dif_butterfly(double2* A, int b, int span, int P
 
 template <int R>
 __device__ __forceinline__ void fft_pass(double2* A, int span, int P, const double2* tw) {
+    static_assert(FFT_PER_CTA == 2, "the FFT index below assumes two FFTs per CTA");
     const int nb = P / R;
+    const float inv_span = 1.0f / (float)span;
     for (int t = threadIdx.x; t < FFT_PER_CTA * nb; t += FFT_THREADS) {
-        const int q = t / nb, j = t - q * nb;
-        dif_butterfly<R>(A + q * P, j, span, P, tw);
+        const int q = t >= nb, j = t - q * nb;
+        dif_butterfly<R>(A + q * P, j, span, inv_span, P, tw);
     }
 }
 
@@ -170,7 +176,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 3) fft_rows_kernel(const __grid_c
 
     // symmetric / antisymmetric extensions, two rows per complex FFT
     for (int t = threadIdx.x; t < FFT_PER_CTA * P; t += FFT_THREADS) {
-        const int q = t / P, m = t - q * P;
+        const int q = t >= P, m = t - q * P;
         double v[2];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
@@ -208,15 +214,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 3) fft_rows_kernel(const __grid_c
         const int k = t / ROWS_PER_CTA, rr = t - k * ROWS_PER_CTA;
         const int row = r0 + rr;
         if (row >= F.rows) continue;
-        int kk = k + off, pos = 0, rem = P;
-        for (int p = 0; p < b.nrad; ++p) {
-            const int R = b.rad[p];
-            const int m = kk % R;
-            kk /= R;
-            rem /= R;
-            pos += m * rem;
-        }
-        const double2 z = A[(rr >> 1) * P + pos];
+        const double2 z = A[(rr >> 1) * P + __ldg(b.pos + k + off)];
         double x;
         if (F.type == 0)
             x = (rr & 1) ? z.y : z.x;
@@ -259,14 +257,28 @@ int fft_init(lc3d_ctx* c) {
     c->fft_ok = fft_plan(P, rad) > 0 && fft_smem_bytes(P) <= 200 * 1024;
     if (!c->fft_ok) return LC3D_OK;
     LC3D_TRY(fft_prepare(P));
-    std::vector<double> tw(2 * (size_t)P);
+    const int nrad = fft_plan(P, rad);
+    // P twiddles exp(-2 pi i m / P), then P int32 positions: frequency k of
+    // the in-place DIF output sits at pos[k] = sum_s m_s P / (R0..Rs) for the
+    // mixed-radix digits k = m0 + R0 (m1 + R1 (...))
+    std::vector<double> buf(3 * (size_t)P);
     for (int m = 0; m < P; ++m) {
-        // exp(-2 pi i m / P) = cos(2 pi m / P) - i sin(2 pi m / P)
-        tw[2 * m] = sin_pi_frac(4LL * m + P, 2LL * P);      // cos(pi (2m) / P)
-        tw[2 * m + 1] = -sin_pi_frac(2LL * m, (long long)P);
+        buf[2 * m] = sin_pi_frac(4LL * m + P, 2LL * P);      // cos(pi (2m) / P)
+        buf[2 * m + 1] = -sin_pi_frac(2LL * m, (long long)P);
     }
-    LC3D_CUDA_TRY(cudaMalloc(&c->fft_tw, tw.size() * sizeof(double)));
-    LC3D_CUDA_TRY(cudaMemcpy(c->fft_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    int32_t* pos = reinterpret_cast<int32_t*>(buf.data() + 2 * (size_t)P);
+    for (int k = 0; k < P; ++k) {
+        int kk = k, p = 0, rem = P;
+        for (int s = 0; s < nrad; ++s) {
+            const int m = kk % rad[s];
+            kk /= rad[s];
+            rem /= rad[s];
+            p += m * rem;
+        }
+        pos[k] = p;
+    }
+    LC3D_CUDA_TRY(cudaMalloc(&c->fft_tw, buf.size() * sizeof(double)));
+    LC3D_CUDA_TRY(cudaMemcpy(c->fft_tw, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice));
     return LC3D_OK;
 }
 
@@ -286,6 +298,7 @@ int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, cudaStream_t s) {
     b.N = c->N;
     b.nrad = fft_plan(b.P, b.rad);
     b.tw = reinterpret_cast<const double2*>(c->fft_tw);
+    b.pos = reinterpret_cast<const int*>(c->fft_tw + 2 * (size_t)b.P);
     int ctas = 0;
     for (int q = 0; q < count; ++q) {
         FftField& f = b.f[b.count++];

@@ -121,6 +121,7 @@ MoveArgs move_base(lc3d_ctx* c) {
     a.n = c->Nc * c->Nc;
     a.N = c->N;
     a.h = c->p.grid_step_size;
+    a.inv_h = 1.0 / c->p.grid_step_size;
     a.dxi = c->p.xi_step_size;
     a.rb = c->rb;
     a.err = c->err;
@@ -137,7 +138,7 @@ int deposit_into(lc3d_ctx* c, const double* ro_initial, const double* x, const d
     a.acc = c->acc;
     a.plane = c->acc_plane;
     a.Nc = c->Nc; a.Nf = c->Nf; a.N = c->N;
-    a.h = c->p.grid_step_size; a.sf = c->sf;
+    a.h = c->p.grid_step_size; a.inv_h = 1.0 / c->p.grid_step_size; a.sf = c->sf;
     a.err = c->err;
     DepositFinalizeArgs f;
     f.acc = c->acc;

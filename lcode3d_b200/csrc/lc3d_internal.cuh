@@ -41,7 +41,7 @@ struct MoveArgs {
     double *out_x, *out_y, *out_px, *out_py, *out_pz;
     int n;                                // coarse particles
     int N;                                // grid_steps
-    double h, dxi, rb;
+    double h, inv_h, dxi, rb;
     unsigned* err;
 };
 
@@ -59,7 +59,7 @@ struct DepositArgs {
     unsigned long long* acc;                                  // 8 planes of fixed-point words
     size_t plane;                                             // plane stride (>= N*N, 256-byte multiple)
     int Nc, Nf, N;
-    double h, sf;
+    double h, inv_h, sf;
     unsigned* err;
 };
 

@@ -32,9 +32,16 @@ struct Tsc {
 };
 
 // Centre cell (i, j) and offset from the cell centre, lcode.py:404-406.
-__device__ __forceinline__ void tsc_cell(double x, double y, int N, double h, int& i, int& j, double& xl,
-                                         double& yl) {
-    double x_h = x / h + .5, y_h = y / h + .5;
+// x / h correctly rounded from the reciprocal: q0 = x (1/h) is within an ulp,
+// one Newton correction with the exact residual fma(-q0, h, x) rounds it.
+__device__ __forceinline__ double div_h(double x, double h, double inv_h) {
+    const double q0 = x * inv_h;
+    return fma(fma(-q0, h, x), inv_h, q0);
+}
+
+__device__ __forceinline__ void tsc_cell(double x, double y, int N, double h, double inv_h, int& i, int& j,
+                                         double& xl, double& yl) {
+    double x_h = div_h(x, h, inv_h) + .5, y_h = div_h(y, h, inv_h) + .5;
     double fx = floor(x_h), fy = floor(y_h);
     xl = x_h - fx - .5;
     yl = y_h - fy - .5;
@@ -52,10 +59,10 @@ __device__ __forceinline__ void tsc_axis(double l, double& wM, double& w0, doubl
     wM = (.5 - l) * (.5 - l) / 2;
 }
 
-__device__ __forceinline__ Tsc tsc_weights(double x, double y, int N, double h) {
+__device__ __forceinline__ Tsc tsc_weights(double x, double y, int N, double h, double inv_h) {
     Tsc t;
     double xl, yl;
-    tsc_cell(x, y, N, h, t.i, t.j, xl, yl);
+    tsc_cell(x, y, N, h, inv_h, t.i, t.j, xl, yl);
     tsc_axis(xl, t.wxM, t.wx0, t.wxP);
     tsc_axis(yl, t.wyM, t.wy0, t.wyP);
     return t;
@@ -124,7 +131,7 @@ __global__ void __launch_bounds__(256) move_smart_kernel(MoveArgs a) {
     }
     double x_half = xi0 + (x_offt + ex) / 2;
     double y_half = yi0 + (y_offt + ey) / 2;
-    Tsc t = tsc_weights(x_half, y_half, a.N, a.h);
+    Tsc t = tsc_weights(x_half, y_half, a.N, a.h, a.inv_h);
     if (!tsc_in_grid(t, a.N)) {
         // the reference would read out of bounds here; flag and keep prev
         atomicOr(a.err, LC3D_FLAG_WINDOW);
@@ -291,7 +298,7 @@ __global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) 
         if (fi < a.Nf && fj < a.Nf) {
             const FineParticle f = fine_particle(a, fi, fj);
             double xl, yl;
-            tsc_cell(f.x, f.y, N, a.h, i, j, xl, yl);
+            tsc_cell(f.x, f.y, N, a.h, a.inv_h, i, j, xl, yl);
             const double vmax = fmax(fmax(fabs(f.dro), fabs(f.djx)), fmax(fabs(f.djy), fabs(f.djz)));
             if (!(i >= 1 && i <= N - 2 && j >= 1 && j <= N - 2)) {
                 atomicOr(a.err, LC3D_FLAG_WINDOW);
@@ -370,10 +377,13 @@ __global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) 
             const double wx4[4] = {si ? 0.0 : wxM, si ? wxM : wx0, si ? wx0 : wxP, si ? wxP : 0.0};
             const double wy4[4] = {sj ? 0.0 : wyM, sj ? wyM : wy0, sj ? wy0 : wyP, sj ? wyP : 0.0};
             const double v = vf[pidx[p]];
+            // v wx wy as (v wx) wy: 20 instead of 32 float64 operations
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
+            for (int r = 0; r < 4; ++r) {
+                const double vx = v * wx4[r];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) acc[r * 4 + c] += v * (wx4[r] * wy4[c]);
+                for (int c = 0; c < 4; ++c) acc[r * 4 + c] = fma(vx, wy4[c], acc[r * 4 + c]);
+            }
         }
         if (!winner) {
 #pragma unroll
@@ -410,11 +420,10 @@ __global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) 
     // ---- phase 3: split each touched window cell once, add to global ----
     if (s_bb[0] <= s_bb[1]) {
         const int ni = min(s_bb[1] + 2 - oi, DEP_W), nj = min(s_bb[3] + 2 - oj, DEP_W);
-        const int plane = ni * nj;
-        for (int w = t; w < 4 * plane; w += DEP_THREADS) {
-            const int q = w / plane, rem = w - q * plane;
-            const int r = rem / nj, c = rem - r * nj;
-            const double v = fwin[q * DEP_WIN + r * DEP_W + c];
+        for (int w = t; w < 4 * DEP_WIN; w += DEP_THREADS) {
+            const int q = w / DEP_WIN, r = (w / DEP_W) % DEP_W, c = w % DEP_W;
+            if (r >= ni || c >= nj) continue;
+            const double v = fwin[w];
             if (v != 0.0)
                 fx_add(a.acc + (2 * q) * NN, a.acc + (2 * q + 1) * NN, (size_t)(oi + r) * N + (oj + c), v);
         }
