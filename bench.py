@@ -145,6 +145,15 @@ def peaks():
     return 6650.0, 'fallback (6.65 TB/s)'
 
 
+def tensor_peak():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get('bf16_tflops', 1590.0), 'measured bf16 burst (MEASURED_PEAKS.json)'
+    return 1590.0, 'fallback bf16 burst (1.59 PFLOP/s)'
+
+
 def fp64_peak_tflops(torch):
     """FP64 denominator measured in this run: cuBLAS DGEMM 8192^3 (best of
     5), since the measured-peaks file holds no float64 figure."""
@@ -200,6 +209,7 @@ def run_ours(args, rank, world, dist):
     torch.cuda.set_device(dev)
     cfg = make_config(args.grid, args.precision)
     cfg.lc3d_fp64_transform = args.fp64_transform
+    cfg.lc3d_mixed_slices = args.slices
     N = cfg.grid_steps
     xs, ys, const, virt, st = L.init(cfg)
     s = L.solver_for(cfg)
@@ -294,7 +304,16 @@ def run_ours(args, rank, world, dist):
     hbm, hbm_src = peaks()
     roof = None
     use_fft = args.fp64_transform != 'dense'
-    if dom == 'transform' and stage[dom]['timed'] and use_fft:
+    if dom == 'transform' and stage[dom]['timed'] and args.precision == 'mixed':
+        avg_ms = stage[dom]['ms'] / stage[dom]['timed']
+        S = args.slices
+        fl = transform_flops_per_launch(N) * S * (S + 1) / 2
+        ach = fl / (avg_ms * 1e-3) / 1e12
+        pk, src = tensor_peak()
+        roof = {'kernel': f'oz_gemm_kernel (tcgen05 split-BF16 transforms, {S} slices, {S * (S + 1) // 2} products)',
+                'bound': 'tensor', 'achieved': ach, 'peak': pk, 'unit': 'TFLOP/s', 'frac': ach / pk,
+                'peak_source': src, 'algorithmic_per_launch': fl, 'avg_launch_ms': avg_ms, 'traffic': None}
+    elif dom == 'transform' and stage[dom]['timed'] and use_fft:
         avg_ms = stage[dom]['ms'] / stage[dom]['timed']
         by = fft_bytes_per_launch(N)
         ach = by / (avg_ms * 1e-3) / 1e9
@@ -334,6 +353,7 @@ def run_ours(args, rank, world, dist):
                                f'{args.precision} field solvers',
                    'grid_steps': N, 'coarse_particles': s.Nc ** 2, 'fine_particles': s.Nf ** 2,
                    'precision': args.precision, 'fp64_transform': args.fp64_transform,
+                   'mixed_slices': args.slices if args.precision == 'mixed' else None,
                    'start_xi_step': x0,
                    'l2': 'flushed between timed steps (256 MiB write, outside the step events)',
                    'parallelism': f'replicas x{world}' if world > 1 else 'single GPU'},
@@ -406,6 +426,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--precision', default='fp64', choices=['fp64', 'mixed'])
     ap.add_argument('--fp64-transform', default='auto', choices=['auto', 'fft', 'dense'])
+    ap.add_argument('--slices', type=int, default=4, help='bf16 slices per operand (mixed precision)')
     ap.add_argument('--grid', type=int, default=641, choices=sorted(GRIDS))
     ap.add_argument('--pre', type=int, default=400, help='untimed steps into the beam')
     ap.add_argument('--cpu-steps', type=int, default=16, help='oracle steps for cpu_baseline')

@@ -44,10 +44,12 @@ extern "C" {
 #define LC3D_ERR_NONFINITE 4    /* device flag: non-finite or out-of-range deposit */
 #define LC3D_ERR_STATE 5        /* call order: state / const not set */
 #define LC3D_ERR_SIZE 6         /* size beyond a documented maximum */
+#define LC3D_ERR_TIMEOUT 7      /* device flag: a bounded wait in a kernel ran out */
 
 /* Precision of the field solvers. */
 #define LC3D_PREC_FP64 0        /* float64 dense-transform (DGEMM-form) solvers */
-#define LC3D_PREC_MIXED 1       /* split-BF16 tcgen05 transforms, fp32 accumulate */
+#define LC3D_PREC_MIXED 1       /* split-BF16 tcgen05 transforms, fp32 accumulate,
+                                   float64 combination; grid_steps <= 1000 */
 
 /* Float64 transform method (lc3d_params.fp64_transform). */
 #define LC3D_FP64_AUTO 0        /* FFT when 2(N-1) factors into 2, 3, 5, 7; else dense */
@@ -67,6 +69,7 @@ typedef struct lc3d_params {
     int field_solver_variant_A;
     int precision;                        /* LC3D_PREC_* */
     int fp64_transform;                   /* LC3D_FP64_* */
+    int mixed_slices;                     /* bf16 slices per operand, 1..6 (0: 4) */
 } lc3d_params;
 
 /* The xi-step state, attribute names of lcode.py:926-929. */
@@ -177,8 +180,9 @@ int lc3d_calculate_Bz(lc3d_ctx* ctx, const double* jx, const double* jy,
 #define LC3D_STAGE_RHS 3           /* field-solver right-hand sides */
 #define LC3D_STAGE_TRANSFORM 4     /* DST/DCT transform GEMMs */
 #define LC3D_STAGE_FIELD_FIN 5     /* Variant A, Bz mean, half-step averages */
-#define LC3D_STAGE_OTHER 6
-#define LC3D_NSTAGES 7
+#define LC3D_STAGE_SLICE 6          /* float64 -> bf16 operand slicing (mixed precision) */
+#define LC3D_STAGE_OTHER 7
+#define LC3D_NSTAGES 8
 
 /* Enable (1) or disable (0) CUDA-event timing of every kernel launch of
  * this context, and reset the counters. Not for use under stream capture.
@@ -192,7 +196,7 @@ int lc3d_profile(lc3d_ctx* ctx, int enable);
 int lc3d_profile_read(lc3d_ctx* ctx, long long* launches, double* ms, long long* timed);
 
 /* Read and clear the device error flag (synchronises `stream`); returns
- * LC3D_OK, LC3D_ERR_WINDOW or LC3D_ERR_NONFINITE. */
+ * LC3D_OK, LC3D_ERR_WINDOW, LC3D_ERR_NONFINITE or LC3D_ERR_TIMEOUT. */
 int lc3d_check_error(lc3d_ctx* ctx, void* stream);
 
 #ifdef __cplusplus

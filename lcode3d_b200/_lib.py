@@ -11,7 +11,7 @@ LIB_PATH = os.path.join(HERE, 'liblc3d.so')
 
 c_int, c_double, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
-OK, ERR_PARAM, ERR_CUDA, ERR_WINDOW, ERR_NONFINITE, ERR_STATE, ERR_SIZE = range(7)
+OK, ERR_PARAM, ERR_CUDA, ERR_WINDOW, ERR_NONFINITE, ERR_STATE, ERR_SIZE, ERR_TIMEOUT = range(8)
 PREC_FP64, PREC_MIXED = 0, 1
 FP64_AUTO, FP64_FFT, FP64_DENSE = 0, 1, 2
 
@@ -27,7 +27,8 @@ class Params(ctypes.Structure):
                 ('field_solver_subtraction_trick', c_double),
                 ('field_solver_variant_A', c_int),
                 ('precision', c_int),
-                ('fp64_transform', c_int)]
+                ('fp64_transform', c_int),
+                ('mixed_slices', c_int)]
 
 
 STATE_NAMES = ('x_offt', 'y_offt', 'px', 'py', 'pz', 'Ex', 'Ey', 'Ez',
@@ -73,7 +74,7 @@ SIGNATURES = [
     ('lc3d_profile_read', c_int, [P, P, P, P]),
 ]
 
-STAGES = ('move', 'deposit', 'deposit_finalize', 'rhs', 'transform', 'field_finalize', 'other')
+STAGES = ('move', 'deposit', 'deposit_finalize', 'rhs', 'transform', 'field_finalize', 'slice', 'other')
 
 
 class LC3DError(RuntimeError):

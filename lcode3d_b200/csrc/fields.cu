@@ -420,7 +420,45 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
             dst[f] = c->raw[f];
         }
     }
-    if (c->use_fft) {
+    if (c->p.precision == LC3D_PREC_MIXED) {
+        // four split-BF16 tensor-core GEMM stages (fields_mixed.cu)
+        for (int stage = 0; stage < 4; ++stage) {
+            MixedStageDesc d[6];
+            int cnt = 0;
+            for (int f = 0; f < 6; ++f) {
+                if (!on[f]) continue;
+                const FieldGeom g = geom(c, f);
+                MixedStageDesc& e = d[cnt++];
+                memset(&e, 0, sizeof(e));
+                e.field = f;
+                e.M = g.rows;
+                e.N = g.cols;
+                e.ld_data = N;
+                e.ldo = N;
+                const int fixed_L = g.type0 ? 0 : 1, fixed_RT = g.type1 ? 0 : 1;   // 0: S2, 1: C
+                switch (stage) {
+                    case 0:   // T1^T = (X R)^T
+                        e.data = c->rhs[f] + g.off; e.data_rows = g.rows; e.K = g.cols;
+                        e.data_is_a = 1; e.fixed = fixed_RT; e.out = c->t1[f]; e.transposed = 1;
+                        break;
+                    case 1:   // Z = Lambda o (L T1)
+                        e.data = c->t1[f]; e.data_rows = g.cols; e.K = g.rows;
+                        e.data_is_a = 0; e.fixed = fixed_L; e.out = c->t2[f];
+                        e.lam = g.Lam; e.ldl = g.ldLam;
+                        break;
+                    case 2:   // U^T = (Z R)^T
+                        e.data = c->t2[f]; e.data_rows = g.rows; e.K = g.cols;
+                        e.data_is_a = 1; e.fixed = fixed_RT; e.out = c->t1[f]; e.transposed = 1;
+                        break;
+                    default:  // F = L U
+                        e.data = c->t1[f]; e.data_rows = g.cols; e.K = g.rows;
+                        e.data_is_a = 0; e.fixed = fixed_L; e.out = dst[f] + g.off;
+                        break;
+                }
+            }
+            LC3D_TRY(mixed_stage(c, d, cnt, s));
+        }
+    } else if (c->use_fft) {
         // four FFT row passes, each writing its output transposed
         for (int stage = 0; stage < 4; ++stage) {
             FftRowsDesc d[6];

@@ -79,9 +79,8 @@ __device__ __forceinline__ void dft<2>(double2 (&v)[2], const double2*, int) {
     v[1] = csub(a, b);
 }
 
-// x -> -i x and x -> +i x
+// x -> -i x
 __device__ __forceinline__ double2 mul_mi(double2 a) { return make_double2(a.y, -a.x); }
-__device__ __forceinline__ double2 mul_pi(double2 a) { return make_double2(-a.y, a.x); }
 __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 
 // 3-point DFT: W = exp(-2 pi i / 3) = (c, -s) read from the twiddle table.

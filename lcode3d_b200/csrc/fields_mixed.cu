@@ -1,0 +1,571 @@
+// Mixed-precision field solvers: the dense-transform stages of
+// F = L (Lambda o (L X R)) R (see fields.cu) as split-BF16 GEMMs on the
+// 5th-generation tensor cores (tcgen05, accumulators in TMEM, operands
+// staged by TMA), accumulated in FP32 and combined in float64.
+//
+// Splitting (an Ozaki-type scheme). Every row r of an operand is scaled by a
+// power of two 2^-e_r so that |x| < 1, then written as S digit slices
+//     x 2^-e = sum_s d_s 2^-7(s+1),  d_s integer, |d_0| <= 128, |d_s| <= 64,
+// each slice d_s 2^-7(s+1) exact in bf16. For C = A B^T (both K-major):
+//     C = 2^(e_a + e_b) [ A_0 B_0^T + sum_{1 <= s+t < S} A_s B_t^T ].
+// The first product is a sum of K integers below 2^14 in units of 2^-14, so
+// its FP32 accumulation is exact while K * 128^2 < 2^24 (K < 1024); the
+// other products are 2^-7 smaller and share a second accumulator whose FP32
+// rounding is ~2^-31 of the leading term. The truncation after S slices is
+// ~2^-7S. The two accumulators are added in float64 in the epilogue.
+//
+// GEMM kernel: one 128 x 128 output tile per CTA, K in blocks of 32 (64-byte
+// rows, 64-byte swizzle), all 2S operand slices of a K block per pipeline
+// stage. Warp 0 issues TMA loads, warp 1 owns the TMEM allocation and
+// issues tcgen05.mma (128 x 128 x 16, bf16 -> f32) from one thread, warps
+// 2-5 read the two accumulators with tcgen05.ld and write float64. Every
+// mbarrier wait is bounded: on time-out the kernel raises an error flag and
+// exits its loops, and TMEM is always freed.
+//
+// Stages of one solve (rows x cols field, L = axis-0 and R = axis-1
+// transform; S2 and C are symmetric or appear as C^T^T = C, so the two
+// fixed operands are S2 and C, sliced once on the host):
+//   1. T1^T = (X R)^T     A = X       B^T = R^T     output transposed
+//   2. Z = Lam o (L T1)   A = L       B^T = T1^T
+//   3. U^T = (Z R)^T      A = Z       B^T = R^T     output transposed
+//   4. F = L U            A = L       B^T = U^T
+// The data operands are sliced by a row kernel before each stage.
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lc3d_internal.cuh"
+
+namespace {
+
+constexpr int TM = 128, TN = 128, BK = 32;                     // tile and K block
+constexpr int TILE_BYTES = TM * BK * 2;                          // 8 KiB (A and B tiles alike)
+constexpr int MAX_SLICES = 6;
+constexpr int GEMM_THREADS = 192;
+constexpr int TMEM_COLS = 256;                                   // two 128-column f32 accumulators
+constexpr int ROWS_PAD_ALIGN = 128;
+constexpr long long WAIT_LIMIT = 2000000000ll;                  // clock cycles
+
+struct OzProb {
+    CUtensorMap ta, tb;            // A slices / B^T slices, stacked [S][rows_pad][k_pad]
+    int a_rows_pad, b_rows_pad;
+    int M, N, K;                   // output M x N, reduction K
+    const int* ea;                 // per A row exponent
+    const int* eb;                 // per B^T row exponent
+    double* out;
+    int ldo, transposed;           // out[m][n] or out[n][m]
+    const double* lam;             // optional Lambda[m][n]
+    int ldl;
+    int tiles_n, tile_start;
+};
+
+struct OzBatch {
+    OzProb p[6];
+    int count, S, stages;
+    unsigned* err;
+};
+
+// ---------------------------------------------------------------------------
+// PTX wrappers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bounded wait for the phase with the given parity: false once WAIT_LIMIT
+// SM clock cycles (~1-2 s at 1-2 GHz) have passed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > WAIT_LIMIT) return false;
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// UMMA shared-memory descriptor, K-major operand in the canonical 64-byte
+// swizzled layout: 64-byte rows, 8-row groups 512 bytes apart.
+__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3fff);          // start address
+    d |= (uint64_t)1 << 16;                          // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(512 >> 4) << 32;                 // stride byte offset
+    d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
+    d |= (uint64_t)4 << 61;                          // layout: 64-byte swizzle
+    return d;
+}
+
+// Instruction descriptor: kind::f16 with bf16 A and B, f32 accumulator,
+// both operands K-major, M = 128, N = 128.
+constexpr uint32_t IDESC = (1u << 4) |               // D format f32
+                           (1u << 7) |               // A format bf16
+                           (1u << 10) |              // B format bf16
+                           ((uint32_t)(TN >> 3) << 17) |
+                           ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ double pow2(int e) {
+    return __longlong_as_double((long long)(e + 1023) << 52);   // exact for -1022 <= e <= 1023
+}
+
+// ---------------------------------------------------------------------------
+// The GEMM kernel
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_constant__ OzBatch b) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int S = b.S, NS = b.stages;
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + (size_t)NS * S * TILE_BYTES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + (size_t)NS * S * TILE_BYTES);
+    uint64_t* empty = full + NS;
+    uint64_t* done = empty + NS;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    __shared__ int s_fail;
+
+    int pi = 0;
+#pragma unroll 1
+    for (int q = 1; q < b.count; ++q)
+        if ((int)blockIdx.x >= b.p[q].tile_start) pi = q;
+    const OzProb& P = b.p[pi];
+    const int t = (int)blockIdx.x - P.tile_start;
+    const int m0 = (t / P.tiles_n) * TM, n0 = (t % P.tiles_n) * TN;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nkb = (P.K + BK - 1) / BK;
+
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        for (int i = 0; i < NS; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {   // ---- TMA producer ----
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int st = kb % NS, round = kb / NS;
+                if (round > 0 && !mbar_wait(&empty[st], (round - 1) & 1)) {
+                    s_fail = 1;
+                    break;
+                }
+                mbar_expect_tx(&full[st], 2u * S * TILE_BYTES);
+                for (int s = 0; s < S; ++s) {
+                    tma_load_2d(sA + ((size_t)st * S + s) * TILE_BYTES, &P.ta, &full[st], kb * BK,
+                                s * P.a_rows_pad + m0);
+                    tma_load_2d(sB + ((size_t)st * S + s) * TILE_BYTES, &P.tb, &full[st], kb * BK,
+                                s * P.b_rows_pad + n0);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {   // ---- MMA issuer ----
+            const uint32_t acc0 = tmem, acc1 = tmem + TN;
+            bool ok = true;
+            for (int kb = 0; kb < nkb && ok; ++kb) {
+                const int st = kb % NS, round = kb / NS;
+                if (!mbar_wait(&full[st], round & 1)) {
+                    ok = false;
+                    s_fail = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t a_base = smem_u32(sA + (size_t)st * S * TILE_BYTES);
+                const uint32_t b_base = smem_u32(sB + (size_t)st * S * TILE_BYTES);
+                bool first1 = (kb == 0);
+                for (int s = 0; s < S; ++s)
+                    for (int u = 0; s + u < S; ++u) {
+#pragma unroll
+                        for (int kk = 0; kk < BK / 16; ++kk) {
+                            const uint64_t ad = umma_desc_sw64(a_base + s * TILE_BYTES + kk * 32);
+                            const uint64_t bd = umma_desc_sw64(b_base + u * TILE_BYTES + kk * 32);
+                            if (s == 0 && u == 0) {
+                                umma_bf16(acc0, ad, bd, (kb > 0 || kk > 0) ? 1u : 0u);
+                            } else {
+                                umma_bf16(acc1, ad, bd, (first1 && kk == 0) ? 0u : 1u);
+                                if (kk == BK / 16 - 1) first1 = false;
+                            }
+                        }
+                    }
+                umma_commit(&empty[st]);   // frees the stage once these MMAs have read it
+            }
+            umma_commit(done);             // accumulators complete
+        }
+    } else {   // ---- epilogue: warps 2..5 cover TMEM lanes 32 (warp % 4) .. +31 ----
+        const int quarter = warp & 3;
+        const int row = quarter * 32 + lane;
+        const int m = m0 + row;
+        const bool ok = mbar_wait(done, 0);
+        if (!ok) s_fail = 1;
+        tc_fence_after();
+        if (ok) {
+            const double sa = (m < P.M) ? pow2(P.ea[m]) : 0.0;
+            for (int c0 = 0; c0 < TN; c0 += 32) {
+                uint32_t r0[32], r1[32];
+                const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+                tmem_ld32(tmem + lane_base + c0, r0);
+                if (S > 1) tmem_ld32(tmem + lane_base + TN + c0, r1);
+                tmem_wait_ld();
+                if (m < P.M) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int n = n0 + c0 + j;
+                        if (n >= P.N) continue;
+                        double v = (double)__uint_as_float(r0[j]);
+                        if (S > 1) v += (double)__uint_as_float(r1[j]);
+                        v *= sa * pow2(__ldg(P.eb + n));
+                        if (P.lam) v *= P.lam[(size_t)m * P.ldl + n];
+                        if (P.transposed)
+                            P.out[(size_t)n * P.ldo + m] = v;
+                        else
+                            P.out[(size_t)m * P.ldo + n] = v;
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (s_fail && threadIdx.x == 0) atomicOr(b.err, LC3D_FLAG_TIMEOUT);
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row slicing of float64 data: rows x K (ld) -> S bf16 planes
+// [S][rows_pad][k_pad] and per-row exponents. One warp per row.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int exponent_bound(double amax) {
+    // smallest e with amax < 2^e (0 for amax == 0)
+    if (!(amax > 0)) return 0;
+    const long long bits = __double_as_longlong(amax);
+    int e = (int)((bits >> 52) & 0x7ff) - 1022;
+    return e;
+}
+
+struct SliceArgs {
+    const double* in[6];
+    int ld[6], rows[6], K[6];
+    __nv_bfloat16* out[6];
+    int* e[6];
+    int row_start[7];              // prefix over problems, in rows
+    int count, S, rows_pad, k_pad;
+};
+
+__global__ void __launch_bounds__(256) slice_rows_kernel(const __grid_constant__ SliceArgs a) {
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (gw >= a.row_start[a.count]) return;
+    int q = 0;
+    while (gw >= a.row_start[q + 1]) ++q;
+    const int r = gw - a.row_start[q];
+    const double* x = a.in[q] + (size_t)r * a.ld[q];
+    const int K = a.K[q];
+    double amax = 0;
+    for (int k = lane; k < K; k += 32) amax = fmax(amax, fabs(x[k]));
+#pragma unroll
+    for (int o = 16; o; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    const int e = exponent_bound(amax);
+    if (lane == 0) a.e[q][r] = e;
+    const double scale = pow2(-e);
+    const size_t plane = (size_t)a.rows_pad * a.k_pad;
+    __nv_bfloat16* o = a.out[q] + (size_t)r * a.k_pad;
+    for (int k = lane; k < a.k_pad; k += 32) {
+        double v = k < K ? x[k] * scale : 0.0;   // |v| < 1
+        for (int s = 0; s < a.S; ++s) {
+            const double d = rint(v * 128.0);        // digit, exact
+            v = v * 128.0 - d;                       // exact remainder, |v| <= 1/2
+            o[s * plane + k] = __float2bfloat16_rn((float)(d * pow2(-7 * (s + 1))));
+        }
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct MixedState {
+    int S, stages;
+    int rows_pad, k_pad;           // common padded shape of every operand buffer
+    __nv_bfloat16* fixed[2];       // sliced S2 (M x M) and C (N x N)
+    int* efixed[2];
+    __nv_bfloat16* data[6];        // per-field data slices
+    int* edata[6];
+    CUtensorMap map_fixed[2];
+    CUtensorMap map_data[6];
+};
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+int make_map(CUtensorMap* m, void* base, int S, int rows_pad, int k_pad) {
+    auto enc = get_encode();
+    if (!enc) return LC3D_ERR_CUDA;
+    cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)S * rows_pad};
+    cuuint64_t strides[1] = {(cuuint64_t)k_pad * 2};
+    cuuint32_t box[2] = {BK, TM};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? LC3D_OK : LC3D_ERR_CUDA;
+}
+
+uint16_t bf16_bits(float f) {   // exact values only (digits times powers of two)
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return (uint16_t)(u >> 16);
+}
+
+// Slice a float64 matrix on the host exactly like slice_rows_kernel.
+void slice_host(const std::vector<double>& A, int rows, int K, int S, int rows_pad, int k_pad,
+                std::vector<uint16_t>& out, std::vector<int>& e) {
+    out.assign((size_t)S * rows_pad * k_pad, 0);
+    e.assign(rows_pad, 0);
+    for (int r = 0; r < rows; ++r) {
+        double amax = 0;
+        for (int k = 0; k < K; ++k) amax = std::fmax(amax, std::fabs(A[(size_t)r * K + k]));
+        int er = 0;
+        if (amax > 0) {
+            int ex;
+            std::frexp(amax, &ex);   // amax = f 2^ex, f in [0.5, 1)
+            er = ex;
+        }
+        e[r] = er;
+        for (int k = 0; k < K; ++k) {
+            double v = std::ldexp(A[(size_t)r * K + k], -er);
+            for (int s = 0; s < S; ++s) {
+                const double d = std::nearbyint(v * 128.0);
+                v = v * 128.0 - d;
+                out[((size_t)s * rows_pad + r) * k_pad + k] = bf16_bits((float)std::ldexp(d, -7 * (s + 1)));
+            }
+        }
+    }
+}
+
+}  // namespace
+
+int mixed_init(lc3d_ctx* c, int slices) {
+    if (slices < 1 || slices > MAX_SLICES) return LC3D_ERR_PARAM;
+    const int N = c->N, M = c->M;
+    if (N > 1000) return LC3D_ERR_SIZE;   // exactness of the leading product needs K * 128^2 < 2^24
+    MixedState* ms = new MixedState;
+    memset(ms, 0, sizeof(*ms));
+    c->mixed = ms;
+    ms->S = slices;
+    ms->rows_pad = (N + ROWS_PAD_ALIGN - 1) / ROWS_PAD_ALIGN * ROWS_PAD_ALIGN;
+    ms->k_pad = (N + 7) / 8 * 8;
+    ms->stages = 200 * 1024 / (2 * slices * TILE_BYTES);
+    if (ms->stages > 4) ms->stages = 4;
+    if (ms->stages < 2) return LC3D_ERR_PARAM;
+    // fixed transform matrices, sliced on the host
+    const long long L = N - 1;
+    std::vector<double> S2((size_t)M * M), C((size_t)N * N);
+    auto sinpi = [](long long r, long long Lq) {
+        r %= 2 * Lq;
+        if (r < 0) r += 2 * Lq;
+        double sign = 1;
+        if (r >= Lq) { r -= Lq; sign = -1; }
+        if (2 * r > Lq) r = Lq - r;
+        return sign * std::sin(M_PI * (double)r / (double)Lq);
+    };
+    for (int k = 0; k < M; ++k)
+        for (int n = 0; n < M; ++n) S2[(size_t)k * M + n] = 2 * sinpi((long long)(k + 1) * (n + 1), L);
+    for (int k = 0; k < N; ++k)
+        for (int n = 0; n < N; ++n) {
+            const long long r = ((long long)k * n) % (2 * L);
+            C[(size_t)k * N + n] = ((n == 0 || n == N - 1) ? 1.0 : 2.0) * sinpi(2 * r + L, 2 * L);
+        }
+    const size_t plane_elems = (size_t)slices * ms->rows_pad * ms->k_pad;
+    const std::vector<double>* fx[2] = {&S2, &C};
+    const int fdim[2] = {M, N};
+    for (int q = 0; q < 2; ++q) {
+        std::vector<uint16_t> sl;
+        std::vector<int> e;
+        slice_host(*fx[q], fdim[q], fdim[q], slices, ms->rows_pad, ms->k_pad, sl, e);
+        LC3D_CUDA_TRY(cudaMalloc(&ms->fixed[q], plane_elems * 2));
+        LC3D_CUDA_TRY(cudaMemcpy(ms->fixed[q], sl.data(), plane_elems * 2, cudaMemcpyHostToDevice));
+        LC3D_CUDA_TRY(cudaMalloc(&ms->efixed[q], ms->rows_pad * sizeof(int)));
+        LC3D_CUDA_TRY(cudaMemcpy(ms->efixed[q], e.data(), ms->rows_pad * sizeof(int), cudaMemcpyHostToDevice));
+        LC3D_TRY(make_map(&ms->map_fixed[q], ms->fixed[q], slices, ms->rows_pad, ms->k_pad));
+    }
+    for (int f = 0; f < 6; ++f) {
+        LC3D_CUDA_TRY(cudaMalloc(&ms->data[f], plane_elems * 2));
+        LC3D_CUDA_TRY(cudaMemset(ms->data[f], 0, plane_elems * 2));
+        LC3D_CUDA_TRY(cudaMalloc(&ms->edata[f], ms->rows_pad * sizeof(int)));
+        LC3D_CUDA_TRY(cudaMemset(ms->edata[f], 0, ms->rows_pad * sizeof(int)));
+        LC3D_TRY(make_map(&ms->map_data[f], ms->data[f], slices, ms->rows_pad, ms->k_pad));
+    }
+    const size_t smem = (size_t)ms->stages * 2 * slices * TILE_BYTES + 1024 + 256;
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return LC3D_OK;
+}
+
+void mixed_free(lc3d_ctx* c) {
+    MixedState* ms = static_cast<MixedState*>(c->mixed);
+    if (!ms) return;
+    for (int q = 0; q < 2; ++q) {
+        if (ms->fixed[q]) cudaFree(ms->fixed[q]);
+        if (ms->efixed[q]) cudaFree(ms->efixed[q]);
+    }
+    for (int f = 0; f < 6; ++f) {
+        if (ms->data[f]) cudaFree(ms->data[f]);
+        if (ms->edata[f]) cudaFree(ms->edata[f]);
+    }
+    delete ms;
+    c->mixed = nullptr;
+}
+
+// One transform stage for the fields marked in `on`: slice the data
+// operands (din[f], rows x K with ld N), then the batched GEMM.
+//   data_is_a: the data slices are the A operand (stages 1, 3), else B^T.
+int mixed_stage(lc3d_ctx* c, const MixedStageDesc* d, int count, cudaStream_t s) {
+    MixedState* ms = static_cast<MixedState*>(c->mixed);
+    if (!ms) return LC3D_ERR_STATE;
+    // 1. slice the data operands
+    SliceArgs sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.count = count;
+    sa.S = ms->S;
+    sa.rows_pad = ms->rows_pad;
+    sa.k_pad = ms->k_pad;
+    int rows = 0;
+    for (int q = 0; q < count; ++q) {
+        sa.in[q] = d[q].data;
+        sa.ld[q] = d[q].ld_data;
+        sa.rows[q] = d[q].data_rows;
+        sa.K[q] = d[q].K;
+        sa.out[q] = ms->data[d[q].field];
+        sa.e[q] = ms->edata[d[q].field];
+        sa.row_start[q] = rows;
+        rows += d[q].data_rows;
+    }
+    sa.row_start[count] = rows;
+    {
+        ProfScope ps(c, LC3D_STAGE_SLICE, s);
+        slice_rows_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(sa);
+        LC3D_CUDA_TRY(cudaGetLastError());
+    }
+    // 2. the GEMMs
+    OzBatch b;
+    memset(&b, 0, sizeof(b));
+    b.count = count;
+    b.S = ms->S;
+    b.stages = ms->stages;
+    b.err = c->err;
+    int tiles = 0;
+    for (int q = 0; q < count; ++q) {
+        OzProb& p = b.p[q];
+        const int f = d[q].field, fx = d[q].fixed;   // fixed: 0 = S2, 1 = C
+        if (d[q].data_is_a) {
+            p.ta = ms->map_data[f];
+            p.ea = ms->edata[f];
+            p.tb = ms->map_fixed[fx];
+            p.eb = ms->efixed[fx];
+        } else {
+            p.ta = ms->map_fixed[fx];
+            p.ea = ms->efixed[fx];
+            p.tb = ms->map_data[f];
+            p.eb = ms->edata[f];
+        }
+        p.a_rows_pad = p.b_rows_pad = ms->rows_pad;
+        p.M = d[q].M;
+        p.N = d[q].N;
+        p.K = d[q].K;
+        p.out = d[q].out;
+        p.ldo = d[q].ldo;
+        p.transposed = d[q].transposed;
+        p.lam = d[q].lam;
+        p.ldl = d[q].ldl;
+        p.tiles_n = (p.N + TN - 1) / TN;
+        p.tile_start = tiles;
+        tiles += ((p.M + TM - 1) / TM) * p.tiles_n;
+    }
+    const size_t smem = (size_t)ms->stages * 2 * ms->S * TILE_BYTES + 1024 + 256;
+    ProfScope ps(c, LC3D_STAGE_TRANSFORM, s);
+    oz_gemm_kernel<<<tiles, GEMM_THREADS, smem, s>>>(b);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}

@@ -59,6 +59,8 @@ int check_params(const lc3d_params* p, int* Nc, int* Nf, double* rb) {
     if (!(p->reflect_padding_steps > c + 1)) return LC3D_ERR_PARAM;       // lcode.py:944
     if (p->precision != LC3D_PREC_FP64 && p->precision != LC3D_PREC_MIXED) return LC3D_ERR_PARAM;
     if (p->fp64_transform < LC3D_FP64_AUTO || p->fp64_transform > LC3D_FP64_DENSE) return LC3D_ERR_PARAM;
+    if (p->mixed_slices < 0 || p->mixed_slices > 6) return LC3D_ERR_PARAM;
+    if (p->precision == LC3D_PREC_MIXED && N > 1000) return LC3D_ERR_SIZE;
     const int steps = N - 2 * p->plasma_padding_steps;                   // lcode.py:956
     if (steps < 2) return LC3D_ERR_PARAM;
     const int R = steps / (2 * c);                                        // lcode.py:461
@@ -238,6 +240,7 @@ void destroy(lc3d_ctx* c) {
     if (c->err) cudaFree(c->err);
     if (c->zeros) cudaFree(c->zeros);
     if (c->fft_tw) cudaFree(c->fft_tw);
+    mixed_free(c);
     if (c->prof_ev) {
         for (int k = 0; k < 2 * c->prof_cap; ++k) cudaEventDestroy(c->prof_ev[k]);
         free(c->prof_ev);
@@ -262,6 +265,7 @@ const char* lc3d_strerror(int code) {
         case LC3D_ERR_NONFINITE: return "non-finite or out-of-range density/current contribution";
         case LC3D_ERR_STATE: return "const / virt_params or state not set on the context";
         case LC3D_ERR_SIZE: return "size beyond the documented maximum";
+        case LC3D_ERR_TIMEOUT: return "a bounded wait inside a kernel ran out (tensor-core pipeline stalled)";
         default: return "unknown error";
     }
 }
@@ -323,6 +327,8 @@ int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out) {
         if (p->fp64_transform == LC3D_FP64_FFT && !c->fft_ok) rc = LC3D_ERR_PARAM;
         c->use_fft = c->fft_ok && p->fp64_transform != LC3D_FP64_DENSE;
     }
+    if (rc == LC3D_OK && p->precision == LC3D_PREC_MIXED)
+        rc = mixed_init(c, p->mixed_slices ? p->mixed_slices : 4);
 #undef LC3D_STEP
     if (rc == LC3D_OK && cudaDeviceSynchronize() != cudaSuccess) rc = LC3D_ERR_CUDA;
     if (rc != LC3D_OK) {
@@ -556,6 +562,7 @@ int lc3d_check_error(lc3d_ctx* c, void* stream) {
     if (flag) LC3D_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(unsigned), S(stream)));
     if (flag & LC3D_FLAG_WINDOW) return LC3D_ERR_WINDOW;
     if (flag & LC3D_FLAG_NONFINITE) return LC3D_ERR_NONFINITE;
+    if (flag & LC3D_FLAG_TIMEOUT) return LC3D_ERR_TIMEOUT;
     return LC3D_OK;
 }
 

@@ -10,6 +10,7 @@
 // Device error flag bits (the host maps them to LC3D_ERR_*).
 #define LC3D_FLAG_WINDOW 1u
 #define LC3D_FLAG_NONFINITE 2u
+#define LC3D_FLAG_TIMEOUT 4u
 
 #define LC3D_CUDA_TRY(expr)                                                  \
     do {                                                                     \
@@ -135,6 +136,24 @@ struct FftRowsDesc {
 int fft_init(lc3d_ctx* ctx);
 int fft_rows(lc3d_ctx* ctx, const FftRowsDesc* desc, int count, cudaStream_t s);
 int fft_plan(int P, int* rad);
+
+// Mixed-precision transform stages (fields_mixed.cu): C = A B^T with one
+// operand a sliced fixed transform matrix (0 = S2, 1 = C) and the other the
+// float64 data operand `data` (data_rows x K, row-major, ld_data), sliced
+// into the field's bf16 buffer before the GEMM.
+struct MixedStageDesc {
+    int field, fixed, data_is_a;
+    const double* data;
+    int ld_data, data_rows;
+    int M, N, K;
+    double* out;
+    int ldo, transposed;                  // out[m][n] or out[n][m]
+    const double* lam;                    // optional Lambda[m][n]
+    int ldl;
+};
+int mixed_init(lc3d_ctx* ctx, int slices);
+void mixed_free(lc3d_ctx* ctx);
+int mixed_stage(lc3d_ctx* ctx, const MixedStageDesc* d, int count, cudaStream_t s);
 // one-time per-device kernel attributes (shared-memory opt-ins)
 int particles_prepare();
 int fft_prepare(int P);

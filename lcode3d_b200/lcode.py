@@ -17,7 +17,9 @@ attribute access like the reference's. All device work runs in liblc3d.so
 Extra, optional config attributes (absent in the reference's config):
 ``lc3d_precision`` = 'fp64' (default) or 'mixed';
 ``lc3d_fp64_transform`` = 'auto' (default: FFT where 2(N-1) factors into
-2, 3, 5, 7), 'fft' or 'dense' (DGEMM-form transform matrices).
+2, 3, 5), 'fft' or 'dense' (DGEMM-form transform matrices);
+``lc3d_mixed_slices`` = bf16 slices per operand of the mixed-precision
+transforms (1..6, default 4).
 """
 import ctypes
 import math
@@ -126,6 +128,7 @@ def params_of(config):
     p.field_solver_variant_A = int(bool(config.field_solver_variant_A))
     p.precision = _precision(config)
     p.fp64_transform = _fp64_transform(config)
+    p.mixed_slices = int(getattr(config, 'lc3d_mixed_slices', 0))
     return p
 
 
@@ -236,6 +239,7 @@ def calculate_Ez(config, jx, jy):
     jx, jy = _f64(jx), _f64(jy)
     Ez = _empty(_grid(config))
     check(lib.lc3d_calculate_Ez(s.ctx, _ptr(jx), _ptr(jy), _ptr(Ez), _stream()), 'calculate_Ez')
+    s.check_device_flag('calculate_Ez')
     return Ez
 
 
@@ -251,6 +255,7 @@ def calculate_Ex_Ey_Bx_By(config, Ex_avg, Ey_avg, Bx_avg, By_avg,
     check(lib.lc3d_calculate_Ex_Ey_Bx_By(s.ctx, *[_ptr(a) for a in args],
                                          *[_ptr(o) for o in out], _stream()),
           'calculate_Ex_Ey_Bx_By')
+    s.check_device_flag('calculate_Ex_Ey_Bx_By')
     return tuple(out)
 
 
@@ -260,6 +265,7 @@ def calculate_Bz(config, jx, jy):
     jx, jy = _f64(jx), _f64(jy)
     Bz = _empty(_grid(config))
     check(lib.lc3d_calculate_Bz(s.ctx, _ptr(jx), _ptr(jy), _ptr(Bz), _stream()), 'calculate_Bz')
+    s.check_device_flag('calculate_Bz')
     return Bz
 
 

@@ -59,6 +59,7 @@ def _params(N=161, h=0.05, c=3, f=2, rpad=5, ppad=10):
     p.reflect_padding_steps, p.plasma_padding_steps = rpad, ppad
     p.field_solver_subtraction_trick, p.field_solver_variant_A, p.precision = 1.0, 1, 0
     p.fp64_transform = 0
+    p.mixed_slices = 0
     return p
 
 
@@ -96,7 +97,7 @@ def test_sizes_reject_bad_config(lib, bad):
 
 def test_strerror(lib):
     lib.lc3d_strerror.restype = ctypes.c_char_p
-    for code in range(7):
+    for code in range(8):
         assert lib.lc3d_strerror(code)
     assert b'stencil' in lib.lc3d_strerror(3)
 
