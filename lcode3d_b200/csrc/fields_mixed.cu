@@ -7,18 +7,21 @@
 // power of two 2^-e_r so that |x| < 1, then written as S digit slices
 //     x 2^-e = sum_s d_s 2^-7(s+1),  d_s integer, |d_0| <= 128, |d_s| <= 64,
 // each slice d_s 2^-7(s+1) exact in bf16. For C = A B^T (both K-major):
-//     C = 2^(e_a + e_b) [ A_0 B_0^T + sum_{1 <= s+t < S} A_s B_t^T ].
-// The first product is a sum of K integers below 2^14 in units of 2^-14, so
-// its FP32 accumulation is exact while K * 128^2 < 2^24 (K < 1024); the
-// other products are 2^-7 smaller and share a second accumulator whose FP32
-// rounding is ~2^-31 of the leading term. The truncation after S slices is
-// ~2^-7S. The two accumulators are added in float64 in the epilogue.
+//     C = 2^(e_a + e_b) sum_{s+t < S} A_s B_t^T.
+// All products of one digit level d = s + t share the unit 2^-7(d+2), and
+// per k their integer parts sum to at most 16384, 16384, 20480, 24576 for
+// d = 0, 1, 2, 3, so over K <= 682 every level sum stays below 2^24: with
+// one FP32 accumulator per level (4 x 128 TMEM columns, all of TMEM) the
+// tensor-core accumulation is EXACT for the first four levels (levels >= 4,
+// 2^-28 smaller, join the level-3 accumulator). The only error left is the
+// truncation after S slices, ~2^-7S of the row maxima; the epilogue adds the
+// level sums in float64 and applies 2^(e_a + e_b).
 //
 // GEMM kernel: one 128 x 128 output tile per CTA, K in blocks of 32 (64-byte
 // rows, 64-byte swizzle), all 2S operand slices of a K block per pipeline
 // stage. Warp 0 issues TMA loads, warp 1 owns the TMEM allocation and
 // issues tcgen05.mma (128 x 128 x 16, bf16 -> f32) from one thread, warps
-// 2-5 read the two accumulators with tcgen05.ld and write float64. Every
+// 2-5 read the four accumulators with tcgen05.ld and write float64. Every
 // mbarrier wait is bounded: on time-out the kernel raises an error flag and
 // exits its loops, and TMEM is always freed.
 //
@@ -47,7 +50,8 @@ constexpr int TM = 128, TN = 128, BK = 32;                     // tile and K blo
 constexpr int TILE_BYTES = TM * BK * 2;                          // 8 KiB (A and B tiles alike)
 constexpr int MAX_SLICES = 6;
 constexpr int GEMM_THREADS = 192;
-constexpr int TMEM_COLS = 256;                                   // two 128-column f32 accumulators
+constexpr int NACC = 4;                                          // f32 accumulators, one per digit level
+constexpr int TMEM_COLS = NACC * TN;                             // 512: all of TMEM
 constexpr int ROWS_PAD_ALIGN = 128;
 constexpr long long WAIT_LIMIT = 2000000000ll;                  // clock cycles
 
@@ -228,7 +232,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
         }
     } else if (warp == 1) {
         if (lane == 0) {   // ---- MMA issuer ----
-            const uint32_t acc0 = tmem, acc1 = tmem + TN;
+            // products of digit level s + u go to accumulator min(s + u, 3)
             bool ok = true;
             for (int kb = 0; kb < nkb && ok; ++kb) {
                 const int st = kb % NS, round = kb / NS;
@@ -240,19 +244,17 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
                 tc_fence_after();
                 const uint32_t a_base = smem_u32(sA + (size_t)st * S * TILE_BYTES);
                 const uint32_t b_base = smem_u32(sB + (size_t)st * S * TILE_BYTES);
-                bool first1 = (kb == 0);
+                unsigned fresh = (kb == 0) ? 0xfu : 0u;   // accumulators not yet written
                 for (int s = 0; s < S; ++s)
                     for (int u = 0; s + u < S; ++u) {
+                        const int lvl = min(s + u, NACC - 1);
+                        const uint32_t acc = tmem + lvl * TN;
 #pragma unroll
                         for (int kk = 0; kk < BK / 16; ++kk) {
                             const uint64_t ad = umma_desc_sw64(a_base + s * TILE_BYTES + kk * 32);
                             const uint64_t bd = umma_desc_sw64(b_base + u * TILE_BYTES + kk * 32);
-                            if (s == 0 && u == 0) {
-                                umma_bf16(acc0, ad, bd, (kb > 0 || kk > 0) ? 1u : 0u);
-                            } else {
-                                umma_bf16(acc1, ad, bd, (first1 && kk == 0) ? 0u : 1u);
-                                if (kk == BK / 16 - 1) first1 = false;
-                            }
+                            umma_bf16(acc, ad, bd, ((fresh >> lvl) & 1u) ? 0u : 1u);
+                            fresh &= ~(1u << lvl);
                         }
                     }
                 umma_commit(&empty[st]);   // frees the stage once these MMAs have read it
@@ -268,26 +270,50 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
         tc_fence_after();
         if (ok) {
             const double sa = (m < P.M) ? pow2(P.ea[m]) : 0.0;
+            const int nacc = min(S, NACC);
+            const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
             for (int c0 = 0; c0 < TN; c0 += 32) {
-                uint32_t r0[32], r1[32];
-                const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-                tmem_ld32(tmem + lane_base + c0, r0);
-                if (S > 1) tmem_ld32(tmem + lane_base + TN + c0, r1);
-                tmem_wait_ld();
-                if (m < P.M) {
+                double v[32];
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int n = n0 + c0 + j;
-                        if (n >= P.N) continue;
-                        double v = (double)__uint_as_float(r0[j]);
-                        if (S > 1) v += (double)__uint_as_float(r1[j]);
-                        v *= sa * pow2(__ldg(P.eb + n));
-                        if (P.lam) v *= P.lam[(size_t)m * P.ldl + n];
-                        if (P.transposed)
-                            P.out[(size_t)n * P.ldo + m] = v;
-                        else
-                            P.out[(size_t)m * P.ldo + n] = v;
+                for (int j = 0; j < 32; ++j) v[j] = 0.0;
+                for (int d = 0; d < nacc; ++d) {   // exact f32 level sums, added in float64
+                    uint32_t r[32];
+                    tmem_ld32(tmem + lane_base + d * TN + c0, r);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] += (double)__uint_as_float(r[j]);
+                }
+                if (P.transposed) {
+                    // out[n][m]: the lanes hold consecutive m, stores coalesce
+                    if (m < P.M) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int n = n0 + c0 + j;
+                            if (n >= P.N) continue;
+                            double x = v[j] * (sa * pow2(__ldg(P.eb + n)));
+                            if (P.lam) x *= P.lam[(size_t)m * P.ldl + n];
+                            P.out[(size_t)n * P.ldo + m] = x;
+                        }
                     }
+                } else {
+                    // out[m][n]: transpose the warp's 32 x 32 block through
+                    // shared memory (the pipeline buffers are free once the
+                    // accumulators are complete) so the lanes write
+                    // consecutive n
+                    double* stg = reinterpret_cast<double*>(smem) + (warp - 2) * 32 * 33;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = v[j];
+                    __syncwarp();
+                    const int n = n0 + c0 + lane;
+                    const double sb = (n < P.N) ? pow2(__ldg(P.eb + n)) : 0.0;
+                    for (int r = 0; r < 32; ++r) {
+                        const int mr = m0 + quarter * 32 + r;
+                        if (mr >= P.M || n >= P.N) continue;
+                        double x = stg[r * 33 + lane] * (pow2(__ldg(P.ea + mr)) * sb);
+                        if (P.lam) x *= P.lam[(size_t)mr * P.ldl + n];
+                        P.out[(size_t)mr * P.ldo + n] = x;
+                    }
+                    __syncwarp();
                 }
             }
         }
