@@ -199,6 +199,38 @@ int lc3d_profile_read(lc3d_ctx* ctx, long long* launches, double* ms, long long*
  * LC3D_OK, LC3D_ERR_WINDOW, LC3D_ERR_NONFINITE or LC3D_ERR_TIMEOUT. */
 int lc3d_check_error(lc3d_ctx* ctx, void* stream);
 
+/* ---- deposition that allocates nothing ----
+ *
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory at the point where they deposit: a host program that reserved the
+ * GPU's memory for its own pool up front and forbids further cudaMalloc,
+ * or code that must not call cudaMalloc because it synchronises the device
+ * or because a CUDA graph is being captured. It computes what lc3d_deposit
+ * computes (same kernels, bit-identical results) without a context: every
+ * input comes from the caller (virt_params as in lc3d_virt_ptrs, indices as
+ * int32), and the scratch -- fixed-point accumulators and an error word --
+ * lives in a file-scope device array sized for grids up to
+ * LC3D_NOALLOC_MAX_GRID x LC3D_NOALLOC_MAX_GRID (6.6 MB, held by every GPU
+ * that loads the library until the process exits). Larger grids return
+ * LC3D_ERR_SIZE. ro_initial may be NULL.
+ *
+ * The first call on a device looks up the array's device address and sets
+ * the kernel's shared-memory limit; make that first call before any stream
+ * capture. Each call clears the scratch it uses first; calls that overlap
+ * on the GPU (no ordering between their streams) race on the shared array.
+ * Particles whose stencil leaves the grid are skipped as in lc3d_deposit,
+ * but this entry point does not report them. */
+#define LC3D_NOALLOC_MAX_GRID 321
+int lc3d_deposit_noalloc(const lc3d_params* p, const double* ro_initial,
+        const double* x_offt, const double* y_offt,
+        const double* m, const double* q,
+        const double* px, const double* py, const double* pz,
+        const double* influence_prev, const double* influence_next,
+        const int32_t* indices_prev, const int32_t* indices_next,
+        const double* fine_grid,
+        double* out_ro, double* out_jx, double* out_jy, double* out_jz,
+        void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,6 +72,7 @@ SIGNATURES = [
     ('lc3d_check_error', c_int, [P, P]),
     ('lc3d_profile', c_int, [P, c_int]),
     ('lc3d_profile_read', c_int, [P, P, P, P]),
+    ('lc3d_deposit_noalloc', c_int, [ctypes.POINTER(Params)] + [P] * 18),
 ]
 
 STAGES = ('move', 'deposit', 'deposit_finalize', 'rhs', 'transform', 'field_finalize', 'slice', 'other')

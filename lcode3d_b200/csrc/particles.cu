@@ -19,9 +19,13 @@
 // memory, and a finalize pass converts to float64, adds the ion background
 // and clears the accumulators for the next call.
 
+#include <mutex>
+
 #include "lc3d_internal.cuh"
 
 namespace {
+
+constexpr int DEP_WORDS_PER_CELL = 8;   // accumulator planes: 4 fields x (hi, lo)
 
 // ---------------------------------------------------------------------------
 // TSC weights, lcode.py:396-418. Order MP 0P PP M0 00 P0 MM 0M PM.
@@ -502,4 +506,106 @@ int launch_deposit_finalize(const DepositFinalizeArgs& f, cudaStream_t s) {
     deposit_finalize_kernel<<<((f.n + 1) / 2 + 255) / 256, 256, 0, s>>>(f);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Deposition without any device allocation.
+//
+// Some callers cannot allocate device memory when they deposit: a host
+// program that reserved the GPU's memory up front for its own pool and
+// forbids further cudaMalloc calls, or code that must not call cudaMalloc
+// because it synchronises the device (a latency-critical loop) or is not
+// allowed at all (while a CUDA graph is being captured). Creating a
+// context (lc3d_create) allocates, so lc3d_deposit_noalloc takes every
+// input from the caller and keeps its scratch -- the fixed-point
+// accumulators and the error word -- in the file-scope device array below:
+// 8 planes of LC3D_NOALLOC_MAX_GRID^2 64-bit words (6.6 MB for 321 x 321),
+// which every GPU that loads this library holds until the process exits.
+//
+// Host code cannot use the array's name as a device address; the address
+// is looked up once per device with cudaGetSymbolAddress (with that device
+// current) on the first call made on that device, which also sets the
+// kernel's shared-memory limit. That first call must therefore come before
+// any stream capture. All calls share the array: each call clears the part
+// it uses before depositing, and calls that overlap on the GPU (different
+// streams, no ordering between them) race on it.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr size_t NOALLOC_PLANE =
+    ((size_t)LC3D_NOALLOC_MAX_GRID * LC3D_NOALLOC_MAX_GRID + 31) / 32 * 32;
+constexpr size_t NOALLOC_WORDS = DEP_WORDS_PER_CELL * NOALLOC_PLANE + 32;   // + error word (padded)
+
+}  // namespace
+
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[NOALLOC_WORDS];
+
+namespace {
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mutex;
+unsigned long long* g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+
+// Device address of g_noalloc_scratch on the current device (looked up once).
+int noalloc_scratch(unsigned long long** out) {
+    int dev = 0;
+    LC3D_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return LC3D_ERR_PARAM;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        LC3D_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        LC3D_TRY(particles_prepare());
+        g_noalloc_ptr[dev] = static_cast<unsigned long long*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return LC3D_OK;
+}
+
+}  // namespace
+
+extern "C" int lc3d_deposit_noalloc(const lc3d_params* p, const double* ro_initial, const double* x_offt,
+                                    const double* y_offt, const double* m, const double* q, const double* px,
+                                    const double* py, const double* pz, const double* influence_prev,
+                                    const double* influence_next, const int32_t* indices_prev,
+                                    const int32_t* indices_next, const double* fine_grid, double* out_ro,
+                                    double* out_jx, double* out_jy, double* out_jz, void* stream) {
+    int Nc = 0, Nf = 0;
+    double rb = 0;
+    LC3D_TRY(lc3d_sizes(p, &Nc, &Nf, &rb));
+    if (p->grid_steps > LC3D_NOALLOC_MAX_GRID) return LC3D_ERR_SIZE;
+    const void* req[] = {x_offt, y_offt, m, q, px, py, pz, influence_prev, influence_next,
+                         indices_prev, indices_next, fine_grid, out_ro, out_jx, out_jy, out_jz};
+    for (const void* r : req)
+        if (!r) return LC3D_ERR_PARAM;
+    unsigned long long* scratch = nullptr;
+    LC3D_TRY(noalloc_scratch(&scratch));
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int N = p->grid_steps;
+    const size_t plane = ((size_t)N * N + 31) / 32 * 32;
+    unsigned long long* err_word = scratch + DEP_WORDS_PER_CELL * NOALLOC_PLANE;
+    // clear the accumulators this grid uses and the error word
+    LC3D_CUDA_TRY(cudaMemsetAsync(scratch, 0, DEP_WORDS_PER_CELL * plane * sizeof(unsigned long long), s));
+    LC3D_CUDA_TRY(cudaMemsetAsync(err_word, 0, sizeof(unsigned long long), s));
+    const int c = p->plasma_coarseness, f = p->plasma_fineness;
+    DepositArgs a;
+    a.x_offt = x_offt; a.y_offt = y_offt; a.m = m; a.q = q; a.px = px; a.py = py; a.pz = pz;
+    a.inf_prev = influence_prev; a.inf_next = influence_next; a.fine_grid = fine_grid;
+    a.idx_prev = indices_prev; a.idx_next = indices_next;
+    a.acc = scratch;
+    a.plane = plane;
+    a.Nc = Nc; a.Nf = Nf; a.N = N;
+    a.h = p->grid_step_size;
+    a.inv_h = 1.0 / p->grid_step_size;
+    a.sf = 1.0 / ((double)(c * f) * (c * f));
+    a.err = reinterpret_cast<unsigned*>(err_word);
+    DepositFinalizeArgs fa;
+    fa.acc = scratch;
+    fa.plane = plane;
+    fa.ro_initial = ro_initial;
+    fa.ro = out_ro; fa.jx = out_jx; fa.jy = out_jy; fa.jz = out_jz;
+    fa.n = N * N;
+    LC3D_TRY(launch_deposit_main(a, s));
+    return launch_deposit_finalize(fa, s);
 }
