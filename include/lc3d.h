@@ -124,6 +124,41 @@ int lc3d_step_arrays(lc3d_ctx* ctx, const lc3d_state_ptrs* prev,
                      const lc3d_state_ptrs* out, const double* beam_ro,
                      void* stream);
 
+/* ---- device-side beam and graph-replayed runs ----
+ * The reference evaluates config.beam on the host and copies it to the
+ * device every step (lcode.py:1040, 839), and copies the whole Ez array back
+ * to read Ez(0,0) (lcode.py:1043-1046). For the axisymmetric driver of the
+ * benchmark configurations,
+ *   rho_b = A exp(-(x^2 + y^2) / (2 sigma_r^2)) * 0.5 (1 - cos(sqrt(pi/2) xi / L))
+ * for 0 <= xi <= 2 sqrt(2 pi) L, else 0 (xi = xi_i * xi_step_size, L the
+ * length factor), a run needs no host work: lc3d_set_beam stores the
+ * parameters (NULL: no beam), lc3d_run advances the context-owned state by
+ * nsteps steps starting at xi index xi0, each step a replay of a CUDA graph
+ * captured on first use (beam kernel, the step, Ez(N/2, N/2) appended to
+ * ez_history[k], a device array of nsteps doubles, or NULL). Not while
+ * lc3d_profile timing is enabled. */
+typedef struct lc3d_beam_params {
+    double amplitude, sigma_r, length_factor;
+} lc3d_beam_params;
+
+int lc3d_set_beam(lc3d_ctx* ctx, const lc3d_beam_params* beam);
+int lc3d_run(lc3d_ctx* ctx, int xi0, int nsteps, double* ez_history, void* stream);
+
+/* Batches of independent simulations (a parameter scan; no reference
+ * counterpart -- the reference runs one simulation per process). Each
+ * simulation is a context of its own (grid size, precision, beam and state
+ * may differ; all on one device, const and state set). lc3d_batch_run
+ * advances every simulation by nsteps steps; each step is ONE launch of a
+ * CUDA graph that holds every simulation's whole step (device beam, solver,
+ * Ez(0,0) record) on its own parallel branch. xi0[i] is simulation i's first
+ * xi index, ez_history[i] a device array of nsteps doubles (the array or
+ * its entries may be NULL). The graphs are recaptured when a context was
+ * stepped on its own or its beam changed in between. */
+typedef struct lc3d_batch lc3d_batch;
+int lc3d_batch_create(lc3d_ctx* const* ctxs, int count, lc3d_batch** out);
+int lc3d_batch_run(lc3d_batch* b, const int* xi0, int nsteps, double* const* ez_history, void* stream);
+int lc3d_batch_destroy(lc3d_batch* b);
+
 /* ---- per-stage entry points (the functions step() calls) ---- */
 
 /* move_estimate_wo_fields, lcode.py:369-391. */

@@ -50,6 +50,10 @@ class VirtPtrs(ctypes.Structure):
     _fields_ = [(n, c_void_p) for n in VIRT_NAMES]
 
 
+class BeamParams(ctypes.Structure):
+    _fields_ = [('amplitude', c_double), ('sigma_r', c_double), ('length_factor', c_double)]
+
+
 # (name, restype, argtypes) of every exported entry point
 P = c_void_p
 SIGNATURES = [
@@ -73,6 +77,11 @@ SIGNATURES = [
     ('lc3d_profile', c_int, [P, c_int]),
     ('lc3d_profile_read', c_int, [P, P, P, P]),
     ('lc3d_deposit_noalloc', c_int, [ctypes.POINTER(Params)] + [P] * 18),
+    ('lc3d_set_beam', c_int, [P, ctypes.POINTER(BeamParams)]),
+    ('lc3d_run', c_int, [P, c_int, c_int, P, P]),
+    ('lc3d_batch_create', c_int, [P, c_int, ctypes.POINTER(c_void_p)]),
+    ('lc3d_batch_run', c_int, [P, P, c_int, P, P]),
+    ('lc3d_batch_destroy', c_int, [P]),
 ]
 
 STAGES = ('move', 'deposit', 'deposit_finalize', 'rhs', 'transform', 'field_finalize', 'slice', 'other')

@@ -282,8 +282,10 @@ int fft_init(lc3d_ctx* c) {
 }
 
 int fft_prepare(int P) {
-    LC3D_CUDA_TRY(cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)fft_smem_bytes(P)));
+    // the limit is per kernel, not per context: always the largest size any
+    // context may use (contexts of different grid sizes coexist in batches)
+    (void)P;
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     return LC3D_OK;
 }
 

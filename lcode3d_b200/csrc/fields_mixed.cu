@@ -504,8 +504,11 @@ int mixed_init(lc3d_ctx* c, int slices) {
         LC3D_CUDA_TRY(cudaMemset(ms->edata[f], 0, ms->rows_pad * sizeof(int)));
         LC3D_TRY(make_map(&ms->map_data[f], ms->data[f], slices, ms->rows_pad, ms->k_pad));
     }
-    const size_t smem = (size_t)ms->stages * 2 * slices * TILE_BYTES + 1024 + 256;
-    LC3D_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // per-kernel limit: the largest pipeline any slice count uses (stages x
+    // 2S tiles <= 200 KiB) plus alignment slack and barriers, so contexts
+    // with different slice counts can coexist
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       200 * 1024 + 1024 + 256));
     return LC3D_OK;
 }
 

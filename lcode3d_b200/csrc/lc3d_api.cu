@@ -17,7 +17,7 @@ void lc3d_set_last_cuda_error(cudaError_t e, const char* what, const char* file,
 
 ProfScope::ProfScope(lc3d_ctx* c_, int cat_, cudaStream_t s_) : c(c_), cat(cat_), slot(-1), s(s_) {
     c->launches[cat]++;
-    if (c->prof_on) {
+    if (c->prof_on && !c->capturing) {
         if (c->prof_used < c->prof_cap) {
             slot = c->prof_used++;
             c->prof_cat[slot] = cat;
@@ -241,6 +241,7 @@ void destroy(lc3d_ctx* c) {
     if (c->zeros) cudaFree(c->zeros);
     if (c->fft_tw) cudaFree(c->fft_tw);
     mixed_free(c);
+    run_free(c);
     if (c->prof_ev) {
         for (int k = 0; k < 2 * c->prof_cap; ++k) cudaEventDestroy(c->prof_ev[k]);
         free(c->prof_ev);
@@ -253,6 +254,11 @@ void destroy(lc3d_ctx* c) {
 inline cudaStream_t S(void* p) { return reinterpret_cast<cudaStream_t>(p); }
 
 }  // namespace
+
+int step_schedule(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& out, const double* beam,
+                  cudaStream_t s) {
+    return run_step(c, prev, out, beam, s);
+}
 
 extern "C" {
 
@@ -323,6 +329,7 @@ int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out) {
     LC3D_STEP(particles_prepare());
     LC3D_STEP(fields_init(c));
     LC3D_STEP(fft_init(c));
+    LC3D_STEP(run_init(c));
     if (rc == LC3D_OK) {
         if (p->fp64_transform == LC3D_FP64_FFT && !c->fft_ok) rc = LC3D_ERR_PARAM;
         c->use_fft = c->fft_ok && p->fp64_transform != LC3D_FP64_DENSE;

@@ -204,4 +204,17 @@ struct lc3d_ctx {
     int* prof_cat;
     double prof_ms[LC3D_NSTAGES];
     long long prof_count[LC3D_NSTAGES];
+    // device-side beam and graph-replayed runs (run.cu)
+    int capturing;                        // a step is being captured into a graph
+    double* beam_buf;                     // N x N beam evaluated on the device
+    void* run_ctl;                        // device RunCtl: xi counter, history
+    double beam_A, beam_sr, beam_lf;      // amplitude, sigma_r, length factor
+    cudaGraphExec_t graph[2];             // one xi step from state parity 0 / 1
+    long long graph_launches[2][LC3D_NSTAGES];
 };
+
+// The xi-step schedule (lc3d_api.cu), and the run machinery (run.cu).
+int step_schedule(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& out, const double* beam,
+                  cudaStream_t s);
+int run_init(lc3d_ctx* c);
+void run_free(lc3d_ctx* c);

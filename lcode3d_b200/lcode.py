@@ -411,6 +411,65 @@ def step(config, const, virt_params, prev, beam_ro):
     return new
 
 
+def run(config, const, virt_params, state, xi0, nsteps, beam=None):
+    """Advance ``state`` by ``nsteps`` xi steps starting at xi index ``xi0``
+    with the beam evaluated on the device, each step a CUDA-graph replay
+    (lc3d_run). ``beam`` = (amplitude, sigma_r, length_factor) of the
+    axisymmetric driver rho_b = A exp(-r^2 / (2 sigma_r^2)) 0.5
+    (1 - cos(sqrt(pi/2) xi / L)) on 0 <= xi <= 2 sqrt(2 pi) L, or None for no
+    beam. Returns (new state, Ez(N/2, N/2) after every step as a device
+    tensor). Replaces the reference's host loop (lcode.py:1039-1046) for
+    this beam shape; ``prev`` is not modified."""
+    s = solver_for(config)
+    s.set_virt(virt_params)
+    s.set_const(const)
+    g = _grid(config)
+    shape_p = tuple(state.x_offt.shape)
+    src = [_f64(getattr(state, n), shape_p if k < 5 else g) for k, n in enumerate(_lib.STATE_NAMES)]
+    check(lib.lc3d_set_state(s.ctx, ctypes.byref(_lib.StatePtrs(*[t.data_ptr() for t in src])), _stream()),
+          'lc3d_set_state')
+    bp = None
+    if beam is not None:
+        bp = _lib.BeamParams(*[float(v) for v in beam])
+    check(lib.lc3d_set_beam(s.ctx, ctypes.byref(bp) if bp is not None else None), 'lc3d_set_beam')
+    ez = _empty((max(int(nsteps), 1),))
+    check(lib.lc3d_run(s.ctx, int(xi0), int(nsteps), _ptr(ez), _stream()), 'lc3d_run')
+    out = {n: _empty(shape_p if k < 5 else g) for k, n in enumerate(_lib.STATE_NAMES)}
+    check(lib.lc3d_get_state(s.ctx, ctypes.byref(_lib.StatePtrs(*[out[n].data_ptr() for n in _lib.STATE_NAMES])),
+                             _stream()), 'lc3d_get_state')
+    s.check_device_flag('run')
+    new = GPUArrays.__new__(GPUArrays)
+    for n in _lib.STATE_NAMES:
+        setattr(new, n, out[n])
+    return new, ez[:nsteps]
+
+
+# ---------------------------------------------------------------------------
+# Checkpoint / resume: the arrays of const, virt_params and state under the
+# reference's attribute names (lcode.py:926-929, 964-965, 566-570)
+# ---------------------------------------------------------------------------
+
+def save_checkpoint(path, xi_i, const, virt_params, state):
+    """Write ``xi_i`` (the next xi index) and all arrays to an .npz file."""
+    arrs = {'xi_i': np.array(int(xi_i))}
+    for prefix, group, names in (('const_', const, _lib.CONST_NAMES),
+                                 ('virt_', virt_params, _lib.VIRT_NAMES),
+                                 ('state_', state, _lib.STATE_NAMES)):
+        for n in names:
+            arrs[prefix + n] = getattr(group, n).detach().cpu().numpy()
+    np.savez(path, **arrs)
+
+
+def load_checkpoint(path):
+    """Read a file written by ``save_checkpoint``: (xi_i, const, virt_params,
+    state) with device arrays, ready for ``step``."""
+    with np.load(path) as f:
+        const = GPUArrays(**{n: f['const_' + n] for n in _lib.CONST_NAMES})
+        virt = GPUArrays(**{n: f['virt_' + n] for n in _lib.VIRT_NAMES})
+        state = GPUArrays(**{n: f['state_' + n] for n in _lib.STATE_NAMES})
+        return int(f['xi_i']), const, virt, state
+
+
 def init(config):
     """Check the config, set config.reflect_boundary, lay out the plasma and
     deposit the ion background (lcode.py:936-975)."""

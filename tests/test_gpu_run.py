@@ -1,0 +1,99 @@
+"""Graph-replayed runs with the device-side beam, checkpoint/resume, and
+batches of simulations, against the per-step drop-in path."""
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip('torch')
+
+from make_golden import beam_array, make_config  # noqa: E402
+from oracle import lcode_oracle as O  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+STATE = ('x_offt', 'y_offt', 'px', 'py', 'pz', 'Ex', 'Ey', 'Ez', 'Bx', 'By', 'Bz', 'ro', 'jx', 'jy', 'jz')
+
+
+def rel(a, b):
+    return O.relative_error(a.cpu().numpy() if isinstance(a, torch.Tensor) else a,
+                            b.cpu().numpy() if isinstance(b, torch.Tensor) else b)
+
+
+@pytest.fixture(scope='module')
+def L():
+    if not torch.cuda.is_available():
+        pytest.skip('no GPU')
+    import lcode3d_b200 as L
+    L.lcode.check_errors = True
+    return L
+
+
+def test_run_matches_host_loop(L):
+    """lc3d_run (device beam, graph replay, device Ez history) against the
+    reference-style host loop of step() with the beam from numpy; the two
+    beams differ by rounding of exp/cos only."""
+    cfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    xs, ys, const, virt, st0 = L.init(cfg)
+    st, ez_host = st0, []
+    for i in range(60):
+        st = L.step(cfg, const, virt, st, beam_array(cfg, i, xs, ys))
+        ez_host.append(float(st.Ez[80, 80]))
+    got, ez = L.lcode.run(cfg, const, virt, st0, 0, 60, beam=(0.05, 1.0, 1.0))
+    assert rel(ez, np.array(ez_host)) < 1e-12
+    for k in STATE:
+        assert rel(getattr(got, k), getattr(st, k)) < 1e-11, k
+    # the same 60 steps as 25 + 35 (both state parities)
+    a, ez_a = L.lcode.run(cfg, const, virt, st0, 0, 25, beam=(0.05, 1.0, 1.0))
+    b, ez_b = L.lcode.run(cfg, const, virt, a, 25, 35, beam=(0.05, 1.0, 1.0))
+    assert torch.equal(torch.cat([ez_a, ez_b]), ez)
+    for k in STATE:
+        assert torch.equal(getattr(b, k), getattr(got, k)), k
+
+
+def test_checkpoint_resume(L, tmp_path):
+    cfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    xs, ys, const, virt, st = L.init(cfg)
+    for i in range(20):
+        st = L.step(cfg, const, virt, st, beam_array(cfg, i, xs, ys))
+    path = os.path.join(tmp_path, 'ck.npz')
+    L.lcode.save_checkpoint(path, 20, const, virt, st)
+    straight = st
+    for i in range(20, 30):
+        straight = L.step(cfg, const, virt, straight, beam_array(cfg, i, xs, ys))
+    xi, c2, v2, s2 = L.lcode.load_checkpoint(path)
+    assert xi == 20
+    for i in range(20, 30):
+        s2 = L.step(cfg, c2, v2, s2, beam_array(cfg, i, xs, ys))
+    for k in STATE:
+        assert torch.equal(getattr(s2, k), getattr(straight, k)), k
+
+
+def test_batch_matches_individual_runs(L):
+    """Four simulations of two grid sizes advanced by one graph launch per
+    step give bit-identical results to running each on its own."""
+    from lcode3d_b200 import batch as B
+    specs = [dict(grid_steps=N, grid_step_size=16.0 / (N - 1), xi_step_size=0.01, amplitude=A,
+                  sigma_r=sr, length_factor=lf)
+             for N, A, sr, lf in ((161, 0.3, 1.0, 1.0), (321, 0.05, 0.7, 1.3), (161, 0.8, 1.5, 0.6),
+                                  (321, 0.5, 1.0, 1.0))]
+    bt = B.Batch(specs)
+    hist = [h.clone() for h in bt.run(30)]
+    hist2 = bt.run(15)
+    bt.check_errors()
+    for i, spec in enumerate(specs):
+        cfg = B.make_config(spec)
+        xs, ys, const, virt, st0 = L.init(cfg)
+        beam = (spec['amplitude'], spec['sigma_r'], spec['length_factor'])
+        st, ez = L.lcode.run(cfg, const, virt, st0, 0, 45, beam=beam)
+        assert torch.equal(torch.cat([hist[i], hist2[i]]), ez), i
+        final = bt.sims[i].state()
+        for k in STATE:
+            assert torch.equal(getattr(final, k), getattr(st, k)), (i, k)
+
+
+def test_autotuner_picks_a_form(L):
+    from lcode3d_b200 import batch as B
+    choice, timings = B.autotune_transform([161], steps=3)
+    assert choice[161] in ('fft', 'dense')
+    assert set(timings[161]) == {'fft', 'dense'} and all(v > 0 for v in timings[161].values())
