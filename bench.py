@@ -297,6 +297,27 @@ def run_ours(args, rank, world, dist):
     L.lcode.check_errors = True
     s.check_device_flag('e2e')
 
+    # ---- the same steps as CUDA-graph replays (lc3d_run, device beam) ----
+    bp = _lib.BeamParams(GRIDS[args.grid][2], 1.0, 1.0)
+    _lib.check(lib.lc3d_set_beam(s.ctx, ctypes.byref(bp)), 'set_beam')
+    ezh = torch.empty(W + K, dtype=torch.float64, device='cuda')
+    xg = x0 + W + K   # the context state has advanced by W + K steps
+    _lib.check(lib.lc3d_run(s.ctx, xg, W, ctypes.c_void_p(ezh.data_ptr()), sp), 'graph warmup')
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    _lib.check(lib.lc3d_run(s.ctx, xg + W, K, ctypes.c_void_p(ezh.data_ptr()), sp), 'graph run')
+    g1.record(stream)
+    torch.cuda.synchronize()
+    graph_ms = g0.elapsed_time(g1)
+    if dist:
+        t = torch.tensor([graph_ms], dtype=torch.float64, device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        graph_ms = float(t)
+    _lib.check(lib.lc3d_check_error(s.ctx, sp), 'graph run')
+
     if rank != 0:
         return None
     # ---- roofline of the dominant kernel ----
@@ -366,6 +387,9 @@ def run_ours(args, rank, world, dist):
         'roofline': roof,
         'clocks': clk,
         'pre_steps_seconds': t_pre,
+        'graph': {'value': world * K / (graph_ms * 1e-3), 'ms_per_step': graph_ms / K,
+                  'how': 'the same K steps as one lc3d_run: CUDA-graph replay per step, beam evaluated '
+                         'on the device, Ez(0,0) recorded on the device, no L2 flush between steps'},
     }
     return out
 
@@ -391,6 +415,70 @@ def cpu_threads():
         return len(os.sched_getaffinity(0))
     except AttributeError:
         return os.cpu_count() or 1
+
+
+def run_scan(args, rank, world, dist):
+    """Batched parameter scan: args.scan simulations drawn (seeded) over the
+    grids 161/321/481/641 with the window kept at +-8, dxi = 0.01, beam
+    amplitude log-uniform [0.01, 1], sigma_r U[0.5, 2], length factor
+    U[0.5, 1.5]; partitioned over ranks by cost, each rank's share advanced
+    with one CUDA-graph launch per xi step. value = all simulations' steps /
+    the slowest rank's time."""
+    import torch
+    from lcode3d_b200 import batch as B
+
+    torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+    specs = B.scan_specs(args.scan, args.seed)
+    mine = B.partition(specs, world)[rank]
+    grids = sorted({specs[i]['grid_steps'] for i in mine})
+    choice, timings = B.autotune_transform(grids, steps=4)
+    bt = B.Batch([specs[i] for i in mine], transform=choice)
+    K, W = args.steps, args.warmup
+    bt.run(W)
+    from lcode3d_b200 import _lib
+
+    def read_launches():   # kernel launches counted by every context since the last read
+        n = len(_lib.STAGES)
+        tot = 0
+        for sim in bt.sims:
+            arr = (ctypes.c_longlong * n)()
+            _lib.lib.lc3d_profile_read(sim.solver.ctx, arr, None, None)
+            tot += sum(arr)
+        return tot
+    read_launches()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(int(os.environ.get('LOCAL_RANK', 0)))
+    clocks.start()
+    e0.record(stream)
+    hist = bt.run(K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = read_launches()
+    bt.check_errors()
+    ms = B.max_over_ranks(e0.elapsed_time(e1), dist)
+    last = B.gather_histories({i: h[-1:].cpu().numpy() for i, h in zip(mine, hist)}, dist)
+    if rank != 0:
+        return None
+    counts = {N: sum(1 for s in specs if s['grid_steps'] == N) for N in B.GRIDS}
+    return {
+        'metric': 'aggregate xi-steps/s (batched scan)', 'value': len(specs) * K / (ms * 1e-3),
+        'unit': 'xi-steps/s', 'n_gpus': world, 'steps': K, 'warmup': W, 'ms_per_step': ms / K,
+        'higher_is_better': True, 'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f64',
+        'data': 'synthetic (seeded scan draws, generated plasma and beams)',
+        'config': {'workload': f'{len(specs)} independent simulations, grids {counts}, window +-8, dxi 0.01',
+                   'seed': args.seed, 'l2': 'no flush (each batch step touches several GB, far more than L2)'},
+        'autotune': {'choice': {str(k): v for k, v in choice.items()},
+                     'ms_per_step': {str(k): v for k, v in timings.items()}},
+        'gpu_launches': launches,
+        'launches_per_batch_step': launches / K,
+        'all_final_Ez00_finite': bool(all(np.isfinite(v).all() for v in last.values())),
+        'clocks': clk,
+    }
 
 
 def run_reference(args):
@@ -431,6 +519,9 @@ def main():
     ap.add_argument('--pre', type=int, default=400, help='untimed steps into the beam')
     ap.add_argument('--cpu-steps', type=int, default=16, help='oracle steps for cpu_baseline')
     ap.add_argument('--ref-max-steps', type=int, default=40)
+    ap.add_argument('--scan', type=int, default=0,
+                    help='batched parameter scan of this many simulations instead of the single-grid workload')
+    ap.add_argument('--seed', type=int, default=2025, help='seed of the scan draws')
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == 'ours':
         args.warmup = 3
@@ -448,6 +539,14 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+    if args.scan:
+        out = run_scan(args, rank, world, dist)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     out = run_ours(args, rank, world, dist)
     if rank == 0:
         threads = 1
