@@ -9,16 +9,19 @@
 //     DST-I: Z = -i X_a + X_b (Y imaginary)   -> X_a = -Im Z[k+1], X_b = Re Z[k+1]
 // (unnormalised, the conventions of scipy's dct/dst type 1, so DST-I = S2 x
 // and DCT-I = C x of the dense-transform form). The FFT is an
-// in-place decimation-in-frequency FFT with mixed radices 4, 2, 3, 5 in
-// shared memory, read out in digit-reversed order. Every launch transforms rows and writes its output
-// TRANSPOSED (out[k][r]), optionally scaled by Lambda[k][r]; the 2-D solve
-// F = L (Lambda o (L X R)) R is then four such passes:
-//     A: rows of X by the axis-1 transform          -> T1^T
-//     B: rows of T1^T by the axis-0 transform, x Lambda -> Z
-//     C: rows of Z by the axis-1 transform          -> T3^T
-//     D: rows of T3^T by the axis-0 transform       -> F
+// in-place decimation-in-frequency FFT with mixed radices 8, 4, 2, 3, 5 in
+// shared memory (P = 1280: 8, 8, 4, 5), read out in digit-reversed order
+// through a position-sorted list. Every launch transforms rows, optionally
+// scaled on input by Lambda[r][j], and writes its output TRANSPOSED
+// (out[k][r]); the 2-D solve F = L (Lambda o (L X R)) R is then four such
+// passes:
+//     A: rows of X by the axis-1 transform                 -> T1^T
+//     B: rows of T1^T by the axis-0 transform              -> Z
+//     C: rows of Lambda o Z by the axis-1 transform        -> T3^T
+//     D: rows of T3^T by the axis-0 transform              -> F
 // One launch covers all fields of a solve.
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -30,7 +33,14 @@ namespace {
 constexpr int FFT_THREADS = 256;
 constexpr int FFT_PER_CTA = 2;           // complex FFTs per CTA (4 rows)
 constexpr int ROWS_PER_CTA = 2 * FFT_PER_CTA;
+#ifndef LC3D_FFT_MAX_RADIX
+#define LC3D_FFT_MAX_RADIX 8              // largest power-of-two butterfly in a plan (8 or 4)
+#endif
+#ifndef LC3D_FFT_MIN_BLOCKS
+#define LC3D_FFT_MIN_BLOCKS 3             // resident CTAs per SM the registers allow
+#endif
 constexpr int MAX_RADICES = 24;
+constexpr int FFT_PAD = 4;               // double2 words between the CTA's two FFTs (bank offset)
 
 struct FftField {
     const double* in;
@@ -48,7 +58,7 @@ struct FftBatch {
     int nrad;
     int rad[MAX_RADICES];
     const double2* tw;                   // tw[m] = exp(-2 pi i m / P)
-    const int* pos;                      // position of frequency k after the DIF passes
+    const int* rd;                       // readout lists: DCT-I (N entries), then DST-I (N - 2)
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -127,13 +137,44 @@ __device__ __forceinline__ void dft<4>(double2 (&v)[4], const double2*, int) {
     v[3] = csub(a1, a3);
 }
 
+// 8-point DFT as 2 x 4: a_j = v_j + v_{j+4}, b_j = (v_j - v_{j+4}) W8^j,
+// X_2k = DFT4(a)_k, X_2k+1 = DFT4(b)_k. Outputs are left in register order
+// (X_0 X_2 X_4 X_6 X_1 X_3 X_5 X_7); dft_out<8> maps register -> frequency.
+template <>
+__device__ __forceinline__ void dft<8>(double2 (&v)[8], const double2* tw, int P) {
+    double2 a[4], b[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        a[j] = cadd(v[j], v[j + 4]);
+        const double2 d = csub(v[j], v[j + 4]);
+        b[j] = j ? cmul(d, __ldg(tw + j * (P / 8))) : d;
+    }
+    dft<4>(a, tw, P);
+    dft<4>(b, tw, P);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        v[j] = a[j];
+        v[j + 4] = b[j];
+    }
+}
+
+// Frequency held in register r after dft<R>.
+template <int R>
+__device__ __forceinline__ constexpr int dft_out(int r) {
+    return R == 8 ? (r < 4 ? 2 * r : 2 * (r - 4) + 1) : r;
+}
+
 // One in-place decimation-in-frequency butterfly of radix R inside a
 // sub-transform of length Lr = R * span: the R inputs A[base + r span] are
 // transformed and output m is scaled by exp(-2 pi i m k / Lr), k the
 // position inside the span, and written back in place. After all passes
 // frequency k = m0 + R0 (m1 + R1 (m2 + ...)) sits at sum_s m_s P / (R0..Rs).
+//
+// The twiddles w^m, w = exp(-2 pi i k / Lr), are one table load and a
+// product tree w^m = w^(m/2) w^(m - m/2) (at most three roundings deep for
+// R <= 8), which keeps the R - 1 scattered table loads off the L1 pipe.
 template <int R>
-__device__ __forceinline__ void dif_butterfly(double2* A, int b, int span, float inv_span, int P,
+__device__ __forceinline__ void dif_butterfly(double2* A, int b, int span, float inv_span, int tstep, int P,
                                               const double2* __restrict__ tw) {
     // g = b / span: (b + 0.5) / span lies at least 0.5 / span from an
     // integer, far more than the float rounding for b, span < 2^16
@@ -142,12 +183,16 @@ __device__ __forceinline__ void dif_butterfly(double2* A, int b, int span, float
     double2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = A[base + r * span];
+    double2 w[R];
+    w[1] = __ldg(tw + k * tstep);
+#pragma unroll
+    for (int m = 2; m < R; ++m) w[m] = cmul(w[m / 2], w[m - m / 2]);
     dft<R>(v, tw, P);
-    const int tstep = P / (span * R);
 #pragma unroll
-    for (int m = 1; m < R; ++m) v[m] = cmul(v[m], __ldg(tw + m * k * tstep));
-#pragma unroll
-    for (int m = 0; m < R; ++m) A[base + m * span] = v[m];
+    for (int r = 0; r < R; ++r) {
+        const int m = dft_out<R>(r);   // frequency in register r
+        A[base + m * span] = m ? cmul(v[r], w[m]) : v[r];
+    }
 }
 
 template <int R>
@@ -155,50 +200,74 @@ __device__ __forceinline__ void fft_pass(double2* A, int span, int P, const doub
     static_assert(FFT_PER_CTA == 2, "the FFT index below assumes two FFTs per CTA");
     const int nb = P / R;
     const float inv_span = 1.0f / (float)span;
+    const int tstep = P / (span * R);   // twiddle stride of this pass
     for (int t = threadIdx.x; t < FFT_PER_CTA * nb; t += FFT_THREADS) {
         const int q = t >= nb, j = t - q * nb;
-        dif_butterfly<R>(A + q * P, j, span, inv_span, P, tw);
+        dif_butterfly<R>(A + q * (P + FFT_PAD), j, span, inv_span, tstep, P, tw);
     }
 }
 
-__global__ void __launch_bounds__(FFT_THREADS, 3) fft_rows_kernel(const __grid_constant__ FftBatch b) {
-    extern __shared__ double2 sm[];      // [FFT_PER_CTA][P], transformed in place
+__global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_kernel(const __grid_constant__ FftBatch b) {
+    extern __shared__ double2 sm[];      // FFT q at sm + q (P + FFT_PAD), transformed in place
     int fi = 0;
 #pragma unroll 1
     for (int q = 1; q < b.count; ++q)
         if ((int)blockIdx.x >= b.f[q].cta_start) fi = q;
     const FftField& F = b.f[fi];
-    const int P = b.P, L = P / 2;
+    const int P = b.P, L = P / 2, PS = P + FFT_PAD;
     const int r0 = ((int)blockIdx.x - F.cta_start) * ROWS_PER_CTA;
     const int n = F.type ? b.N - 2 : b.N;     // input / output length
     double2* A = sm;
 
-    // symmetric / antisymmetric extensions, two rows per complex FFT
-    for (int t = threadIdx.x; t < FFT_PER_CTA * P; t += FFT_THREADS) {
-        const int q = t >= P, m = t - q * P;
-        double v[2];
+    // symmetric / antisymmetric extensions, rows 2q and 2q + 1 of the CTA
+    // as the real and imaginary parts of FFT q, each input element (scaled
+    // by Lambda[row][j] when given) loaded once and written to its one or
+    // two positions. All loads of a batch are issued before the first use.
+    constexpr int LU = 2;
+    for (int j0 = 0; j0 < n; j0 += LU * FFT_THREADS) {
+        double x[ROWS_PER_CTA][LU];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int row = r0 + 2 * q + h;
-            double x = 0;
-            if (row < F.rows) {
-                const double* rp = F.in + (size_t)row * F.ld_in;
-                if (F.type == 0) {
-                    x = __ldg(rp + (m <= L ? m : P - m));
-                } else if (m != 0 && m != L) {
-                    x = m < L ? __ldg(rp + m - 1) : -__ldg(rp + P - m - 1);
+        for (int rr = 0; rr < ROWS_PER_CTA; ++rr) {
+            const int row = r0 + rr;
+            const double* rp = F.in + (size_t)row * F.ld_in;
+            const double* lp = F.lam ? F.lam + (size_t)row * F.ld_lam : nullptr;
+#pragma unroll
+            for (int u = 0; u < LU; ++u) {
+                const int j = j0 + u * FFT_THREADS + (int)threadIdx.x;
+                const bool ok = row < F.rows && j < n;
+                x[rr][u] = ok ? __ldg(rp + j) : 0.0;
+                if (F.lam) x[rr][u] *= ok ? __ldg(lp + j) : 0.0;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < FFT_PER_CTA; ++q) {
+            double2* a = A + q * PS;
+#pragma unroll
+            for (int u = 0; u < LU; ++u) {
+                const int j = j0 + u * FFT_THREADS + (int)threadIdx.x;
+                if (j >= n) continue;
+                const double2 z = make_double2(x[2 * q][u], x[2 * q + 1][u]);
+                if (F.type == 0) {           // m = j and P - j
+                    a[j] = z;
+                    if (j > 0 && j < L) a[P - j] = z;
+                } else {                     // m = j + 1 and P - j - 1, negated
+                    a[j + 1] = z;
+                    a[P - j - 1] = make_double2(-z.x, -z.y);
                 }
             }
-            v[h] = x;
         }
-        A[t] = make_double2(v[0], v[1]);
     }
+    if (F.type == 1 && threadIdx.x < 2 * FFT_PER_CTA)   // DST-I: zeros at m = 0 and m = L
+        A[(threadIdx.x >> 1) * PS + (threadIdx.x & 1) * L] = make_double2(0.0, 0.0);
     __syncthreads();
     int span = P;
     for (int p = 0; p < b.nrad; ++p) {
         const int R = b.rad[p];
         span /= R;
         switch (R) {
+#if LC3D_FFT_MAX_RADIX >= 8
+            case 8: fft_pass<8>(A, span, P, b.tw); break;
+#endif
             case 4: fft_pass<4>(A, span, P, b.tw); break;
             case 2: fft_pass<2>(A, span, P, b.tw); break;
             case 3: fft_pass<3>(A, span, P, b.tw); break;
@@ -206,21 +275,30 @@ __global__ void __launch_bounds__(FFT_THREADS, 3) fft_rows_kernel(const __grid_c
         }
         __syncthreads();
     }
-    // transposed output, 4 consecutive rows per output index k; frequency
-    // kk sits at its digit-reversed position
-    const int off = F.type;   // DST-I outputs are Z[1 .. L-1]
-    for (int t = threadIdx.x; t < n * ROWS_PER_CTA; t += FFT_THREADS) {
-        const int k = t / ROWS_PER_CTA, rr = t - k * ROWS_PER_CTA;
-        const int row = r0 + rr;
-        if (row >= F.rows) continue;
-        const double2 z = A[(rr >> 1) * P + __ldg(b.pos + k + off)];
-        double x;
-        if (F.type == 0)
-            x = (rr & 1) ? z.y : z.x;
-        else
-            x = (rr & 1) ? z.x : -z.y;
-        if (F.lam) x *= F.lam[(size_t)k * F.ld_lam + row];
-        F.out[(size_t)k * F.ld_out + row] = x;
+    // transposed output: out[k][row] for the CTA's rows. The readout list
+    // holds (position, k) for the wanted frequencies sorted by position, so
+    // a warp reads nearly consecutive shared-memory words; thread pairs
+    // (FFT 0, FFT 1) of one entry write 4 consecutive rows of out[k].
+    const int* rl = b.rd + (F.type ? b.N : 0);
+    const int total = n * FFT_PER_CTA;
+    constexpr int SU = 8;
+    for (int t0 = 0; t0 < total; t0 += SU * FFT_THREADS) {
+        int e[SU];
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            const int t = t0 + u * FFT_THREADS + (int)threadIdx.x;
+            e[u] = t < total ? __ldg(rl + (t >> 1)) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            const int t = t0 + u * FFT_THREADS + (int)threadIdx.x;
+            const int q = t & 1, row = r0 + 2 * q;
+            if (t >= total || row >= F.rows) continue;
+            const double2 z = A[q * PS + (e[u] >> 16)];
+            double* o = F.out + (size_t)(e[u] & 0xffff) * F.ld_out + row;
+            o[0] = F.type == 0 ? z.x : -z.y;
+            if (row + 1 < F.rows) o[1] = F.type == 0 ? z.y : z.x;
+        }
     }
 }
 
@@ -235,47 +313,59 @@ double sin_pi_frac(long long r, long long L) {
 
 }  // namespace
 
-// Radix plan for a length-P FFT: factors 4, 2, 3, 5 (powers of 4 first).
+// Radix plan for a length-P FFT: factors 8, 4, 2, 3, 5 (largest powers of
+// two first, each a register butterfly).
 // Returns the number of passes, or 0 if P has another prime factor (the
 // dense transform form is used then).
 int fft_plan(int P, int* rad) {
     int n = 0;
     int r = P;
-    while (r % 4 == 0 && n < MAX_RADICES) { rad[n++] = 4; r /= 4; }
-    const int others[] = {2, 3, 5};
+    const int others[] = {8, 4, 2, 3, 5};
     for (int f : others)
-        while (r % f == 0 && n < MAX_RADICES) { rad[n++] = f; r /= f; }
+        while ((f <= LC3D_FFT_MAX_RADIX || f % 2) && r % f == 0 && n < MAX_RADICES) { rad[n++] = f; r /= f; }
     return (r == 1) ? n : 0;
 }
 
-size_t fft_smem_bytes(int P) { return (size_t)FFT_PER_CTA * P * sizeof(double2); }
+size_t fft_smem_bytes(int P) { return ((size_t)FFT_PER_CTA * P + (FFT_PER_CTA - 1) * FFT_PAD) * sizeof(double2); }
 
 int fft_init(lc3d_ctx* c) {
-    const int P = 2 * (c->N - 1);
+    const int N = c->N, P = 2 * (N - 1);
     int rad[MAX_RADICES];
     c->fft_ok = fft_plan(P, rad) > 0 && fft_smem_bytes(P) <= 200 * 1024;
     if (!c->fft_ok) return LC3D_OK;
     LC3D_TRY(fft_prepare(P));
     const int nrad = fft_plan(P, rad);
-    // P twiddles exp(-2 pi i m / P), then P int32 positions: frequency k of
-    // the in-place DIF output sits at pos[k] = sum_s m_s P / (R0..Rs) for the
-    // mixed-radix digits k = m0 + R0 (m1 + R1 (...))
-    std::vector<double> buf(3 * (size_t)P);
+    // P twiddles exp(-2 pi i m / P), then the two readout lists. Frequency k
+    // of the in-place DIF output sits at pos(k) = sum_s m_s P / (R0..Rs) for
+    // the mixed-radix digits k = m0 + R0 (m1 + R1 (...)); a list holds
+    // (pos << 16) | output index for the frequencies a transform keeps
+    // (DCT-I: k = 0 .. N-1 -> output k; DST-I: k = 1 .. N-2 -> output k - 1),
+    // sorted by position.
+    auto pos = [&](int k) {
+        int p = 0, rem = P;
+        for (int s = 0; s < nrad; ++s) {
+            const int m = k % rad[s];
+            k /= rad[s];
+            rem /= rad[s];
+            p += m * rem;
+        }
+        return p;
+    };
+    // P <= 6400 under the shared-memory limit above: positions fit 16 bits
+    std::vector<int32_t> rd;
+    for (int type = 0; type < 2; ++type) {
+        std::vector<int32_t> l;
+        const int n = type ? N - 2 : N;
+        for (int o = 0; o < n; ++o) l.push_back((pos(o + type) << 16) | o);
+        std::sort(l.begin(), l.end());
+        rd.insert(rd.end(), l.begin(), l.end());
+    }
+    std::vector<double> buf(2 * (size_t)P + (rd.size() + 1) / 2);
     for (int m = 0; m < P; ++m) {
         buf[2 * m] = sin_pi_frac(4LL * m + P, 2LL * P);      // cos(pi (2m) / P)
         buf[2 * m + 1] = -sin_pi_frac(2LL * m, (long long)P);
     }
-    int32_t* pos = reinterpret_cast<int32_t*>(buf.data() + 2 * (size_t)P);
-    for (int k = 0; k < P; ++k) {
-        int kk = k, p = 0, rem = P;
-        for (int s = 0; s < nrad; ++s) {
-            const int m = kk % rad[s];
-            kk /= rad[s];
-            rem /= rad[s];
-            p += m * rem;
-        }
-        pos[k] = p;
-    }
+    memcpy(buf.data() + 2 * (size_t)P, rd.data(), rd.size() * sizeof(int32_t));
     LC3D_CUDA_TRY(cudaMalloc(&c->fft_tw, buf.size() * sizeof(double)));
     LC3D_CUDA_TRY(cudaMemcpy(c->fft_tw, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice));
     return LC3D_OK;
@@ -299,7 +389,7 @@ int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, cudaStream_t s) {
     b.N = c->N;
     b.nrad = fft_plan(b.P, b.rad);
     b.tw = reinterpret_cast<const double2*>(c->fft_tw);
-    b.pos = reinterpret_cast<const int*>(c->fft_tw + 2 * (size_t)b.P);
+    b.rd = reinterpret_cast<const int*>(c->fft_tw + 2 * (size_t)b.P);
     int ctas = 0;
     for (int q = 0; q < count; ++q) {
         FftField& f = b.f[b.count++];
