@@ -142,6 +142,8 @@ typedef struct lc3d_beam_params {
 } lc3d_beam_params;
 
 int lc3d_set_beam(lc3d_ctx* ctx, const lc3d_beam_params* beam);
+/* the beam set by lc3d_set_beam at xi index xi_i into beam_ro (N x N, device) */
+int lc3d_beam_eval(lc3d_ctx* ctx, int xi_i, double* beam_ro, void* stream);
 int lc3d_run(lc3d_ctx* ctx, int xi0, int nsteps, double* ez_history, void* stream);
 
 /* Batches of independent simulations (a parameter scan; no reference
@@ -265,6 +267,93 @@ int lc3d_deposit_noalloc(const lc3d_params* p, const double* ro_initial,
         const double* fine_grid,
         double* out_ro, double* out_jx, double* out_jy, double* out_jz,
         void* stream);
+
+/* ---- learned predictor stage ----
+ *
+ * No counterpart in the reference. The reference's step (lcode.py:828-931)
+ * makes three particle passes: a predictor pass that moves the particles
+ * with the PREVIOUS step's fields ("no halfstep-averaged fields yet",
+ * lcode.py:846-871) and solves for first-pass fields F1, a corrector pass
+ * with (F1 + prev) / 2 that solves for the step's fields F2 (lcode.py:
+ * 876-901), and a final pass with (F2 + prev) / 2 (lcode.py:906-918).
+ *
+ * lc3d_step_arrays_first_pass is lc3d_step_arrays that also writes F1
+ * (Ex, Ey, Ez, Bx, By, Bz after the Variant A extrapolation) to first[6]
+ * (device arrays, N x N): the training targets of a predictor.
+ *
+ * lc3d_step_arrays_predicted runs the step with F1 replaced by pred[6]
+ * (Ex, Ey, Ez, Bx, By, Bz; device arrays): the predictor pass only moves
+ * the particles (its deposit and field solve are skipped), the corrector
+ * and final passes are the reference's; with pred = F1 it reproduces
+ * lc3d_step_arrays bit for bit. residual (a device double, or NULL)
+ * receives max_f max|F2_f - pred_f| / max_f max|F2_f| over Ex, Ey, Bx, By,
+ * Bz, the corrector's change of the prediction (a diagnostic: the plain
+ * method's own F2 - F1 is of the same order).
+ *
+ * lc3d_fields_rel_diff writes max_f max|a_f - b_f| / max_f max|b_f| over
+ * Ex, Ey, Bx, By, Bz of two sets of 6 fields to *out (a device double): a
+ * caller that checks a prediction against a step's true F1 (recorded by
+ * lc3d_step_arrays_first_pass) decides with it whether to keep predicting
+ * (see lcode3d_b200.predictor.run_learned). */
+int lc3d_step_arrays_first_pass(lc3d_ctx* ctx, const lc3d_state_ptrs* prev,
+        const lc3d_state_ptrs* out, const double* beam_ro,
+        double* const* first, void* stream);
+int lc3d_step_arrays_predicted(lc3d_ctx* ctx, const lc3d_state_ptrs* prev,
+        const lc3d_state_ptrs* out, const double* beam_ro,
+        const double* const* pred, double* residual, void* stream);
+int lc3d_fields_rel_diff(lc3d_ctx* ctx, const double* const* a, const double* const* b,
+        double* out, void* stream);
+
+/* A learned field predictor (no counterpart in the reference): a 3-level
+ * convolutional U-Net (3x3 convolutions, 32 / 64 / 128 channels, bf16
+ * weights and activations, fp32 accumulation; inference on the tcgen05
+ * tensor cores) mapping the fields ro, jx, jy, jz, Ex, Ey, Bx, By, Bz of
+ * steps t-1 and t-2 (pack: arrays of 9 in that order) to the first-pass
+ * fields Ex, Ey, Bx, By, Bz of step t:
+ *     pred_f = 2 F_f(t-1) - F_f(t-2) + o_f * net_f(F(t-1) / s, (F(t-1) - F(t-2)) / d, log10(s) / 4)
+ * The scales are per sample: s_c and d_c are the root mean squares of field
+ * c and of its difference over the grid, o is the root mean square of the
+ * differences of Ex, Ey, Bx, By, Bz (each times a multiplier set by
+ * lc3d_predictor_set_scales, default 1), computed on the device by
+ * lc3d_predictor_pack, which also feeds log10(s_c) / 4 as 9 constant input
+ * channels (27 of the 32 input channels are used). Parameters are one float32
+ * array of lc3d_predictor_num_params() entries (per layer: weights
+ * [9][Cout][Cin], then biases [Cout]). Arrays are device arrays; the
+ * float64 fields are N x N as elsewhere. */
+typedef struct lc3d_predictor lc3d_predictor;
+#define LC3D_PRED_INPUT 0       /* bf16 [N][N + 1][32] network input */
+#define LC3D_PRED_OUTPUT 1      /* f32 [N][N + 1][16] network output */
+#define LC3D_PRED_TARGET 2      /* f32 [N][N + 1][16] training target */
+long long lc3d_predictor_num_params(void);
+int lc3d_predictor_create(int grid_steps, int device, lc3d_predictor** out);
+int lc3d_predictor_destroy(lc3d_predictor* p);
+int lc3d_predictor_set_params(lc3d_predictor* p, const float* params, void* stream);
+int lc3d_predictor_get_params(lc3d_predictor* p, float* params, void* stream);
+int lc3d_predictor_get_grad(lc3d_predictor* p, float* grad, void* stream);
+/* multipliers (host arrays) of the 18 input and 5 output scales */
+int lc3d_predictor_set_scales(lc3d_predictor* p, const double* in_mult, const double* out_mult);
+/* scales and network input from f1[9] (step t-1) and f2[9] (step t-2) */
+int lc3d_predictor_pack(lc3d_predictor* p, const double* const* f1, const double* const* f2, void* stream);
+/* the network on the packed input */
+int lc3d_predictor_forward(lc3d_predictor* p, void* stream);
+/* after pack and forward: pred_f = 2 f1_f - f2_f + o_f output_f for Ex, Ey,
+ * Bx, By, Bz, and 2 f1 - f2 for Ez (arrays of 6: Ex, Ey, Ez, Bx, By, Bz) */
+int lc3d_predictor_predict(lc3d_predictor* p, const double* const* f1, const double* const* f2,
+        double* const* pred, void* stream);
+/* training target (first - (2 f1 - f2)) / o from the first-pass fields
+ * (arrays of 6 as above; the Ez entries are not used and may be NULL),
+ * after pack */
+int lc3d_predictor_set_target(lc3d_predictor* p, const double* const* first, const double* const* f1,
+        const double* const* f2, void* stream);
+/* after lc3d_predictor_forward: mean squared error of the output against the
+ * target added to *loss (device float), gradients of all parameters */
+int lc3d_predictor_backward(lc3d_predictor* p, float* loss, void* stream);
+/* one Adam step (beta 0.9 / 0.999) on the last gradients */
+int lc3d_predictor_adam(lc3d_predictor* p, float lr, void* stream);
+/* a device buffer of the predictor (LC3D_PRED_*): its address and size */
+int lc3d_predictor_tensor(lc3d_predictor* p, int which, void** ptr, long long* bytes);
+/* read and clear the predictor's device error flag (LC3D_ERR_TIMEOUT) */
+int lc3d_predictor_check_error(lc3d_predictor* p, void* stream);
 
 #ifdef __cplusplus
 }

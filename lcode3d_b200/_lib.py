@@ -82,7 +82,28 @@ SIGNATURES = [
     ('lc3d_batch_create', c_int, [P, c_int, ctypes.POINTER(c_void_p)]),
     ('lc3d_batch_run', c_int, [P, P, c_int, P, P]),
     ('lc3d_batch_destroy', c_int, [P]),
+    ('lc3d_beam_eval', c_int, [P, c_int, P, P]),
+    ('lc3d_step_arrays_first_pass', c_int, [P, ctypes.POINTER(StatePtrs), ctypes.POINTER(StatePtrs), P, P, P]),
+    ('lc3d_step_arrays_predicted', c_int, [P, ctypes.POINTER(StatePtrs), ctypes.POINTER(StatePtrs), P, P, P, P]),
+    ('lc3d_fields_rel_diff', c_int, [P, P, P, P, P]),
+    ('lc3d_predictor_num_params', ctypes.c_longlong, []),
+    ('lc3d_predictor_create', c_int, [c_int, c_int, ctypes.POINTER(c_void_p)]),
+    ('lc3d_predictor_destroy', c_int, [P]),
+    ('lc3d_predictor_set_params', c_int, [P, P, P]),
+    ('lc3d_predictor_get_params', c_int, [P, P, P]),
+    ('lc3d_predictor_get_grad', c_int, [P, P, P]),
+    ('lc3d_predictor_set_scales', c_int, [P, P, P]),
+    ('lc3d_predictor_pack', c_int, [P, P, P, P]),
+    ('lc3d_predictor_forward', c_int, [P, P]),
+    ('lc3d_predictor_predict', c_int, [P, P, P, P, P]),
+    ('lc3d_predictor_set_target', c_int, [P, P, P, P, P]),
+    ('lc3d_predictor_backward', c_int, [P, P, P]),
+    ('lc3d_predictor_adam', c_int, [P, ctypes.c_float, P]),
+    ('lc3d_predictor_tensor', c_int, [P, c_int, ctypes.POINTER(c_void_p), ctypes.POINTER(ctypes.c_longlong)]),
+    ('lc3d_predictor_check_error', c_int, [P, P]),
 ]
+
+PRED_INPUT, PRED_OUTPUT, PRED_TARGET = 0, 1, 2
 
 STAGES = ('move', 'deposit', 'deposit_finalize', 'rhs', 'transform', 'field_finalize', 'slice', 'other')
 

@@ -43,6 +43,7 @@
 #include <vector>
 
 #include "lc3d_internal.cuh"
+#include "tc_sm100.cuh"
 
 namespace {
 
@@ -53,7 +54,6 @@ constexpr int GEMM_THREADS = 192;
 constexpr int NACC = 4;                                          // f32 accumulators, one per digit level
 constexpr int TMEM_COLS = NACC * TN;                             // 512: all of TMEM
 constexpr int ROWS_PAD_ALIGN = 128;
-constexpr long long WAIT_LIMIT = 2000000000ll;                  // clock cycles
 
 struct OzProb {
     CUtensorMap ta, tb;            // A slices / B^T slices, stacked [S][rows_pad][k_pad]
@@ -74,96 +74,9 @@ struct OzBatch {
     unsigned* err;
 };
 
-// ---------------------------------------------------------------------------
-// PTX wrappers
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
+using namespace tc;
 
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// Bounded wait for the phase with the given parity: false once WAIT_LIMIT
-// SM clock cycles (~1-2 s at 1-2 GHz) have passed.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    const uint32_t a = smem_u32(bar);
-    const long long t0 = clock64();
-    for (;;) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (done) return true;
-        if (clock64() - t0 > WAIT_LIMIT) return false;
-    }
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
-            "r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// UMMA shared-memory descriptor, K-major operand in the canonical 64-byte
-// swizzled layout: 64-byte rows, 8-row groups 512 bytes apart.
-__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t saddr) {
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr >> 4) & 0x3fff);          // start address
-    d |= (uint64_t)1 << 16;                          // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(512 >> 4) << 32;                 // stride byte offset
-    d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
-    d |= (uint64_t)4 << 61;                          // layout: 64-byte swizzle
-    return d;
-}
-
-// Instruction descriptor: kind::f16 with bf16 A and B, f32 accumulator,
-// both operands K-major, M = 128, N = 128.
-constexpr uint32_t IDESC = (1u << 4) |               // D format f32
-                           (1u << 7) |               // A format bf16
-                           (1u << 10) |              // B format bf16
-                           ((uint32_t)(TN >> 3) << 17) |
-                           ((uint32_t)(TM >> 4) << 24);
-
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate));
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+constexpr uint32_t IDESC = idesc_bf16(TM, TN);
 
 __device__ __forceinline__ double pow2(int e) {
     return __longlong_as_double((long long)(e + 1023) << 52);   // exact for -1022 <= e <= 1023
@@ -208,9 +121,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
                      "r"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    tc_fence_before();
+    fence_before();
     __syncthreads();
-    tc_fence_after();
+    fence_after();
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0) {
@@ -241,7 +154,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
                     s_fail = 1;
                     break;
                 }
-                tc_fence_after();
+                fence_after();
                 const uint32_t a_base = smem_u32(sA + (size_t)st * S * TILE_BYTES);
                 const uint32_t b_base = smem_u32(sB + (size_t)st * S * TILE_BYTES);
                 unsigned fresh = (kb == 0) ? 0xfu : 0u;   // accumulators not yet written
@@ -253,7 +166,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
                         for (int kk = 0; kk < BK / 16; ++kk) {
                             const uint64_t ad = umma_desc_sw64(a_base + s * TILE_BYTES + kk * 32);
                             const uint64_t bd = umma_desc_sw64(b_base + u * TILE_BYTES + kk * 32);
-                            umma_bf16(acc, ad, bd, ((fresh >> lvl) & 1u) ? 0u : 1u);
+                            umma_bf16(acc, ad, bd, IDESC, ((fresh >> lvl) & 1u) ? 0u : 1u);
                             fresh &= ~(1u << lvl);
                         }
                     }
@@ -267,7 +180,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
         const int m = m0 + row;
         const bool ok = mbar_wait(done, 0);
         if (!ok) s_fail = 1;
-        tc_fence_after();
+        fence_after();
         if (ok) {
             const double sa = (m < P.M) ? pow2(P.ea[m]) : 0.0;
             const int nacc = min(S, NACC);
@@ -318,11 +231,11 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
             }
         }
     }
-    tc_fence_before();
+    fence_before();
     __syncthreads();
     if (s_fail && threadIdx.x == 0) atomicOr(b.err, LC3D_FLAG_TIMEOUT);
     if (warp == 1) {
-        tc_fence_after();
+        fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
     }
 }
@@ -394,20 +307,8 @@ struct MixedState {
     CUtensorMap map_data[6];
 };
 
-PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        cudaDriverEntryPointQueryResult q;
-        void* p = nullptr;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
-}
-
 int make_map(CUtensorMap* m, void* base, int S, int rows_pad, int k_pad) {
-    auto enc = get_encode();
+    auto enc = tc_get_encode();
     if (!enc) return LC3D_ERR_CUDA;
     cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)S * rows_pad};
     cuuint64_t strides[1] = {(cuuint64_t)k_pad * 2};
@@ -597,4 +498,16 @@ int mixed_stage(lc3d_ctx* c, const MixedStageDesc* d, int count, cudaStream_t s)
     oz_gemm_kernel<<<tiles, GEMM_THREADS, smem, s>>>(b);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tc_get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
 }

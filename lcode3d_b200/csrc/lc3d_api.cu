@@ -156,11 +156,68 @@ int deposit_into(lc3d_ctx* c, const double* ro_initial, const double* x, const d
     return launch_deposit_finalize(f, s);
 }
 
+// Optional extras of a step: first-pass fields out, or a prediction that
+// replaces the first pass, with the residual of the corrector against it.
+struct StepExtras {
+    double* const* first;                 // 6 fields, or NULL
+    const double* const* pred;            // 6 fields, or NULL
+    double* residual;                     // device double, or NULL
+};
+
+struct AvgArgs {
+    const double* a[6];
+    const double* b[6];
+    double* out[6];
+    int n;
+};
+
+// out = (a + b) / 2 for 6 fields
+__global__ void pred_avg_kernel(const __grid_constant__ AvgArgs g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) g.out[f][i] = (g.a[f][i] + g.b[f][i]) / 2;
+}
+
+struct ResidArgs {
+    const double* f[5];                   // corrector fields Ex Ey Bx By Bz
+    const double* pred[5];
+    unsigned long long* acc;              // [max |f - pred|, max |f|] as double bits
+    int n;
+};
+
+// Maxima over the 5 fields; non-negative doubles order like their bits.
+__global__ void resid_kernel(const __grid_constant__ ResidArgs a) {
+    double d = 0, m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+            const double x = a.f[f][i];
+            d = fmax(d, fabs(x - a.pred[f][i]));
+            m = fmax(m, fabs(x));
+        }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(a.acc, (unsigned long long)__double_as_longlong(d));
+        atomicMax(a.acc + 1, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+__global__ void resid_final_kernel(const unsigned long long* acc, double* out) {
+    const double d = __longlong_as_double((long long)acc[0]), m = __longlong_as_double((long long)acc[1]);
+    *out = m > 0 ? d / m : d;
+}
+
 // The xi step of lcode.py:828-931.
 int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& out, const double* beam,
-             cudaStream_t s) {
+             cudaStream_t s, const StepExtras* x = nullptr) {
     const double* prevF[6] = {prev.Ex, prev.Ey, prev.Ez, prev.Bx, prev.By, prev.Bz};
     const bool A = c->p.field_solver_variant_A != 0;
+    const bool predicted = x && x->pred;
     MoveArgs mv = move_base(c);
     mv.m = c->m; mv.q = c->q; mv.x_init = c->x_init; mv.y_init = c->y_init;
     mv.x_prev = prev.x_offt; mv.y_prev = prev.y_offt;
@@ -194,17 +251,48 @@ int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& ou
             ProfScope ps(c, LC3D_STAGE_MOVE, s);
             LC3D_TRY(launch_move_smart(mv, s));
         }
+        if (pass == 0 && predicted) {
+            // the prediction stands in for the first-pass fields: only the
+            // particle positions of this pass are used (as the estimate)
+            AvgArgs g;
+            for (int f = 0; f < 6; ++f) {
+                g.a[f] = x->pred[f];
+                g.b[f] = prevF[f];
+                g.out[f] = c->avg[f];
+            }
+            g.n = c->N * c->N;
+            ProfScope ps(c, LC3D_STAGE_FIELD_FIN, s);
+            pred_avg_kernel<<<(g.n + 255) / 256, 256, 0, s>>>(g);
+            LC3D_CUDA_TRY(cudaGetLastError());
+            continue;
+        }
         LC3D_TRY(deposit_into(c, c->ro_initial, pw[0], pw[1], c->m, c->q, pw[2], pw[3], pw[4], c->dens[0],
                               c->dens[1], c->dens[2], c->dens[3], s));
         if (pass == 0) {
             in.Ex_sub = prev.Ex; in.Ey_sub = prev.Ey; in.Bx_sub = prev.Bx; in.By_sub = prev.By;
-            for (int f = 0; f < 6; ++f) so.out[f] = nullptr;
+            for (int f = 0; f < 6; ++f) so.out[f] = (x && x->first) ? x->first[f] : nullptr;
         } else {
             in.Ex_sub = c->avg[0]; in.Ey_sub = c->avg[1]; in.Bx_sub = c->avg[3]; in.By_sub = c->avg[4];
             so.out[0] = out.Ex; so.out[1] = out.Ey; so.out[2] = out.Ez;
             so.out[3] = out.Bx; so.out[4] = out.By; so.out[5] = out.Bz;
         }
         LC3D_TRY(solve_fields(c, LC3D_F_ALL, in, so, s));
+    }
+    if (predicted && x->residual) {
+        ResidArgs ra;
+        const double* F2[5] = {out.Ex, out.Ey, out.Bx, out.By, out.Bz};
+        const int pi[5] = {0, 1, 3, 4, 5};
+        for (int f = 0; f < 5; ++f) {
+            ra.f[f] = F2[f];
+            ra.pred[f] = x->pred[pi[f]];
+        }
+        ra.acc = c->resid;
+        ra.n = c->N * c->N;
+        ProfScope ps(c, LC3D_STAGE_OTHER, s);
+        LC3D_CUDA_TRY(cudaMemsetAsync(c->resid, 0, 2 * sizeof(unsigned long long), s));
+        resid_kernel<<<296, 256, 0, s>>>(ra);
+        resid_final_kernel<<<1, 1, 0, s>>>(c->resid, x->residual);
+        LC3D_CUDA_TRY(cudaGetLastError());
     }
     // final move with the corrector's averaged fields, then deposit
     mv.est_x = c->pw[1][0];
@@ -239,6 +327,7 @@ void destroy(lc3d_ctx* c) {
     if (c->acc) cudaFree(c->acc);
     if (c->err) cudaFree(c->err);
     if (c->zeros) cudaFree(c->zeros);
+    if (c->resid) cudaFree(c->resid);
     if (c->fft_tw) cudaFree(c->fft_tw);
     mixed_free(c);
     run_free(c);
@@ -326,6 +415,7 @@ int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out) {
     LC3D_STEP(dalloc(&c->acc, c->acc_plane * 8));
     LC3D_STEP(dalloc(&c->err, (size_t)1));
     LC3D_STEP(dalloc(&c->zeros, ng));
+    LC3D_STEP(dalloc(&c->resid, (size_t)2));
     LC3D_STEP(particles_prepare());
     LC3D_STEP(fields_init(c));
     LC3D_STEP(fft_init(c));
@@ -416,6 +506,48 @@ int lc3d_step_arrays(lc3d_ctx* c, const lc3d_state_ptrs* prev, const lc3d_state_
     if (c->const_set != 3) return LC3D_ERR_STATE;
     DeviceGuard g(c->device);
     return run_step(c, *prev, *out, beam_ro ? beam_ro : c->zeros, S(stream));
+}
+
+int lc3d_step_arrays_first_pass(lc3d_ctx* c, const lc3d_state_ptrs* prev, const lc3d_state_ptrs* out,
+                                const double* beam_ro, double* const* first, void* stream) {
+    if (!c || !state_complete(prev) || !state_complete(out) || !first) return LC3D_ERR_PARAM;
+    for (int f = 0; f < 6; ++f)
+        if (!first[f]) return LC3D_ERR_PARAM;
+    if (c->const_set != 3) return LC3D_ERR_STATE;
+    DeviceGuard g(c->device);
+    StepExtras x{first, nullptr, nullptr};
+    return run_step(c, *prev, *out, beam_ro ? beam_ro : c->zeros, S(stream), &x);
+}
+
+int lc3d_step_arrays_predicted(lc3d_ctx* c, const lc3d_state_ptrs* prev, const lc3d_state_ptrs* out,
+                               const double* beam_ro, const double* const* pred, double* residual, void* stream) {
+    if (!c || !state_complete(prev) || !state_complete(out) || !pred) return LC3D_ERR_PARAM;
+    for (int f = 0; f < 6; ++f)
+        if (!pred[f]) return LC3D_ERR_PARAM;
+    if (c->const_set != 3) return LC3D_ERR_STATE;
+    DeviceGuard g(c->device);
+    StepExtras x{nullptr, pred, residual};
+    return run_step(c, *prev, *out, beam_ro ? beam_ro : c->zeros, S(stream), &x);
+}
+
+int lc3d_fields_rel_diff(lc3d_ctx* c, const double* const* a, const double* const* b, double* out, void* stream) {
+    if (!c || !a || !b || !out) return LC3D_ERR_PARAM;
+    ResidArgs ra;
+    const int pi[5] = {0, 1, 3, 4, 5};   // Ex, Ey, Bx, By, Bz
+    for (int f = 0; f < 5; ++f) {
+        if (!a[pi[f]] || !b[pi[f]]) return LC3D_ERR_PARAM;
+        ra.pred[f] = a[pi[f]];
+        ra.f[f] = b[pi[f]];
+    }
+    ra.acc = c->resid;
+    ra.n = c->N * c->N;
+    DeviceGuard g(c->device);
+    const cudaStream_t s = S(stream);
+    LC3D_CUDA_TRY(cudaMemsetAsync(c->resid, 0, 2 * sizeof(unsigned long long), s));
+    resid_kernel<<<296, 256, 0, s>>>(ra);
+    resid_final_kernel<<<1, 1, 0, s>>>(c->resid, out);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
 }
 
 int lc3d_move_estimate_wo_fields(lc3d_ctx* c, const double* m, const double* x_init, const double* y_init,

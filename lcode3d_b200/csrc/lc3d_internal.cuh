@@ -185,6 +185,7 @@ struct lc3d_ctx {
     size_t acc_plane;                     // plane stride in words
     unsigned* err;                        // device error flag
     double* zeros;                        // N x N zeros (absent beam)
+    unsigned long long* resid;            // predicted-step residual maxima (2 words, double bits)
     // field-solver workspaces (fields.cu)
     double *S2, *C, *CT;                  // 2*DST-I (M x M), DCT-I (N x N), its transpose
     double *lam_dir, *lam_mix, *lam_mixT, *lam_neu;

@@ -1,0 +1,1032 @@
+// Learned field predictor: a small convolutional U-Net that predicts the
+// first-pass (predictor-stage) fields Ex, Ey, Bx, By, Bz of the next xi
+// step from the fields of the two previous steps, so that the solver can
+// skip the first deposit + field solve of lcode.py:846-871 (the pass that
+// moves the particles with the previous step's fields, "no halfstep-averaged
+// fields yet") and go straight to the corrector. No counterpart in the
+// reference; the corrector that follows is the reference's own
+// (lcode.py:882-911) and judges the prediction.
+//
+// Network (all 3x3 convolutions, BF16 weights and activations, FP32
+// accumulation, sum skip connections):
+//   x0  (27 of 32 channels)          N x N      normalised fields of t-1, t-1 minus t-2, levels
+//   e1 = relu(conv1(x0))     32      N x N
+//   e2 = relu(conv2(pool(e1))) 64    N2 x N2    N2 = (N + 1) / 2
+//   e3 = relu(conv3(pool(e2))) 128   N3 x N3    N3 = (N2 + 1) / 2
+//   u3 = conv4(e3)           64      N3 x N3
+//   d2 = relu(up(u3) + e2)   64      N2 x N2    up: nearest neighbour
+//   u2 = conv5(d2)           32      N2 x N2
+//   d1 = relu(up(u2) + e1)   32      N x N
+//   y  = conv6(d1)           16 (5 used), float32
+// prediction = 2 F(t-1) - F(t-2) + out_scale * y (per field), i.e. the
+// network learns the correction to linear extrapolation.
+//
+// Layout. An activation at a level with H x W pixels is [H][W + 1][C]
+// (NHWC, row pitch Wp = W + 1): column W of every row is kept zero, so in
+// the flattened pixel index p = y Wp + x the 3x3 neighbours of p are
+// p + dy Wp + dx and the zero column doubles as the left/right padding;
+// rows above and below fall outside [0, H Wp) and are zero-filled by TMA.
+//
+// Inference convolution: implicit GEMM on the 5th-generation tensor cores.
+// A CTA owns 128 consecutive flattened pixels (M = 128) and all output
+// channels (N = Cout); K runs over 9 taps x Cin in blocks of 32 channels.
+// Per K block warp 0 TMA-loads the 128 x 32 input tile shifted by the tap
+// (a 2-D tensor map over [H Wp][Cin], 64-byte swizzle) and the Cout x 32
+// weight tile of that tap, warp 1 issues two tcgen05.mma (128 x Cout x 16,
+// bf16 -> f32 in TMEM), warps 2-5 add the bias, apply ReLU and store bf16
+// (or f32) NHWC, writing zeros in the pad column. Every mbarrier wait is
+// bounded; on time-out the kernel sets an error flag and exits, and TMEM is
+// always freed.
+//
+// Training (float32 SIMT kernels): backward data (the transposed 3x3
+// convolution), weight and bias gradients (reductions over pixels), the
+// pooling / upsampling / ReLU adjoints, an MSE loss on the 5 fields and
+// Adam. Weights are kept as float32 master copies; the bf16 copies the
+// forward pass reads are refreshed after every update.
+
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lc3d.h"
+#include "lc3d_internal.cuh"
+#include "tc_sm100.cuh"
+
+namespace {
+
+using namespace tc;
+
+constexpr int NLAYERS = 6;
+constexpr int CONV_THREADS = 192;
+constexpr int CONV_STAGES = 4;
+constexpr int TILE_PIX = 128;                      // M
+constexpr int KB = 32;                             // channels per K block (64 bytes of bf16)
+constexpr int A_TILE_BYTES = TILE_PIX * KB * 2;     // 8 KiB
+constexpr int B_TILE_MAX = 128 * KB * 2;            // Cout <= 128
+
+struct ConvArgs {
+    CUtensorMap tin;               // [H Wp][Cin] bf16, box (32, 128)
+    CUtensorMap twt;               // [9 Cout][Cin] bf16, box (32, Cout)
+    const float* bias;             // [Cout]
+    void* out;                     // [H Wp][Cout], bf16 or f32
+    int out_f32, relu;
+    int H, W, Wp, NP, Cin, Cout;
+    uint32_t idesc;
+    unsigned* err;
+};
+
+__global__ void __launch_bounds__(CONV_THREADS, 1) conv3x3_tc_kernel(const __grid_constant__ ConvArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + CONV_STAGES * A_TILE_BYTES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + CONV_STAGES * B_TILE_MAX);
+    uint64_t* empty = full + CONV_STAGES;
+    uint64_t* done = empty + CONV_STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    __shared__ int s_fail;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p0 = blockIdx.x * TILE_PIX;
+    const int cblocks = a.Cin / KB, nkb = 9 * cblocks;
+    const uint32_t tcols = a.Cout < 32 ? 32u : (uint32_t)a.Cout;
+    const uint32_t b_bytes = (uint32_t)a.Cout * KB * 2;
+
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        for (int i = 0; i < CONV_STAGES; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) tmem_alloc(tmem_slot, tcols);
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {   // ---- TMA producer ----
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int st = kb % CONV_STAGES, round = kb / CONV_STAGES;
+                if (round > 0 && !mbar_wait(&empty[st], (round - 1) & 1)) {
+                    s_fail = 1;
+                    break;
+                }
+                const int tap = kb / cblocks, cb = kb - tap * cblocks;
+                const int off = (tap / 3 - 1) * a.Wp + (tap % 3 - 1);
+                mbar_expect_tx(&full[st], A_TILE_BYTES + b_bytes);
+                tma_load_2d(sA + st * A_TILE_BYTES, &a.tin, &full[st], cb * KB, p0 + off);
+                tma_load_2d(sB + st * B_TILE_MAX, &a.twt, &full[st], cb * KB, tap * a.Cout);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {   // ---- MMA issuer ----
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int st = kb % CONV_STAGES, round = kb / CONV_STAGES;
+                if (!mbar_wait(&full[st], round & 1)) {
+                    s_fail = 1;
+                    break;
+                }
+                fence_after();
+                const uint32_t a_base = smem_u32(sA + st * A_TILE_BYTES);
+                const uint32_t b_base = smem_u32(sB + st * B_TILE_MAX);
+#pragma unroll
+                for (int kk = 0; kk < KB / 16; ++kk)
+                    umma_bf16(tmem, umma_desc_sw64(a_base + kk * 32), umma_desc_sw64(b_base + kk * 32), a.idesc,
+                              (kb | kk) ? 1u : 0u);
+                umma_commit(&empty[st]);   // frees the stage once these MMAs have read it
+            }
+            umma_commit(done);
+        }
+    } else {   // ---- epilogue: warps 2..5 read TMEM lanes 32 (warp % 4) .. +31 ----
+        const int quarter = warp & 3;
+        const int p = p0 + quarter * 32 + lane;
+        const bool ok = mbar_wait(done, 0);
+        if (!ok) s_fail = 1;
+        fence_after();
+        if (ok) {
+            const int x = p % a.Wp;
+            const bool live = p < a.NP, pad = x >= a.W;
+            const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+            for (int c0 = 0; c0 < a.Cout; c0 += 16) {
+                uint32_t r[16];
+                tmem_ld16(tmem + lane_base + c0, r);
+                tmem_wait_ld();
+                float v[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    float t = __uint_as_float(r[j]) + __ldg(a.bias + c0 + j);
+                    if (a.relu) t = fmaxf(t, 0.0f);
+                    v[j] = pad ? 0.0f : t;
+                }
+                if (!live) continue;
+                if (a.out_f32) {
+                    float4* o = reinterpret_cast<float4*>(static_cast<float*>(a.out) + (size_t)p * a.Cout + c0);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) o[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+                } else {
+                    uint4 w[2];
+                    uint32_t* wp = reinterpret_cast<uint32_t*>(w);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+                        wp[j] = *reinterpret_cast<uint32_t*>(&h);
+                    }
+                    uint4* o = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.out) + (size_t)p * a.Cout + c0);
+                    o[0] = w[0];
+                    o[1] = w[1];
+                }
+            }
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (s_fail && threadIdx.x == 0) atomicOr(a.err, LC3D_FLAG_TIMEOUT);
+    if (warp == 1) {
+        fence_after();
+        tmem_dealloc(tmem, tcols);
+    }
+}
+
+constexpr size_t conv_smem_bytes() {
+    return 1024 + CONV_STAGES * (A_TILE_BYTES + B_TILE_MAX) + (2 * CONV_STAGES + 1) * 8 + 16;
+}
+
+// ---------------------------------------------------------------------------
+// Element-wise kernels
+// ---------------------------------------------------------------------------
+struct Level {
+    int H, W, Wp, NP;
+};
+
+__device__ __forceinline__ uint32_t pack_bf2(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+
+__device__ __forceinline__ void unpack_bf8(uint4 u, float (&v)[8]) {
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float2 f = __bfloat1622float2(h[j]);
+        v[2 * j] = f.x;
+        v[2 * j + 1] = f.y;
+    }
+}
+
+__device__ __forceinline__ uint4 pack_bf8(const float (&v)[8]) {
+    return make_uint4(pack_bf2(v[0], v[1]), pack_bf2(v[2], v[3]), pack_bf2(v[4], v[5]), pack_bf2(v[6], v[7]));
+}
+
+struct PackArgs {
+    const double* f1[9];           // ro, jx, jy, jz, Ex, Ey, Bx, By, Bz at t-1
+    const double* f2[9];           // the same at t-2
+    const double* scale;           // [23] device: input channel scales, then output scales
+    double* partial;               // [STAT_BLOCKS][18] sums of squares
+    double mult[23];               // multipliers of the scales
+    __nv_bfloat16* x0;             // [NP][32]
+    Level L;
+};
+
+// Per-sample channel statistics: partial sums of f1_c^2 and (f1_c - f2_c)^2
+// per block, then one block adds them in a fixed order (deterministic) and
+// sets scale_c = mult_c rms_c (1 where rms_c = 0). The output scale, shared
+// by the 5 predicted fields, is the root mean square of the step
+// differences of Ex, Ey, Bx, By, Bz (times the field's multiplier): the
+// first-pass correction is of the order of one step's change.
+constexpr int STAT_BLOCKS = 296;
+
+__global__ void __launch_bounds__(256) stats_kernel(const __grid_constant__ PackArgs a) {
+    double s[18];
+#pragma unroll
+    for (int c = 0; c < 18; ++c) s[c] = 0.0;
+    const int n = a.L.H * a.L.W;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            const double u1 = __ldg(a.f1[c] + i), d = u1 - __ldg(a.f2[c] + i);
+            s[c] += u1 * u1;
+            s[9 + c] += d * d;
+        }
+    __shared__ double ws[8][18];
+#pragma unroll
+    for (int c = 0; c < 18; ++c) {
+        double v = s[c];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5][c] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 18) {
+        double v = 0.0;
+        for (int w = 0; w < 8; ++w) v += ws[w][threadIdx.x];
+        a.partial[blockIdx.x * 18 + threadIdx.x] = v;
+    }
+}
+
+__global__ void scale_final_kernel(const __grid_constant__ PackArgs a) {
+    const int c = threadIdx.x;
+    double* scale = const_cast<double*>(a.scale);
+    __shared__ double rms[18];
+    if (c < 18) {
+        double v = 0.0;
+        for (int b = 0; b < STAT_BLOCKS; ++b) v += a.partial[b * 18 + c];
+        rms[c] = sqrt(v / ((double)a.L.H * a.L.W));
+        scale[c] = rms[c] > 0 ? a.mult[c] * rms[c] : 1.0;
+    }
+    __syncthreads();
+    if (c < 5) {
+        // differences of Ex, Ey, Bx, By, Bz: channels 13..17
+        double m2 = 0.0;
+        for (int f = 13; f < 18; ++f) m2 += rms[f] * rms[f];
+        const double o = sqrt(m2 / 5.0);
+        scale[18 + c] = o > 0 ? a.mult[18 + c] * o : 1.0;
+    }
+}
+
+// x0[p] = (f1 / s_c, (f1 - f2) / d_c, log10(s_c) / 4, 0 ...), zero in the
+// pad column: 9 fields, 9 differences, 9 constant channels that carry the
+// absolute field levels the per-sample normalisation removes.
+__global__ void pack_kernel(const __grid_constant__ PackArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.L.NP) return;
+    const int y = p / a.L.Wp, x = p - y * a.L.Wp;
+    float v[32];
+#pragma unroll
+    for (int c = 0; c < 32; ++c) v[c] = 0.0f;
+    if (x < a.L.W) {
+        const size_t i = (size_t)y * a.L.W + x;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            const double u1 = __ldg(a.f1[c] + i), u2 = __ldg(a.f2[c] + i);
+            v[c] = (float)(u1 * (1.0 / a.scale[c]));
+            v[9 + c] = (float)((u1 - u2) * (1.0 / a.scale[9 + c]));
+            v[18 + c] = (float)(log10(a.scale[c]) * 0.25);
+        }
+    }
+    uint4* o = reinterpret_cast<uint4*>(a.x0 + (size_t)p * 32);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float w[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) w[j] = v[8 * q + j];
+        o[q] = pack_bf8(w);
+    }
+}
+
+// 2 x 2 average pooling (ceil mode: border cells average their valid
+// children). One thread per (output pixel, 8 channels).
+__global__ void pool_kernel(const __nv_bfloat16* __restrict__ in, Level li, __nv_bfloat16* __restrict__ out, Level lo,
+                            int C) {
+    const int groups = C / 8;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)lo.NP * groups) return;
+    const int p = (int)(t / groups), g = (int)(t - (long long)p * groups);
+    const int Y = p / lo.Wp, X = p - Y * lo.Wp;
+    float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (X < lo.W) {
+        int cnt = 0;
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                const int y = 2 * Y + dy, x = 2 * X + dx;
+                if (y >= li.H || x >= li.W) continue;
+                float v[8];
+                unpack_bf8(*reinterpret_cast<const uint4*>(in + ((size_t)y * li.Wp + x) * C + 8 * g), v);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) s[j] += v[j];
+                ++cnt;
+            }
+        const float r = 1.0f / (float)cnt;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s[j] *= r;
+    }
+    *reinterpret_cast<uint4*>(out + (size_t)p * C + 8 * g) = pack_bf8(s);
+}
+
+// d = relu(up(u) + e): u at the coarse level, e and d at the fine level.
+__global__ void upadd_relu_kernel(const __nv_bfloat16* __restrict__ u, Level lc, const __nv_bfloat16* __restrict__ e,
+                                  __nv_bfloat16* __restrict__ d, Level lf, int C) {
+    const int groups = C / 8;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)lf.NP * groups) return;
+    const int p = (int)(t / groups), g = (int)(t - (long long)p * groups);
+    const int y = p / lf.Wp, x = p - y * lf.Wp;
+    float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (x < lf.W) {
+        float a[8], b[8];
+        unpack_bf8(*reinterpret_cast<const uint4*>(u + ((size_t)(y >> 1) * lc.Wp + (x >> 1)) * C + 8 * g), a);
+        unpack_bf8(*reinterpret_cast<const uint4*>(e + (size_t)p * C + 8 * g), b);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s[j] = fmaxf(a[j] + b[j], 0.0f);
+    }
+    *reinterpret_cast<uint4*>(d + (size_t)p * C + 8 * g) = pack_bf8(s);
+}
+
+// Fields Ex, Ey, Ez, Bx, By, Bz; the network's 5 outputs are Ex, Ey, Bx,
+// By, Bz (field indices net_field(k)); Ez is extrapolated linearly.
+__device__ __host__ constexpr int net_field(int k) { return k < 2 ? k : k + 1; }
+
+struct OutArgs {
+    const double* f1[6];           // Ex, Ey, Ez, Bx, By, Bz at t-1
+    const double* f2[6];           // ... at t-2
+    const double* first[6];        // target: first-pass fields at t (training; Ez unused)
+    double* pred[6];               // prediction at t (inference)
+    const double* scale;           // [23] device scales; the output scales at 18..
+    const float* y;                // [NP][16]
+    float* target;                 // [NP][16]
+    Level L;
+};
+
+// pred = 2 f1 - f2 + scale * y (Ez: 2 f1 - f2)
+__global__ void unpack_kernel(const __grid_constant__ OutArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.L.H * a.L.W) return;
+    const int yy = i / a.L.W, x = i - yy * a.L.W;
+    const float* yp = a.y + ((size_t)yy * a.L.Wp + x) * 16;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int f = net_field(k);
+        a.pred[f][i] = 2.0 * __ldg(a.f1[f] + i) - __ldg(a.f2[f] + i) + a.scale[18 + k] * (double)yp[k];
+    }
+    a.pred[2][i] = 2.0 * __ldg(a.f1[2] + i) - __ldg(a.f2[2] + i);
+}
+
+// target = (first - (2 f1 - f2)) / scale, zero elsewhere
+__global__ void target_kernel(const __grid_constant__ OutArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.L.NP) return;
+    const int yy = p / a.L.Wp, x = p - yy * a.L.Wp;
+    float v[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) v[c] = 0.0f;
+    if (x < a.L.W) {
+        const size_t i = (size_t)yy * a.L.W + x;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const int f = net_field(k);
+            v[k] = (float)((__ldg(a.first[f] + i) - (2.0 * __ldg(a.f1[f] + i) - __ldg(a.f2[f] + i))) / a.scale[18 + k]);
+        }
+    }
+    float4* o = reinterpret_cast<float4*>(a.target + (size_t)p * 16);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+
+// Mean squared error over the 5 used channels of the H x W pixels; g = dL/dy.
+__global__ void loss_kernel(const float* __restrict__ y, const float* __restrict__ t, float* __restrict__ g,
+                            Level L, float* loss) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const float inv = 1.0f / (5.0f * (float)L.H * (float)L.W);
+    float s = 0.0f;
+    if (p < L.NP) {
+        const int x = p % L.Wp;
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+            float d = 0.0f;
+            if (c < 5 && x < L.W) d = y[(size_t)p * 16 + c] - t[(size_t)p * 16 + c];
+            s += d * d;
+            g[(size_t)p * 16 + c] = 2.0f * d * inv;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ float ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float b = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += ws[w];
+        atomicAdd(loss, b * inv);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Training kernels (float32)
+// ---------------------------------------------------------------------------
+constexpr int BWD_THREADS = 256;
+constexpr int BWD_PIX = 64;
+
+// dX[p][ci] = sum_tap sum_co g[p - off(tap)][co] W[tap][co][ci], times
+// (mask[p][ci] > 0) when a mask is given; zero in the pad column.
+template <int CIN>
+__global__ void __launch_bounds__(BWD_THREADS) conv_bwd_data_kernel(const float* __restrict__ g, int CG,
+                                                                    const __nv_bfloat16* __restrict__ w,
+                                                                    const __nv_bfloat16* __restrict__ mask,
+                                                                    float* __restrict__ dx, Level L) {
+    extern __shared__ float sm[];
+    const int GP = CG + 1;                         // padded row of gs
+    float* gs = sm;                                // [BWD_PIX][CG + 1]
+    float* ws = sm + BWD_PIX * GP;                 // [CG][CIN]
+    constexpr int CGRP = CIN / 4, PGRP = BWD_THREADS / CGRP, PPT = BWD_PIX / PGRP;
+    const int cg = threadIdx.x % CGRP, pg = threadIdx.x / CGRP;
+    const int p0 = blockIdx.x * BWD_PIX;
+    float acc[PPT][4];
+#pragma unroll
+    for (int i = 0; i < PPT; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+    for (int tap = 0; tap < 9; ++tap) {
+        const int off = (tap / 3 - 1) * L.Wp + (tap % 3 - 1);
+        __syncthreads();
+        for (int i = threadIdx.x; i < BWD_PIX * CG; i += BWD_THREADS) {
+            const int px = i / CG, co = i - px * CG;
+            const int q = p0 + px - off;
+            gs[px * GP + co] = (q >= 0 && q < L.NP) ? g[(size_t)q * CG + co] : 0.0f;
+        }
+        for (int i = threadIdx.x; i < CG * CIN; i += BWD_THREADS)
+            ws[i] = __bfloat162float(w[(size_t)tap * CG * CIN + i]);
+        __syncthreads();
+        for (int co = 0; co < CG; ++co) {
+            const float4 wv = *reinterpret_cast<const float4*>(ws + co * CIN + 4 * cg);
+#pragma unroll
+            for (int i = 0; i < PPT; ++i) {
+                const float gv = gs[(pg * PPT + i) * GP + co];
+                acc[i][0] += gv * wv.x;
+                acc[i][1] += gv * wv.y;
+                acc[i][2] += gv * wv.z;
+                acc[i][3] += gv * wv.w;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) {
+        const int p = p0 + pg * PPT + i;
+        if (p >= L.NP) continue;
+        const bool pad = (p % L.Wp) >= L.W;
+        float v[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            v[j] = pad ? 0.0f : acc[i][j];
+            if (mask && !(__bfloat162float(mask[(size_t)p * CIN + 4 * cg + j]) > 0.0f)) v[j] = 0.0f;
+        }
+        *reinterpret_cast<float4*>(dx + (size_t)p * CIN + 4 * cg) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+}
+
+// dW[tap][co][ci] += sum_p g[p][co] x[p + off(tap)][ci] over one chunk of
+// pixels (blockIdx.x) for one tap (blockIdx.y).
+constexpr int WG_SUB = 32;
+template <int CG, int CIN>
+__global__ void __launch_bounds__(BWD_THREADS) conv_bwd_w_kernel(const float* __restrict__ g,
+                                                                 const __nv_bfloat16* __restrict__ x,
+                                                                 float* __restrict__ dw, Level L, int chunk) {
+    __shared__ float gs[WG_SUB][CG];
+    __shared__ __align__(16) float xs[WG_SUB][CIN];
+    constexpr int CGRP = CIN / 4, OGRP = BWD_THREADS / CGRP;
+    constexpr int ROWS = CG >= OGRP ? CG / OGRP : 1;
+    const int cg = threadIdx.x % CGRP, og = threadIdx.x / CGRP;
+    const int tap = blockIdx.y, off = (tap / 3 - 1) * L.Wp + (tap % 3 - 1);
+    const int pa = blockIdx.x * chunk, pb = min(L.NP, pa + chunk);
+    float acc[ROWS][4];
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[r][j] = 0.0f;
+    for (int s0 = pa; s0 < pb; s0 += WG_SUB) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < WG_SUB * CG; i += BWD_THREADS) {
+            const int px = i / CG, co = i - px * CG, p = s0 + px;
+            gs[px][co] = p < pb ? g[(size_t)p * CG + co] : 0.0f;
+        }
+        for (int i = threadIdx.x; i < WG_SUB * CIN; i += BWD_THREADS) {
+            const int px = i / CIN, ci = i - px * CIN, q = s0 + px + off;
+            xs[px][ci] = (s0 + px < pb && q >= 0 && q < L.NP) ? __bfloat162float(x[(size_t)q * CIN + ci]) : 0.0f;
+        }
+        __syncthreads();
+        if (og * ROWS < CG) {
+            for (int px = 0; px < WG_SUB; ++px) {
+                const float4 xv = *reinterpret_cast<const float4*>(&xs[px][4 * cg]);
+#pragma unroll
+                for (int r = 0; r < ROWS; ++r) {
+                    const float gv = gs[px][og * ROWS + r];
+                    acc[r][0] += gv * xv.x;
+                    acc[r][1] += gv * xv.y;
+                    acc[r][2] += gv * xv.z;
+                    acc[r][3] += gv * xv.w;
+                }
+            }
+        }
+    }
+    if (og * ROWS >= CG) return;
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            atomicAdd(dw + ((size_t)tap * CG + og * ROWS + r) * CIN + 4 * cg + j, acc[r][j]);
+}
+
+// db[co] += sum_p g[p][co] over one chunk of pixels.
+__global__ void bias_grad_kernel(const float* __restrict__ g, int CG, float* __restrict__ db, int NP, int chunk) {
+    const int pa = blockIdx.x * chunk, pb = min(NP, pa + chunk);
+    for (int co = threadIdx.x; co < CG; co += blockDim.x) {
+        float s = 0.0f;
+        for (int p = pa; p < pb; ++p) s += g[(size_t)p * CG + co];
+        atomicAdd(db + co, s);
+    }
+}
+
+// g_u[Y][X][c] = sum of g_d over the valid fine children (adjoint of the
+// nearest-neighbour upsampling).
+__global__ void downsum_kernel(const float* __restrict__ gd, Level lf, float* __restrict__ gu, Level lc, int C) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)lc.NP * C) return;
+    const int p = (int)(t / C), c = (int)(t - (long long)p * C);
+    const int Y = p / lc.Wp, X = p - Y * lc.Wp;
+    float s = 0.0f;
+    if (X < lc.W)
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                const int y = 2 * Y + dy, x = 2 * X + dx;
+                if (y < lf.H && x < lf.W) s += gd[((size_t)y * lf.Wp + x) * C + c];
+            }
+    gu[t] = s;
+}
+
+// g_e = (g_e + g_p[parent] / children(parent)) * (e > 0) (adjoint of the
+// average pooling, plus the skip gradient already in g_e, through the ReLU).
+__global__ void pool_bwd_mask_kernel(float* __restrict__ ge, const __nv_bfloat16* __restrict__ e, Level lf,
+                                     const float* __restrict__ gp, Level lc, int C) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)lf.NP * C) return;
+    const int p = (int)(t / C), c = (int)(t - (long long)p * C);
+    const int y = p / lf.Wp, x = p - y * lf.Wp;
+    float v = 0.0f;
+    if (x < lf.W) {
+        const int Y = y >> 1, X = x >> 1;
+        const int cnt = (min(2 * Y + 2, lf.H) - 2 * Y) * (min(2 * X + 2, lf.W) - 2 * X);
+        v = ge[t] + gp[((size_t)Y * lc.Wp + X) * C + c] / (float)cnt;
+        if (!(__bfloat162float(e[t]) > 0.0f)) v = 0.0f;
+    }
+    ge[t] = v;
+}
+
+// Adam on the float32 master parameters; refreshes the bf16 copy.
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, __nv_bfloat16* __restrict__ pb, long long n, float lr, float b1,
+                            float b2, float eps, float c1, float c2) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    p[i] = pi;
+    pb[i] = __float2bfloat16_rn(pi);
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ p, __nv_bfloat16* __restrict__ pb, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) pb[i] = __float2bfloat16_rn(p[i]);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+
+struct LayerDef {
+    int cin, cout, level, relu, out_f32;
+};
+// conv1 .. conv6 (see the network at the top of this file)
+constexpr LayerDef LAYERS[NLAYERS] = {{32, 32, 0, 1, 0},  {32, 64, 1, 1, 0},  {64, 128, 2, 1, 0},
+                                      {128, 64, 2, 0, 0}, {64, 32, 1, 0, 0},  {32, 16, 0, 0, 1}};
+
+long long layer_wsize(int l) { return 9LL * LAYERS[l].cout * LAYERS[l].cin; }
+
+long long param_offsets(long long* w_off, long long* b_off) {
+    long long o = 0;
+    for (int l = 0; l < NLAYERS; ++l) {
+        if (w_off) w_off[l] = o;
+        o += layer_wsize(l);
+        if (b_off) b_off[l] = o;
+        o += LAYERS[l].cout;
+    }
+    return o;
+}
+
+int make_map_2d(CUtensorMap* m, const void* base, long long rows, int cols, int box_rows) {
+    auto enc = tc_get_encode();
+    if (!enc) return LC3D_ERR_CUDA;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+    cuuint32_t box[2] = {(cuuint32_t)KB, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? LC3D_OK : LC3D_ERR_CUDA;
+}
+
+unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+struct lc3d_predictor {
+    int device = 0, N = 0;
+    Level lv[3];
+    long long np = 0, w_off[NLAYERS], b_off[NLAYERS];
+    float *params = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    __nv_bfloat16* wbf = nullptr;
+    int adam_t = 0;
+    // activations (bf16 NHWC) and the float32 output / target
+    __nv_bfloat16 *x0 = nullptr, *e1 = nullptr, *p1 = nullptr, *e2 = nullptr, *p2 = nullptr, *e3 = nullptr,
+                  *u3 = nullptr, *d2 = nullptr, *u2 = nullptr, *d1 = nullptr;
+    float *y = nullptr, *target = nullptr;
+    // gradients (float32 NHWC)
+    float *g_out = nullptr, *g_d1 = nullptr, *g_u2 = nullptr, *g_d2 = nullptr, *g_u3 = nullptr, *g_e3 = nullptr,
+          *g_p2 = nullptr, *g_p1 = nullptr;
+    unsigned* err = nullptr;
+    double* scale = nullptr;       // [23] per-sample channel scales (device)
+    double* partial = nullptr;     // [STAT_BLOCKS][18]
+    double mult[23];               // scale multipliers (host-set)
+    ConvArgs conv[NLAYERS];
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(lc3d_predictor* P, T** p, size_t count) {
+    void* q = nullptr;
+    LC3D_CUDA_TRY(cudaMalloc(&q, count * sizeof(T)));
+    LC3D_CUDA_TRY(cudaMemset(q, 0, count * sizeof(T)));
+    P->allocs.push_back(q);
+    *p = static_cast<T*>(q);
+    return LC3D_OK;
+}
+
+int setup_conv(lc3d_predictor* P, int l, const __nv_bfloat16* in, void* out) {
+    const LayerDef& d = LAYERS[l];
+    const Level& L = P->lv[d.level];
+    ConvArgs& a = P->conv[l];
+    memset(&a, 0, sizeof(a));
+    LC3D_TRY(make_map_2d(&a.tin, in, L.NP, d.cin, TILE_PIX));
+    LC3D_TRY(make_map_2d(&a.twt, P->wbf + P->w_off[l], 9LL * d.cout, d.cin, d.cout));
+    a.bias = P->params + P->b_off[l];
+    a.out = out;
+    a.out_f32 = d.out_f32;
+    a.relu = d.relu;
+    a.H = L.H; a.W = L.W; a.Wp = L.Wp; a.NP = L.NP;
+    a.Cin = d.cin; a.Cout = d.cout;
+    a.idesc = idesc_bf16(TILE_PIX, d.cout);
+    a.err = P->err;
+    return LC3D_OK;
+}
+
+int run_conv(lc3d_predictor* P, int l, cudaStream_t s) {
+    const ConvArgs& a = P->conv[l];
+    conv3x3_tc_kernel<<<blocks_for(a.NP, TILE_PIX), CONV_THREADS, conv_smem_bytes(), s>>>(a);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+template <int CIN>
+int bwd_data(const float* g, int CG, const __nv_bfloat16* w, const __nv_bfloat16* mask, float* dx, const Level& L,
+             cudaStream_t s) {
+    const size_t smem = ((size_t)BWD_PIX * (CG + 1) + (size_t)CG * CIN) * sizeof(float);
+    conv_bwd_data_kernel<CIN><<<blocks_for(L.NP, BWD_PIX), BWD_THREADS, smem, s>>>(g, CG, w, mask, dx, L);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+template <int CG, int CIN>
+int bwd_weights(lc3d_predictor* P, int l, const float* g, const __nv_bfloat16* x, cudaStream_t s) {
+    const Level& L = P->lv[LAYERS[l].level];
+    const int nchunks = (int)std::min<long long>(128, (L.NP + 1023) / 1024);
+    int chunk = (L.NP + nchunks - 1) / nchunks;
+    chunk = (chunk + WG_SUB - 1) / WG_SUB * WG_SUB;
+    const int nc = (L.NP + chunk - 1) / chunk;
+    conv_bwd_w_kernel<CG, CIN><<<dim3(nc, 9), BWD_THREADS, 0, s>>>(g, x, P->grad + P->w_off[l], L, chunk);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    bias_grad_kernel<<<nc, 128, 0, s>>>(g, CG, P->grad + P->b_off[l], L.NP, chunk);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+int forward(lc3d_predictor* P, cudaStream_t s) {
+    const Level *l0 = &P->lv[0], *l1 = &P->lv[1], *l2 = &P->lv[2];
+    LC3D_TRY(run_conv(P, 0, s));
+    pool_kernel<<<blocks_for((long long)l1->NP * 4, 256), 256, 0, s>>>(P->e1, *l0, P->p1, *l1, 32);
+    LC3D_TRY(run_conv(P, 1, s));
+    pool_kernel<<<blocks_for((long long)l2->NP * 8, 256), 256, 0, s>>>(P->e2, *l1, P->p2, *l2, 64);
+    LC3D_TRY(run_conv(P, 2, s));
+    LC3D_TRY(run_conv(P, 3, s));
+    upadd_relu_kernel<<<blocks_for((long long)l1->NP * 8, 256), 256, 0, s>>>(P->u3, *l2, P->e2, P->d2, *l1, 64);
+    LC3D_TRY(run_conv(P, 4, s));
+    upadd_relu_kernel<<<blocks_for((long long)l0->NP * 4, 256), 256, 0, s>>>(P->u2, *l1, P->e1, P->d1, *l0, 32);
+    LC3D_TRY(run_conv(P, 5, s));
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+int backward(lc3d_predictor* P, float* loss, cudaStream_t s) {
+    const Level &l0 = P->lv[0], &l1 = P->lv[1], &l2 = P->lv[2];
+    const __nv_bfloat16* w = P->wbf;
+    LC3D_CUDA_TRY(cudaMemsetAsync(P->grad, 0, (size_t)P->np * sizeof(float), s));
+    loss_kernel<<<blocks_for(l0.NP, 256), 256, 0, s>>>(P->y, P->target, P->g_out, l0, loss);
+    // conv6: d1 -> y
+    LC3D_TRY((bwd_weights<16, 32>(P, 5, P->g_out, P->d1, s)));
+    LC3D_TRY(bwd_data<32>(P->g_out, 16, w + P->w_off[5], P->d1, P->g_d1, l0, s));
+    downsum_kernel<<<blocks_for((long long)l1.NP * 32, 256), 256, 0, s>>>(P->g_d1, l0, P->g_u2, l1, 32);
+    // conv5: d2 -> u2
+    LC3D_TRY((bwd_weights<32, 64>(P, 4, P->g_u2, P->d2, s)));
+    LC3D_TRY(bwd_data<64>(P->g_u2, 32, w + P->w_off[4], P->d2, P->g_d2, l1, s));
+    downsum_kernel<<<blocks_for((long long)l2.NP * 64, 256), 256, 0, s>>>(P->g_d2, l1, P->g_u3, l2, 64);
+    // conv4: e3 -> u3
+    LC3D_TRY((bwd_weights<64, 128>(P, 3, P->g_u3, P->e3, s)));
+    LC3D_TRY(bwd_data<128>(P->g_u3, 64, w + P->w_off[3], P->e3, P->g_e3, l2, s));
+    // conv3: p2 -> e3
+    LC3D_TRY((bwd_weights<128, 64>(P, 2, P->g_e3, P->p2, s)));
+    LC3D_TRY(bwd_data<64>(P->g_e3, 128, w + P->w_off[2], nullptr, P->g_p2, l2, s));
+    pool_bwd_mask_kernel<<<blocks_for((long long)l1.NP * 64, 256), 256, 0, s>>>(P->g_d2, P->e2, l1, P->g_p2, l2, 64);
+    // conv2: p1 -> e2 (g_d2 now holds dL/d pre-activation of e2)
+    LC3D_TRY((bwd_weights<64, 32>(P, 1, P->g_d2, P->p1, s)));
+    LC3D_TRY(bwd_data<32>(P->g_d2, 64, w + P->w_off[1], nullptr, P->g_p1, l1, s));
+    pool_bwd_mask_kernel<<<blocks_for((long long)l0.NP * 32, 256), 256, 0, s>>>(P->g_d1, P->e1, l0, P->g_p1, l1, 32);
+    // conv1: x0 -> e1
+    LC3D_TRY((bwd_weights<32, 32>(P, 0, P->g_d1, P->x0, s)));
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+struct PredDevice {
+    int dev;
+    explicit PredDevice(int d) {
+        cudaGetDevice(&dev);
+        cudaSetDevice(d);
+    }
+    ~PredDevice() { cudaSetDevice(dev); }
+};
+
+cudaStream_t St(void* s) { return static_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+extern "C" {
+
+long long lc3d_predictor_num_params(void) { return param_offsets(nullptr, nullptr); }
+
+int lc3d_predictor_create(int grid_steps, int device, lc3d_predictor** out) {
+    if (!out || grid_steps < 9 || grid_steps > 4097) return LC3D_ERR_PARAM;
+    *out = nullptr;
+    PredDevice g(device);
+    lc3d_predictor* P = new lc3d_predictor();
+    P->device = device;
+    P->N = grid_steps;
+    int H = grid_steps;
+    for (int k = 0; k < 3; ++k) {
+        P->lv[k] = Level{H, H, H + 1, H * (H + 1)};
+        H = (H + 1) / 2;
+    }
+    P->np = param_offsets(P->w_off, P->b_off);
+    for (int c = 0; c < 23; ++c) P->mult[c] = 1.0;
+    const size_t n0 = P->lv[0].NP, n1 = P->lv[1].NP, n2 = P->lv[2].NP;
+    int rc = LC3D_OK;
+#define PA(ptr, cnt) \
+    if (rc == LC3D_OK) rc = dalloc(P, &(ptr), (cnt))
+    PA(P->params, P->np); PA(P->grad, P->np); PA(P->adam_m, P->np); PA(P->adam_v, P->np); PA(P->wbf, P->np);
+    PA(P->x0, n0 * 32); PA(P->e1, n0 * 32); PA(P->p1, n1 * 32); PA(P->e2, n1 * 64); PA(P->p2, n2 * 64);
+    PA(P->e3, n2 * 128); PA(P->u3, n2 * 64); PA(P->d2, n1 * 64); PA(P->u2, n1 * 32); PA(P->d1, n0 * 32);
+    PA(P->y, n0 * 16); PA(P->target, n0 * 16);
+    PA(P->g_out, n0 * 16); PA(P->g_d1, n0 * 32); PA(P->g_u2, n1 * 32); PA(P->g_d2, n1 * 64);
+    PA(P->g_u3, n2 * 64); PA(P->g_e3, n2 * 128); PA(P->g_p2, n2 * 64); PA(P->g_p1, n1 * 32);
+    PA(P->err, 1); PA(P->scale, 23); PA(P->partial, (size_t)STAT_BLOCKS * 18);
+#undef PA
+    if (rc == LC3D_OK) rc = setup_conv(P, 0, P->x0, P->e1);
+    if (rc == LC3D_OK) rc = setup_conv(P, 1, P->p1, P->e2);
+    if (rc == LC3D_OK) rc = setup_conv(P, 2, P->p2, P->e3);
+    if (rc == LC3D_OK) rc = setup_conv(P, 3, P->e3, P->u3);
+    if (rc == LC3D_OK) rc = setup_conv(P, 4, P->d2, P->u2);
+    if (rc == LC3D_OK) rc = setup_conv(P, 5, P->d1, P->y);
+    if (rc == LC3D_OK) {
+        static bool attrs_set[64] = {};
+        bool& attrs = attrs_set[device & 63];
+        if (!attrs) {
+            cudaFuncSetAttribute(conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem_bytes());
+            cudaFuncSetAttribute(conv_bwd_data_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+            cudaFuncSetAttribute(conv_bwd_data_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+            cudaFuncSetAttribute(conv_bwd_data_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+            attrs = cudaGetLastError() == cudaSuccess;
+            if (!attrs) rc = LC3D_ERR_CUDA;
+        }
+    }
+    if (rc != LC3D_OK) {
+        lc3d_predictor_destroy(P);
+        return rc;
+    }
+    *out = P;
+    return LC3D_OK;
+}
+
+int lc3d_predictor_destroy(lc3d_predictor* P) {
+    if (!P) return LC3D_OK;
+    PredDevice g(P->device);
+    for (void* q : P->allocs) cudaFree(q);
+    delete P;
+    return LC3D_OK;
+}
+
+int lc3d_predictor_set_params(lc3d_predictor* P, const float* params, void* stream) {
+    if (!P || !params) return LC3D_ERR_PARAM;
+    PredDevice g(P->device);
+    LC3D_CUDA_TRY(cudaMemcpyAsync(P->params, params, (size_t)P->np * sizeof(float), cudaMemcpyDeviceToDevice,
+                                  St(stream)));
+    to_bf16_kernel<<<blocks_for(P->np, 256), 256, 0, St(stream)>>>(P->params, P->wbf, P->np);
+    LC3D_CUDA_TRY(cudaMemsetAsync(P->adam_m, 0, (size_t)P->np * sizeof(float), St(stream)));
+    LC3D_CUDA_TRY(cudaMemsetAsync(P->adam_v, 0, (size_t)P->np * sizeof(float), St(stream)));
+    P->adam_t = 0;
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+int lc3d_predictor_get_params(lc3d_predictor* P, float* params, void* stream) {
+    if (!P || !params) return LC3D_ERR_PARAM;
+    PredDevice g(P->device);
+    LC3D_CUDA_TRY(cudaMemcpyAsync(params, P->params, (size_t)P->np * sizeof(float), cudaMemcpyDeviceToDevice,
+                                  St(stream)));
+    return LC3D_OK;
+}
+
+int lc3d_predictor_get_grad(lc3d_predictor* P, float* grad, void* stream) {
+    if (!P || !grad) return LC3D_ERR_PARAM;
+    PredDevice g(P->device);
+    LC3D_CUDA_TRY(cudaMemcpyAsync(grad, P->grad, (size_t)P->np * sizeof(float), cudaMemcpyDeviceToDevice,
+                                  St(stream)));
+    return LC3D_OK;
+}
+
+int lc3d_predictor_set_scales(lc3d_predictor* P, const double* in_mult, const double* out_mult) {
+    if (!P || !in_mult || !out_mult) return LC3D_ERR_PARAM;
+    for (int c = 0; c < 18; ++c)
+        if (!(in_mult[c] > 0) || !std::isfinite(in_mult[c])) return LC3D_ERR_PARAM;
+    for (int c = 0; c < 5; ++c)
+        if (!(out_mult[c] > 0) || !std::isfinite(out_mult[c])) return LC3D_ERR_PARAM;
+    memcpy(P->mult, in_mult, 18 * sizeof(double));
+    memcpy(P->mult + 18, out_mult, 5 * sizeof(double));
+    return LC3D_OK;
+}
+
+int lc3d_predictor_pack(lc3d_predictor* P, const double* const* f1, const double* const* f2, void* stream) {
+    if (!P || !f1 || !f2) return LC3D_ERR_PARAM;
+    PackArgs a;
+    for (int c = 0; c < 9; ++c) {
+        if (!f1[c] || !f2[c]) return LC3D_ERR_PARAM;
+        a.f1[c] = f1[c];
+        a.f2[c] = f2[c];
+    }
+    a.scale = P->scale;
+    a.partial = P->partial;
+    memcpy(a.mult, P->mult, sizeof(a.mult));
+    a.x0 = P->x0;
+    a.L = P->lv[0];
+    PredDevice g(P->device);
+    stats_kernel<<<STAT_BLOCKS, 256, 0, St(stream)>>>(a);
+    scale_final_kernel<<<1, 32, 0, St(stream)>>>(a);
+    pack_kernel<<<blocks_for(a.L.NP, 128), 128, 0, St(stream)>>>(a);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+int lc3d_predictor_forward(lc3d_predictor* P, void* stream) {
+    if (!P) return LC3D_ERR_PARAM;
+    PredDevice g(P->device);
+    return forward(P, St(stream));
+}
+
+static int out_args(lc3d_predictor* P, OutArgs* a, const double* const* f1, const double* const* f2, bool ez) {
+    memset(a, 0, sizeof(*a));
+    for (int f = 0; f < 6; ++f) {
+        if ((f != 2 || ez) && (!f1[f] || !f2[f])) return LC3D_ERR_PARAM;
+        a->f1[f] = f1[f];
+        a->f2[f] = f2[f];
+    }
+    a->scale = P->scale;
+    a->y = P->y;
+    a->target = P->target;
+    a->L = P->lv[0];
+    return LC3D_OK;
+}
+
+int lc3d_predictor_predict(lc3d_predictor* P, const double* const* f1, const double* const* f2,
+                           double* const* pred, void* stream) {
+    if (!P || !f1 || !f2 || !pred) return LC3D_ERR_PARAM;
+    OutArgs a;
+    LC3D_TRY(out_args(P, &a, f1, f2, true));
+    for (int f = 0; f < 6; ++f) {
+        if (!pred[f]) return LC3D_ERR_PARAM;
+        a.pred[f] = pred[f];
+    }
+    PredDevice g(P->device);
+    unpack_kernel<<<blocks_for((long long)P->N * P->N, 256), 256, 0, St(stream)>>>(a);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+int lc3d_predictor_set_target(lc3d_predictor* P, const double* const* first, const double* const* f1,
+                              const double* const* f2, void* stream) {
+    if (!P || !first || !f1 || !f2) return LC3D_ERR_PARAM;
+    OutArgs a;
+    LC3D_TRY(out_args(P, &a, f1, f2, false));
+    for (int k = 0; k < 5; ++k) {
+        if (!first[net_field(k)]) return LC3D_ERR_PARAM;
+        a.first[net_field(k)] = first[net_field(k)];
+    }
+    PredDevice g(P->device);
+    target_kernel<<<blocks_for(P->lv[0].NP, 128), 128, 0, St(stream)>>>(a);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+int lc3d_predictor_backward(lc3d_predictor* P, float* loss, void* stream) {
+    if (!P || !loss) return LC3D_ERR_PARAM;
+    PredDevice g(P->device);
+    return backward(P, loss, St(stream));
+}
+
+int lc3d_predictor_adam(lc3d_predictor* P, float lr, void* stream) {
+    if (!P || !(lr > 0)) return LC3D_ERR_PARAM;
+    PredDevice g(P->device);
+    const float b1 = 0.9f, b2 = 0.999f;
+    P->adam_t += 1;
+    const float c1 = 1.0f - powf(b1, (float)P->adam_t), c2 = 1.0f - powf(b2, (float)P->adam_t);
+    adam_kernel<<<blocks_for(P->np, 256), 256, 0, St(stream)>>>(P->params, P->grad, P->adam_m, P->adam_v, P->wbf,
+                                                                P->np, lr, b1, b2, 1e-8f, c1, c2);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+int lc3d_predictor_tensor(lc3d_predictor* P, int which, void** ptr, long long* bytes) {
+    if (!P || !ptr || !bytes) return LC3D_ERR_PARAM;
+    const long long n0 = P->lv[0].NP;
+    switch (which) {
+        case LC3D_PRED_INPUT: *ptr = P->x0; *bytes = n0 * 32 * 2; break;
+        case LC3D_PRED_OUTPUT: *ptr = P->y; *bytes = n0 * 16 * 4; break;
+        case LC3D_PRED_TARGET: *ptr = P->target; *bytes = n0 * 16 * 4; break;
+        default: return LC3D_ERR_PARAM;
+    }
+    return LC3D_OK;
+}
+
+int lc3d_predictor_check_error(lc3d_predictor* P, void* stream) {
+    if (!P) return LC3D_ERR_PARAM;
+    PredDevice g(P->device);
+    unsigned h = 0;
+    LC3D_CUDA_TRY(cudaMemcpyAsync(&h, P->err, sizeof(unsigned), cudaMemcpyDeviceToHost, St(stream)));
+    LC3D_CUDA_TRY(cudaStreamSynchronize(St(stream)));
+    if (h) {
+        LC3D_CUDA_TRY(cudaMemsetAsync(P->err, 0, sizeof(unsigned), St(stream)));
+        return LC3D_ERR_TIMEOUT;
+    }
+    return LC3D_OK;
+}
+
+}  // extern "C"

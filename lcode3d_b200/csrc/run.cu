@@ -24,18 +24,28 @@ struct RunCtl {
     double* ez;    // history of the current run (may be NULL)
 };
 
-__global__ void __launch_bounds__(256) beam_kernel(double* out, int N, double h, double dxi, double A, double sr,
-                                                   double lf, const RunCtl* ctl) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= N * N) return;
+__device__ __forceinline__ double beam_value(int k, int N, double h, double xi, double A, double sr, double lf) {
     const int i = k / N, j = k - i * N;
-    const double xi = ctl->xi * dxi;
     double v = 0;
     if (xi >= 0 && xi <= 2 * sqrt(2 * M_PI) * lf) {
         const double x = (i - N / 2) * h, y = (j - N / 2) * h;
         v = A * exp(-(x * x + y * y) / (2 * sr * sr)) * 0.5 * (1 - cos(sqrt(M_PI / 2) * xi / lf));
     }
-    out[k] = v;
+    return v;
+}
+
+__global__ void __launch_bounds__(256) beam_kernel(double* out, int N, double h, double dxi, double A, double sr,
+                                                   double lf, const RunCtl* ctl) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N * N) return;
+    out[k] = beam_value(k, N, h, ctl->xi * dxi, A, sr, lf);
+}
+
+__global__ void __launch_bounds__(256) beam_at_kernel(double* out, int N, double h, double xi, double A, double sr,
+                                                      double lf) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N * N) return;
+    out[k] = beam_value(k, N, h, xi, A, sr, lf);
 }
 
 __global__ void record_kernel(const double* Ez, int center, RunCtl* ctl) {
@@ -151,6 +161,23 @@ extern "C" int lc3d_set_beam(lc3d_ctx* c, const lc3d_beam_params* b) {
     c->beam_A = A;
     c->beam_sr = sr;
     c->beam_lf = lf;
+    return LC3D_OK;
+}
+
+extern "C" int lc3d_beam_eval(lc3d_ctx* c, int xi_i, double* beam_ro, void* stream) {
+    if (!c || !beam_ro) return LC3D_ERR_PARAM;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != c->device) cudaSetDevice(c->device);
+    const int N = c->N;
+    beam_at_kernel<<<(N * N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        beam_ro, N, c->p.grid_step_size, xi_i * c->p.xi_step_size, c->beam_A, c->beam_sr, c->beam_lf);
+    const cudaError_t e = cudaGetLastError();
+    if (dev >= 0 && dev != c->device) cudaSetDevice(dev);
+    if (e != cudaSuccess) {
+        lc3d_set_last_cuda_error(e, "beam_at_kernel", __FILE__, __LINE__);
+        return LC3D_ERR_CUDA;
+    }
     return LC3D_OK;
 }
 
