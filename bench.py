@@ -481,6 +481,76 @@ def run_scan(args, rank, world, dist):
     }
 
 
+def run_learned_bench(args):
+    """The learned first pass on the bench workload: ``pre`` plain steps into
+    the beam, W warm-up and K timed steps under periodic verification
+    (lcode3d_b200.predictor.learned_steps; verification syncs included in
+    the timed region), and the same K steps by the plain method from the
+    same state for the Ez(N/2, N/2) error and the same-GPU comparison."""
+    import torch
+    from lcode3d_b200 import predictor as P
+    from lcode3d_b200 import train_predictor as T
+
+    dev = int(os.environ.get('LOCAL_RANK', 0))
+    torch.cuda.set_device(dev)
+    path = T.DEFAULT_WEIGHTS if args.learned == 'default' else args.learned
+    if not os.path.exists(path):
+        return {'impl': 'ours', 'form': 'fp64+learned',
+                'unavailable': f'no trained parameters at {os.path.relpath(path, ROOT)} '
+                               '(python -m lcode3d_b200.train_predictor writes them)'}
+    cfg = make_config(args.grid, 'fp64')
+    N = cfg.grid_steps
+    A = GRIDS[args.grid][2]
+    pr = P.FieldPredictor.load(path, grid_steps=N)
+    K, W = args.steps, args.warmup
+
+    def advance(sim, learned):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if learned:
+            P.learned_steps(sim, pr, W, args.tol, args.verify_every, 0, False)
+        else:
+            for _ in range(W):
+                sim.step_plain()
+        torch.cuda.synchronize()
+        ev0.record()
+        if learned:
+            ez, st = P.learned_steps(sim, pr, K, args.tol, args.verify_every, 0, True)
+        else:
+            ez = []
+            for _ in range(K):
+                sim.step_plain()
+                ez.append(sim.state.Ez[N // 2, N // 2].clone())
+            st = None
+        ev1.record()
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1), torch.stack(ez).cpu().numpy(), st
+
+    sims = []
+    for _ in range(2):
+        sim = P.Stepper(cfg, (A, 1.0, 1.0))
+        for _ in range(args.pre):
+            sim.step_plain()
+        sims.append(sim)
+    clocks = Clocks(dev)
+    clocks.start()
+    ms_l, ez_l, st = advance(sims[0], True)
+    clk = clocks.stop()
+    ms_p, ez_p, _ = advance(sims[1], False)
+    err = float(np.abs(ez_l - ez_p).max() / max(np.abs(ez_p).max(), 1e-300))
+    return {
+        'metric': 'xi-steps/s', 'value': K / (ms_l * 1e-3), 'unit': 'xi-steps/s', 'n_gpus': 1, 'steps': K,
+        'warmup': W, 'ms_per_step': ms_l / K, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f64+bf16', 'form': 'fp64+learned',
+        'data': 'synthetic (generated cold uniform plasma + axisymmetric beam; no dataset)',
+        'config': {'workload': f'LCODE 3D xi step, {N}x{N} grid, learned first pass (U-Net, tcgen05) with '
+                               f'periodic verification, tol {args.tol:g}, every {args.verify_every} steps',
+                   'grid_steps': N, 'start_xi_step': args.pre, 'weights': os.path.relpath(path, ROOT),
+                   'l2': 'not flushed', 'parallelism': 'single GPU'},
+        'learned': st, 'plain_same_steps': {'value': K / (ms_p * 1e-3), 'ms_per_step': ms_p / K},
+        'ez_max_rel_err_vs_plain': err, 'clocks': clk,
+    }
+
+
 def run_reference(args):
     threads = cpu_threads()
     K = max(1, min(args.steps, args.ref_max_steps))
@@ -522,6 +592,10 @@ def main():
     ap.add_argument('--scan', type=int, default=0,
                     help='batched parameter scan of this many simulations instead of the single-grid workload')
     ap.add_argument('--seed', type=int, default=2025, help='seed of the scan draws')
+    ap.add_argument('--learned', nargs='?', const='default', default=None,
+                    help='learned first pass with these trained parameters (.npz; default: the packaged ones)')
+    ap.add_argument('--tol', type=float, default=1e-6, help='learned: verification tolerance on max|pred - F1| / max|F1|')
+    ap.add_argument('--verify-every', type=int, default=10, help='learned: steps between verifications')
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == 'ours':
         args.warmup = 3
@@ -539,6 +613,13 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+    if args.learned:
+        if rank == 0:
+            print(json.dumps(run_learned_bench(args)), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.scan:
         out = run_scan(args, rank, world, dist)
         if rank == 0:

@@ -342,21 +342,19 @@ def evaluate(predictor, samples):
     return net / len(samples), base / len(samples)
 
 
-def run_learned(config, beam, nsteps, predictor, tol=1e-6, verify_every=10, warm=20, record=True):
-    """Run ``nsteps`` steps from the initial state with the learned first
-    pass under periodic verification: ``warm`` plain steps, then every
-    ``verify_every``-th step is a plain step that also checks the network
-    against that step's true first-pass fields (Stepper.step_verify); while
-    the last check's error max|pred - F1| / max|F1| is within ``tol`` the
-    steps in between use the prediction, otherwise they are plain (the
-    fallback). Returns (Ez(N/2, N/2) history or None, stats, the Stepper)."""
-    sim = Stepper(config, beam)
-    N = config.grid_steps
+def learned_steps(sim, predictor, nsteps, tol=1e-6, verify_every=10, warm=0, record=True):
+    """Advance ``sim`` (a Stepper) by ``nsteps`` steps with the learned first
+    pass under periodic verification: the first ``warm`` steps are plain,
+    then every ``verify_every``-th step is a plain step that also checks the
+    network against that step's true first-pass fields
+    (Stepper.step_verify); while the last check's error max|pred - F1| /
+    max|F1| is within ``tol`` the steps in between use the prediction,
+    otherwise they are plain (the fallback). Returns (list of Ez(N/2, N/2)
+    device scalars, or [] without ``record``; counters)."""
+    N = sim.config.grid_steps
     ez, errs = [], []
     n_learned = n_plain = n_verify = n_fail = 0
     use = False
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
     for i in range(nsteps):
         if i < warm:
             sim.step_plain()
@@ -375,13 +373,25 @@ def run_learned(config, beam, nsteps, predictor, tol=1e-6, verify_every=10, warm
             n_plain += 1
         if record:
             ez.append(sim.state.Ez[N // 2, N // 2].clone())
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
     stats = {'steps': nsteps, 'learned_steps': n_learned, 'plain_steps': n_plain, 'verify_steps': n_verify,
              'first_passes_saved': n_learned, 'fallback_rate': (n_fail / n_verify) if n_verify else None,
              'pred_err_median': float(np.median(errs)) if errs else None,
-             'pred_err_max': float(np.max(errs)) if errs else None, 'tol': tol, 'verify_every': verify_every,
-             'wall_s': wall, 'xi_steps_per_s': nsteps / wall}
+             'pred_err_max': float(np.max(errs)) if errs else None, 'tol': tol, 'verify_every': verify_every}
+    return ez, stats
+
+
+def run_learned(config, beam, nsteps, predictor, tol=1e-6, verify_every=10, warm=20, record=True):
+    """Run ``nsteps`` steps from the initial state (learned_steps after
+    ``warm`` plain steps). Returns (Ez(N/2, N/2) history or None, stats, the
+    Stepper)."""
+    sim = Stepper(config, beam)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ez, stats = learned_steps(sim, predictor, nsteps, tol, verify_every, warm, record)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    stats['wall_s'] = wall
+    stats['xi_steps_per_s'] = nsteps / wall
     return (torch.stack(ez).cpu().numpy() if record else None), stats, sim
 
 
