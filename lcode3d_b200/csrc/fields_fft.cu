@@ -30,9 +30,16 @@
 
 namespace {
 
-constexpr int FFT_THREADS = 256;
-constexpr int FFT_PER_CTA = 2;           // complex FFTs per CTA (4 rows)
+#ifndef LC3D_FFT_THREADS
+#define LC3D_FFT_THREADS 256
+#endif
+#ifndef LC3D_FFT_PER_CTA
+#define LC3D_FFT_PER_CTA 2
+#endif
+constexpr int FFT_THREADS = LC3D_FFT_THREADS;
+constexpr int FFT_PER_CTA = LC3D_FFT_PER_CTA;   // complex FFTs per CTA (1 or 2; two rows each)
 constexpr int ROWS_PER_CTA = 2 * FFT_PER_CTA;
+static_assert(FFT_PER_CTA == 1 || FFT_PER_CTA == 2, "one or two FFTs per CTA");
 #ifndef LC3D_FFT_MAX_RADIX
 #define LC3D_FFT_MAX_RADIX 8              // largest power-of-two butterfly in a plan (8 or 4)
 #endif
@@ -197,12 +204,11 @@ __device__ __forceinline__ void dif_butterfly(double2* A, int b, int span, float
 
 template <int R>
 __device__ __forceinline__ void fft_pass(double2* A, int span, int P, const double2* tw) {
-    static_assert(FFT_PER_CTA == 2, "the FFT index below assumes two FFTs per CTA");
     const int nb = P / R;
     const float inv_span = 1.0f / (float)span;
     const int tstep = P / (span * R);   // twiddle stride of this pass
     for (int t = threadIdx.x; t < FFT_PER_CTA * nb; t += FFT_THREADS) {
-        const int q = t >= nb, j = t - q * nb;
+        const int q = FFT_PER_CTA == 2 && t >= nb, j = t - q * nb;
         dif_butterfly<R>(A + q * (P + FFT_PAD), j, span, inv_span, tstep, P, tw);
     }
 }
@@ -277,8 +283,8 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
     }
     // transposed output: out[k][row] for the CTA's rows. The readout list
     // holds (position, k) for the wanted frequencies sorted by position, so
-    // a warp reads nearly consecutive shared-memory words; thread pairs
-    // (FFT 0, FFT 1) of one entry write 4 consecutive rows of out[k].
+    // a warp reads nearly consecutive shared-memory words; the threads of
+    // one entry (one per FFT) write the CTA's consecutive rows of out[k].
     const int* rl = b.rd + (F.type ? b.N : 0);
     const int total = n * FFT_PER_CTA;
     constexpr int SU = 8;
@@ -287,12 +293,12 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
 #pragma unroll
         for (int u = 0; u < SU; ++u) {
             const int t = t0 + u * FFT_THREADS + (int)threadIdx.x;
-            e[u] = t < total ? __ldg(rl + (t >> 1)) : 0;
+            e[u] = t < total ? __ldg(rl + t / FFT_PER_CTA) : 0;
         }
 #pragma unroll
         for (int u = 0; u < SU; ++u) {
             const int t = t0 + u * FFT_THREADS + (int)threadIdx.x;
-            const int q = t & 1, row = r0 + 2 * q;
+            const int q = t % FFT_PER_CTA, row = r0 + 2 * q;
             if (t >= total || row >= F.rows) continue;
             const double2 z = A[q * PS + (e[u] >> 16)];
             double* o = F.out + (size_t)(e[u] & 0xffff) * F.ld_out + row;
