@@ -335,7 +335,8 @@ int fields_init(lc3d_ctx* c) {
         LC3D_CUDA_TRY(cudaMemset(c->raw[f], 0, plane));
     }
     c->red_blocks = 160;
-    LC3D_CUDA_TRY(cudaMalloc(&c->red, c->red_blocks * sizeof(double)));
+    // room for the partial-sum kernel's blocks and for the FFT pass's per-CTA sums
+    LC3D_CUDA_TRY(cudaMalloc(&c->red, 4096 * sizeof(double)));
     return LC3D_OK;
 }
 
@@ -420,6 +421,7 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
             dst[f] = c->raw[f];
         }
     }
+    int bz_partials = 0;   // > 0: the FFT pass left this many Bz partial sums in c->red
     if (c->p.precision == LC3D_PREC_MIXED) {
         // four split-BF16 tensor-core GEMM stages (fields_mixed.cu)
         for (int stage = 0; stage < 4; ++stage) {
@@ -475,7 +477,12 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
                     case 1: e.in = c->t1[f]; e.rows = g.cols; e.type = g.type0; e.out = c->t2[f]; break;
                     case 2: e.in = c->t2[f]; e.rows = g.rows; e.type = g.type1; e.out = c->t1[f];
                             e.lam = g.Lam; e.ld_lam = g.ldLam; break;   // Lambda o Z, row by row
-                    default: e.in = c->t1[f]; e.rows = g.cols; e.type = g.type0; e.out = dst[f] + g.off; break;
+                    default: e.in = c->t1[f]; e.rows = g.cols; e.type = g.type0; e.out = dst[f] + g.off;
+                             if (f == 5) {   // Bz: the mean's partial sums come with the last pass
+                                 e.partial = c->red;
+                                 bz_partials = (g.cols + fft_cta_rows() - 1) / fft_cta_rows();
+                             }
+                             break;
                 }
             }
             LC3D_TRY(fft_rows(c, d, cnt, s));
@@ -521,16 +528,17 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
         }
     }
     const double inv_n = 1.0 / n;
-    if (on[5]) {
+    if (on[5] && !bz_partials) {
         ProfScope ps(c, LC3D_STAGE_FIELD_FIN, s);
         partial_sum_kernel<<<c->red_blocks, RED_THREADS, 0, s>>>(dst[5], n, c->red);
         LC3D_CUDA_TRY(cudaGetLastError());
     }
+    const int nred = bz_partials ? bz_partials : c->red_blocks;
     if (o.mode == 0) {
         if (on[5]) {
             ProfScope ps(c, LC3D_STAGE_FIELD_FIN, s);
             subtract_mean_kernel<<<(n + RED_THREADS - 1) / RED_THREADS, RED_THREADS, 0, s>>>(
-                dst[5], n, c->red, c->red_blocks, inv_n);
+                dst[5], n, c->red, nred, inv_n);
             LC3D_CUDA_TRY(cudaGetLastError());
         }
         return LC3D_OK;
@@ -545,7 +553,7 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
         fa.avg[f] = o.avg[f];
     }
     fa.partial = c->red;
-    fa.nblocks = c->red_blocks;
+    fa.nblocks = nred;
     fa.n = n;
     fa.variant_A = c->p.field_solver_variant_A;
     fa.has_bz = on[5];

@@ -40,6 +40,7 @@ constexpr int FFT_THREADS = LC3D_FFT_THREADS;
 constexpr int FFT_PER_CTA = LC3D_FFT_PER_CTA;   // complex FFTs per CTA (1 or 2; two rows each)
 constexpr int ROWS_PER_CTA = 2 * FFT_PER_CTA;
 static_assert(FFT_PER_CTA == 1 || FFT_PER_CTA == 2, "one or two FFTs per CTA");
+static_assert((FFT_THREADS & (FFT_THREADS - 1)) == 0, "the partial-sum tree assumes a power-of-two CTA");
 #ifndef LC3D_FFT_MAX_RADIX
 #define LC3D_FFT_MAX_RADIX 8              // largest power-of-two butterfly in a plan (8 or 4)
 #endif
@@ -56,6 +57,7 @@ struct FftField {
     int ld_out;
     const double* lam;
     int ld_lam;
+    double* partial;                     // per-CTA sums of the written values, or NULL
     int cta_start;
 };
 
@@ -287,6 +289,7 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
     // one entry (one per FFT) write the CTA's consecutive rows of out[k].
     const int* rl = b.rd + (F.type ? b.N : 0);
     const int total = n * FFT_PER_CTA;
+    double psum = 0.0;
     constexpr int SU = 8;
     for (int t0 = 0; t0 < total; t0 += SU * FFT_THREADS) {
         int e[SU];
@@ -302,9 +305,25 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
             if (t >= total || row >= F.rows) continue;
             const double2 z = A[q * PS + (e[u] >> 16)];
             double* o = F.out + (size_t)(e[u] & 0xffff) * F.ld_out + row;
-            o[0] = F.type == 0 ? z.x : -z.y;
-            if (row + 1 < F.rows) o[1] = F.type == 0 ? z.y : z.x;
+            const double x0 = F.type == 0 ? z.x : -z.y, x1 = F.type == 0 ? z.y : z.x;
+            o[0] = x0;
+            psum += x0;
+            if (row + 1 < F.rows) {
+                o[1] = x1;
+                psum += x1;
+            }
         }
+    }
+    if (F.partial) {   // uniform per CTA: fixed-order sum of everything this CTA wrote
+        __syncthreads();   // the FFT buffer is free
+        double* red = reinterpret_cast<double*>(sm);
+        red[threadIdx.x] = psum;
+        __syncthreads();
+        for (int h = FFT_THREADS / 2; h > 0; h >>= 1) {
+            if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) F.partial[blockIdx.x - F.cta_start] = red[0];
     }
 }
 
@@ -331,6 +350,8 @@ int fft_plan(int P, int* rad) {
         while ((f <= LC3D_FFT_MAX_RADIX || f % 2) && r % f == 0 && n < MAX_RADICES) { rad[n++] = f; r /= f; }
     return (r == 1) ? n : 0;
 }
+
+int fft_cta_rows() { return ROWS_PER_CTA; }
 
 size_t fft_smem_bytes(int P) { return ((size_t)FFT_PER_CTA * P + (FFT_PER_CTA - 1) * FFT_PAD) * sizeof(double2); }
 
@@ -401,6 +422,7 @@ int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, cudaStream_t s) {
         FftField& f = b.f[b.count++];
         f.in = desc[q].in; f.ld_in = desc[q].ld_in; f.rows = desc[q].rows; f.type = desc[q].type;
         f.out = desc[q].out; f.ld_out = desc[q].ld_out; f.lam = desc[q].lam; f.ld_lam = desc[q].ld_lam;
+        f.partial = desc[q].partial;
         f.cta_start = ctas;
         ctas += (f.rows + ROWS_PER_CTA - 1) / ROWS_PER_CTA;
     }

@@ -70,6 +70,7 @@ struct DepositFinalizeArgs {
     const double* ro_initial;             // may be NULL
     double *ro, *jx, *jy, *jz;
     int n;                                // N*N
+    int vec;                              // set by the launcher: 16-byte aligned float64 arrays
 };
 
 int launch_move_estimate(const EstimateArgs& a, cudaStream_t s);
@@ -132,8 +133,10 @@ struct FftRowsDesc {
     int ld_out;
     const double* lam;
     int ld_lam;
+    double* partial;                      // optional: per-CTA sums of the written values
 };
 int fft_init(lc3d_ctx* ctx);
+int fft_cta_rows();                       // rows per CTA: partial sums per field = ceil(rows / this)
 int fft_rows(lc3d_ctx* ctx, const FftRowsDesc* desc, int count, cudaStream_t s);
 int fft_plan(int P, int* rad);
 

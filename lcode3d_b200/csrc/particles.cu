@@ -11,7 +11,7 @@
 //     c = hi * 2^-24 + lo * 2^-76 + (rounding below 2^-77),
 // which are summed with 64-bit integer adds; integer addition is associative,
 // so the sums do not depend on the order in which threads add them, and the
-// final conversion rounds once. Each CTA owns a 16x16 patch of the fine
+// final conversion rounds once. Each CTA owns a 32x32 patch of the fine
 // lattice and accumulates into a shared-memory window placed on the bounding
 // box of its particles' cells; particles whose stencil falls outside the
 // window (strongly displaced plasma) add straight to the global accumulators.
@@ -434,42 +434,66 @@ __global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) 
     }
 }
 
-// Accumulators -> float64 (+ ion background), two cells per thread with
-// 16-byte loads; the accumulators are cleared for the next deposition.
+// Accumulators -> float64 (+ ion background), two cells per thread; the
+// accumulators are cleared for the next deposition. All eight 16-byte
+// accumulator loads of a thread are issued before any store (the clears
+// could alias later loads for the compiler otherwise, serialising them);
+// the float64 side uses 16-byte accesses when every array allows it.
 __global__ void __launch_bounds__(256) deposit_finalize_kernel(DepositFinalizeArgs f) {
     const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     if (k >= f.n) return;
     const size_t P = f.plane;
-    double out[4][2];
+    unsigned long long* acc = f.acc;
     if (k + 1 < f.n) {
+        ulonglong2 w[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) w[q] = __ldcg(reinterpret_cast<const ulonglong2*>(acc + q * P + k));
+        double2 ri = make_double2(0.0, 0.0);
+        if (f.ro_initial) {
+            if (f.vec) {
+                ri = __ldg(reinterpret_cast<const double2*>(f.ro_initial + k));
+            } else {
+                ri.x = __ldg(f.ro_initial + k);
+                ri.y = __ldg(f.ro_initial + k + 1);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) __stcg(reinterpret_cast<ulonglong2*>(acc + q * P + k), make_ulonglong2(0ull, 0ull));
+        double2 o[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            o[q] = make_double2(fx_value((long long)w[2 * q].x, (long long)w[2 * q + 1].x),
+                                fx_value((long long)w[2 * q].y, (long long)w[2 * q + 1].y));
+        if (f.ro_initial) {
+            o[0].x += ri.x;
+            o[0].y += ri.y;
+        }
+        double* dst[4] = {f.ro, f.jx, f.jy, f.jz};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            ulonglong2* hp = reinterpret_cast<ulonglong2*>(f.acc + (2 * q) * P + k);
-            ulonglong2* lp = reinterpret_cast<ulonglong2*>(f.acc + (2 * q + 1) * P + k);
-            const ulonglong2 h = *hp, l = *lp;
-            *hp = make_ulonglong2(0ull, 0ull);
-            *lp = make_ulonglong2(0ull, 0ull);
-            out[q][0] = fx_value((long long)h.x, (long long)l.x);
-            out[q][1] = fx_value((long long)h.y, (long long)l.y);
+            if (f.vec) {
+                *reinterpret_cast<double2*>(dst[q] + k) = o[q];
+            } else {
+                dst[q][k] = o[q].x;
+                dst[q][k + 1] = o[q].y;
+            }
         }
     } else {
+        double out[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            unsigned long long* hp = f.acc + (2 * q) * P + k;
-            unsigned long long* lp = f.acc + (2 * q + 1) * P + k;
-            out[q][0] = fx_value((long long)*hp, (long long)*lp);
+            unsigned long long* hp = acc + (2 * q) * P + k;
+            unsigned long long* lp = acc + (2 * q + 1) * P + k;
+            out[q] = fx_value((long long)*hp, (long long)*lp);
             *hp = 0ull;
             *lp = 0ull;
         }
-    }
-    const int nk = (k + 1 < f.n) ? 2 : 1;
-    for (int e = 0; e < nk; ++e) {
-        double ro = out[0][e];
-        if (f.ro_initial) ro += f.ro_initial[k + e];
-        f.ro[k + e] = ro;
-        f.jx[k + e] = out[1][e];
-        f.jy[k + e] = out[2][e];
-        f.jz[k + e] = out[3][e];
+        double ro = out[0];
+        if (f.ro_initial) ro += f.ro_initial[k];
+        f.ro[k] = ro;
+        f.jx[k] = out[1];
+        f.jy[k] = out[2];
+        f.jz[k] = out[3];
     }
 }
 
@@ -502,7 +526,12 @@ int launch_deposit_main(const DepositArgs& a, cudaStream_t s) {
     return LC3D_OK;
 }
 
-int launch_deposit_finalize(const DepositFinalizeArgs& f, cudaStream_t s) {
+int launch_deposit_finalize(const DepositFinalizeArgs& f_in, cudaStream_t s) {
+    DepositFinalizeArgs f = f_in;
+    const uintptr_t al = reinterpret_cast<uintptr_t>(f.ro) | reinterpret_cast<uintptr_t>(f.jx) |
+                         reinterpret_cast<uintptr_t>(f.jy) | reinterpret_cast<uintptr_t>(f.jz) |
+                         reinterpret_cast<uintptr_t>(f.ro_initial);
+    f.vec = (al & 15) == 0;
     deposit_finalize_kernel<<<((f.n + 1) / 2 + 255) / 256, 256, 0, s>>>(f);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
