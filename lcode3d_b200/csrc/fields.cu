@@ -33,12 +33,21 @@ namespace {
 struct RhsArgs {
     SolveInputs in;
     double st, h, dxi;
+    double inv_h2, inv_dxi;   // 1 / (2 h), 1 / dxi
     double* out[6];       // Ex Ey Ez Bx By Bz right-hand sides (N x N, may be NULL)
     int N;
 };
 
 __device__ __forceinline__ double avg_in(const double* a, const double* a_prev, size_t k) {
     return a_prev ? (a[k] + a_prev[k]) / 2 : a[k];
+}
+
+// x / d from the reciprocal: q0 = x (1/d) is within an ulp of the quotient and
+// one correction with the exact residual fma(-q0, d, x) rounds it (the
+// float64 divisions of the reference, without the division sequence).
+__device__ __forceinline__ double div_by(double x, double d, double inv_d) {
+    const double q0 = x * inv_d;
+    return fma(fma(-q0, d, x), inv_d, q0);
 }
 
 __global__ void __launch_bounds__(256) rhs_kernel(const __grid_constant__ RhsArgs a) {
@@ -54,17 +63,17 @@ __global__ void __launch_bounds__(256) rhs_kernel(const __grid_constant__ RhsArg
         if (interior) {
             // (ro_in + beam_ro) and (jz_in + beam_ro) at the four neighbours
             const size_t kp = k + N, km = k - N, lp = k + 1, lm = k - 1;
-            dro_dx = ((avg_in(in.ro, in.ro_prev, kp) + in.beam[kp]) -
-                      (avg_in(in.ro, in.ro_prev, km) + in.beam[km])) / h2;
-            dro_dy = ((avg_in(in.ro, in.ro_prev, lp) + in.beam[lp]) -
-                      (avg_in(in.ro, in.ro_prev, lm) + in.beam[lm])) / h2;
-            djz_dx = ((avg_in(in.jz, in.jz_prev, kp) + in.beam[kp]) -
-                      (avg_in(in.jz, in.jz_prev, km) + in.beam[km])) / h2;
-            djz_dy = ((avg_in(in.jz, in.jz_prev, lp) + in.beam[lp]) -
-                      (avg_in(in.jz, in.jz_prev, lm) + in.beam[lm])) / h2;
+            dro_dx = div_by((avg_in(in.ro, in.ro_prev, kp) + in.beam[kp]) -
+                            (avg_in(in.ro, in.ro_prev, km) + in.beam[km]), h2, a.inv_h2);
+            dro_dy = div_by((avg_in(in.ro, in.ro_prev, lp) + in.beam[lp]) -
+                            (avg_in(in.ro, in.ro_prev, lm) + in.beam[lm]), h2, a.inv_h2);
+            djz_dx = div_by((avg_in(in.jz, in.jz_prev, kp) + in.beam[kp]) -
+                            (avg_in(in.jz, in.jz_prev, km) + in.beam[km]), h2, a.inv_h2);
+            djz_dy = div_by((avg_in(in.jz, in.jz_prev, lp) + in.beam[lp]) -
+                            (avg_in(in.jz, in.jz_prev, lm) + in.beam[lm]), h2, a.inv_h2);
         }
-        const double djx_dxi = (in.jx_prev[k] - in.jx[k]) / a.dxi;
-        const double djy_dxi = (in.jy_prev[k] - in.jy[k]) / a.dxi;
+        const double djx_dxi = div_by(in.jx_prev[k] - in.jx[k], a.dxi, a.inv_dxi);
+        const double djy_dxi = div_by(in.jy_prev[k] - in.jy[k], a.dxi, a.inv_dxi);
         const double st = a.st;
         a.out[0][k] = -((dro_dx - djx_dxi) - in.Ex_sub[k] * st);
         a.out[1][k] = -((dro_dy - djy_dxi) - in.Ey_sub[k] * st);
@@ -78,8 +87,8 @@ __global__ void __launch_bounds__(256) rhs_kernel(const __grid_constant__ RhsArg
             const double djy_dy = in.jy[k + 1] - in.jy[k - 1];
             const double djx_dy = in.jx[k + 1] - in.jx[k - 1];
             const double djy_dx = in.jy[k + N] - in.jy[k - N];
-            ez = -(djx_dx + djy_dy) / h2;
-            bz = -(djx_dy - djy_dx) / h2;
+            ez = -div_by(djx_dx + djy_dy, h2, a.inv_h2);
+            bz = -div_by(djx_dy - djy_dx, h2, a.inv_h2);
         }
         if (a.out[2]) a.out[2][k] = ez;
         if (a.out[5]) a.out[5][k] = bz;
@@ -401,6 +410,8 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
     ra.st = c->p.field_solver_subtraction_trick;
     ra.h = c->p.grid_step_size;
     ra.dxi = c->p.xi_step_size;
+    ra.inv_h2 = 1.0 / (ra.h * 2);
+    ra.inv_dxi = 1.0 / ra.dxi;
     ra.N = N;
     for (int f = 0; f < 6; ++f) ra.out[f] = on[f] ? c->rhs[f] : nullptr;
     {
