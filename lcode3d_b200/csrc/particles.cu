@@ -208,8 +208,14 @@ __device__ __forceinline__ double fx_value(long long hi, long long lo) {
            (double)lo * 0x1p-76;
 }
 
-constexpr int DEP_T = 32;                 // fine particles per CTA side
-constexpr int DEP_THREADS = DEP_T * DEP_T; // phase 1: one fine particle per thread
+#ifndef LC3D_DEP_ROWS
+#define LC3D_DEP_ROWS 16
+#endif
+constexpr int DEP_TJ = 32;                // fine particles per CTA along j (one warp)
+constexpr int DEP_TI = LC3D_DEP_ROWS;     // ... along i (16: two CTAs share an SM)
+constexpr int DEP_THREADS = DEP_TI * DEP_TJ; // phase 1: one fine particle per thread
+constexpr int DEP_BLOCKS = DEP_THREADS / 4;  // phase 2: 2 x 2 blocks of the patch
+static_assert(DEP_TI % 2 == 0 && DEP_THREADS % 4 == 0, "the patch is tiled by 2 x 2 blocks");
 constexpr int DEP_W = 32;                 // shared window side (cells)
 constexpr int DEP_WIN = DEP_W * DEP_W;
 // shared memory: float64 window (4 fields), anchor claims, per-particle
@@ -261,9 +267,11 @@ __device__ __forceinline__ void fx_add(unsigned long long* hi_plane, unsigned lo
     atomicAdd(lo_plane + cell, (unsigned long long)lo);
 }
 
-// Deposition of a 32 x 32 patch of the fine lattice by one CTA of 1024
-// threads. Deterministic: every float64 sum below has a fixed order, and the
-// sums that cross CTAs are exact integer (fixed-point) sums.
+// Deposition of a DEP_TI x 32 patch of the fine lattice by one CTA, one
+// thread per fine particle (16 x 32 by default: with 64 registers two CTAs
+// share an SM, so one CTA's phases overlap the other's barriers and load
+// latencies). Deterministic: every float64 sum below has a fixed order, and
+// the sums that cross CTAs are exact integer (fixed-point) sums.
 //  1. One thread per fine particle: coarse->fine interpolation, deposit
 //     values and TSC cell, staged in shared memory; the CTA's bounding box
 //     of cells places a 32 x 32-cell float64 window.
@@ -281,7 +289,7 @@ __device__ __forceinline__ void fx_add(unsigned long long* hi_plane, unsigned lo
 //     to the global accumulators through the exact fixed-point split.
 //  3. Each touched window cell is split once into fixed point and added to
 //     the global accumulators.
-__global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) {
+__global__ void __launch_bounds__(DEP_THREADS, 1024 / DEP_THREADS) deposit_kernel(DepositArgs a) {
     extern __shared__ double smem_f64[];
     double* fwin = smem_f64;                                   // [4][DEP_WIN]
     double* s_xl = fwin + 4 * DEP_WIN;                         // [DEP_THREADS]
@@ -302,7 +310,7 @@ __global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) 
 
     // ---- phase 1: one fine particle per thread ----
     {
-        const int fi = blockIdx.y * DEP_T + (t >> 5), fj = blockIdx.x * DEP_T + (t & 31);
+        const int fi = blockIdx.y * DEP_TI + (t >> 5), fj = blockIdx.x * DEP_TJ + (t & 31);
         int cell = -1, i = 1 << 30, j = 1 << 30;
         if (fi < a.Nf && fj < a.Nf) {
             const FineParticle f = fine_particle(a, fi, fj);
@@ -345,9 +353,9 @@ __global__ void __launch_bounds__(DEP_THREADS, 1) deposit_kernel(DepositArgs a) 
     const int oi = s_bb[0] - 1, oj = s_bb[2] - 1;   // window origin (cells)
 
     // ---- phase 2: one (2 x 2 block, field) per thread ----
-    const int f = t >> 8, blk = t & 255;
-    const int p0 = (blk >> 4) * 2 * DEP_T + (blk & 15) * 2;   // top-left particle of the block
-    const int pidx[4] = {p0, p0 + 1, p0 + DEP_T, p0 + DEP_T + 1};
+    const int f = t / DEP_BLOCKS, blk = t % DEP_BLOCKS;
+    const int p0 = (blk >> 4) * 2 * DEP_TJ + (blk & 15) * 2;   // top-left particle of the block
+    const int pidx[4] = {p0, p0 + 1, p0 + DEP_TJ, p0 + DEP_TJ + 1};
     int ci[4], cj[4];
     bool ok[4];
     int i0 = 1 << 30, i1 = -(1 << 30), j0 = 1 << 30, j1 = -(1 << 30);
@@ -525,7 +533,7 @@ int particles_prepare() {
 
 int launch_deposit_main(const DepositArgs& a, cudaStream_t s) {
     if (a.Nf <= 0) return LC3D_OK;
-    dim3 grid((a.Nf + DEP_T - 1) / DEP_T, (a.Nf + DEP_T - 1) / DEP_T);
+    dim3 grid((a.Nf + DEP_TJ - 1) / DEP_TJ, (a.Nf + DEP_TI - 1) / DEP_TI);
     deposit_kernel<<<grid, DEP_THREADS, DEP_SMEM, s>>>(a);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
