@@ -124,6 +124,19 @@ int lc3d_step_arrays(lc3d_ctx* ctx, const lc3d_state_ptrs* prev,
                      const lc3d_state_ptrs* out, const double* beam_ro,
                      void* stream);
 
+/* lc3d_step_arrays with the beam in HOST memory (N x N float64; NULL: no
+ * beam), as the reference's loop produces it (lcode.py:1040, 839). The copy
+ * to the device runs on a stream of the context while the step's first
+ * push and deposition run, and the first field solve waits for it. At
+ * entry the call waits (on the host) for the previous call's copy to have
+ * read its buffer; the caller must keep beam_host unchanged until the next
+ * call on this context returns or the stream is synchronised. For a pinned
+ * buffer the copy is asynchronous; for pageable memory the CUDA runtime
+ * stages it during the call. */
+int lc3d_step_arrays_host_beam(lc3d_ctx* ctx, const lc3d_state_ptrs* prev,
+                               const lc3d_state_ptrs* out, const double* beam_host,
+                               void* stream);
+
 /* ---- device-side beam and graph-replayed runs ----
  * The reference evaluates config.beam on the host and copies it to the
  * device every step (lcode.py:1040, 839), and copies the whole Ez array back
@@ -207,6 +220,16 @@ int lc3d_calculate_Ez(lc3d_ctx* ctx, const double* jx, const double* jy,
 /* calculate_Bz, lcode.py:333-364. */
 int lc3d_calculate_Bz(lc3d_ctx* ctx, const double* jx, const double* jy,
                       double* Bz, void* stream);
+
+/* ---- diagnostics ---- */
+
+/* The density-noise figure of diags_ro_zn (lcode.py:979-987) for one N x N
+ * array ro: mean |ro - G(ro)| / 4.23045376e-04 with G the Gaussian blur of
+ * scipy.ndimage.gaussian_filter (sigma = 0.25 / grid_step_size, truncated at
+ * 4 sigma, 'reflect' edges), written to *zn (a device double). The running
+ * maximum over calls that the reference keeps is the caller's (a host
+ * variable in lcode3d_b200.lcode.diags_ro_zn). Deterministic. */
+int lc3d_diag_zn(lc3d_ctx* ctx, const double* ro, double* zn, void* stream);
 
 /* ---- launch accounting and kernel timing ---- */
 

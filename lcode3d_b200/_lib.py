@@ -67,6 +67,7 @@ SIGNATURES = [
     ('lc3d_get_state', c_int, [P, ctypes.POINTER(StatePtrs), P]),
     ('lc3d_step', c_int, [P, P, P]),
     ('lc3d_step_arrays', c_int, [P, ctypes.POINTER(StatePtrs), ctypes.POINTER(StatePtrs), P, P]),
+    ('lc3d_step_arrays_host_beam', c_int, [P, ctypes.POINTER(StatePtrs), ctypes.POINTER(StatePtrs), P, P]),
     ('lc3d_move_estimate_wo_fields', c_int, [P] * 12),
     ('lc3d_move_smart', c_int, [P] * 24),
     ('lc3d_deposit', c_int, [P] * 14),
@@ -83,6 +84,7 @@ SIGNATURES = [
     ('lc3d_batch_run', c_int, [P, P, c_int, P, P]),
     ('lc3d_batch_destroy', c_int, [P]),
     ('lc3d_beam_eval', c_int, [P, c_int, P, P]),
+    ('lc3d_diag_zn', c_int, [P, P, P, P]),
     ('lc3d_step_arrays_first_pass', c_int, [P, ctypes.POINTER(StatePtrs), ctypes.POINTER(StatePtrs), P, P, P]),
     ('lc3d_step_arrays_predicted', c_int, [P, ctypes.POINTER(StatePtrs), ctypes.POINTER(StatePtrs), P, P, P, P]),
     ('lc3d_fields_rel_diff', c_int, [P, P, P, P, P]),

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'liblc3d.so')
 
-SOURCES = ['particles.cu', 'fields.cu', 'fields_fft.cu', 'fields_mixed.cu', 'run.cu', 'predictor.cu', 'lc3d_api.cu']
+SOURCES = ['particles.cu', 'fields.cu', 'fields_fft.cu', 'fields_mixed.cu', 'run.cu', 'predictor.cu', 'diagnostics.cu', 'lc3d_api.cu']
 
 NVCC_FLAGS = [
     '-gencode', 'arch=compute_100a,code=sm_100a',

@@ -162,6 +162,7 @@ struct StepExtras {
     double* const* first;                 // 6 fields, or NULL
     const double* const* pred;            // 6 fields, or NULL
     double* residual;                     // device double, or NULL
+    const double* beam_host;              // host beam to copy during the first pass, or NULL
 };
 
 struct AvgArgs {
@@ -251,6 +252,16 @@ int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& ou
             ProfScope ps(c, LC3D_STAGE_MOVE, s);
             LC3D_TRY(launch_move_smart(mv, s));
         }
+        if (pass == 0 && x && x->beam_host) {
+            // the host beam crosses on the copy stream while the first
+            // deposition runs; the first field solve waits for it
+            LC3D_CUDA_TRY(cudaEventRecord(c->ev_main, s));
+            LC3D_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, c->ev_main, 0));
+            LC3D_CUDA_TRY(cudaMemcpyAsync(c->beam_dev, x->beam_host, (size_t)c->N * c->N * sizeof(double),
+                                          cudaMemcpyHostToDevice, c->copy_stream));
+            LC3D_CUDA_TRY(cudaEventRecord(c->ev_copy, c->copy_stream));
+            in.beam = c->beam_dev;
+        }
         if (pass == 0 && predicted) {
             // the prediction stands in for the first-pass fields: only the
             // particle positions of this pass are used (as the estimate)
@@ -276,6 +287,7 @@ int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& ou
             so.out[0] = out.Ex; so.out[1] = out.Ey; so.out[2] = out.Ez;
             so.out[3] = out.Bx; so.out[4] = out.By; so.out[5] = out.Bz;
         }
+        if (x && x->beam_host) LC3D_CUDA_TRY(cudaStreamWaitEvent(s, c->ev_copy, 0));
         LC3D_TRY(solve_fields(c, LC3D_F_ALL, in, so, s));
     }
     if (predicted && x->residual) {
@@ -328,6 +340,11 @@ void destroy(lc3d_ctx* c) {
     if (c->err) cudaFree(c->err);
     if (c->zeros) cudaFree(c->zeros);
     if (c->resid) cudaFree(c->resid);
+    if (c->beam_dev) cudaFree(c->beam_dev);
+    if (c->ev_main) cudaEventDestroy(c->ev_main);
+    if (c->ev_copy) cudaEventDestroy(c->ev_copy);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    diag_free(c);
     if (c->fft_tw) cudaFree(c->fft_tw);
     mixed_free(c);
     run_free(c);
@@ -416,10 +433,15 @@ int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out) {
     LC3D_STEP(dalloc(&c->err, (size_t)1));
     LC3D_STEP(dalloc(&c->zeros, ng));
     LC3D_STEP(dalloc(&c->resid, (size_t)2));
+    LC3D_STEP(dalloc(&c->beam_dev, ng));
+    if (rc == LC3D_OK && cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = LC3D_ERR_CUDA;
+    if (rc == LC3D_OK && cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming) != cudaSuccess) rc = LC3D_ERR_CUDA;
+    if (rc == LC3D_OK && cudaEventCreateWithFlags(&c->ev_copy, cudaEventDisableTiming) != cudaSuccess) rc = LC3D_ERR_CUDA;
     LC3D_STEP(particles_prepare());
     LC3D_STEP(fields_init(c));
     LC3D_STEP(fft_init(c));
     LC3D_STEP(run_init(c));
+    LC3D_STEP(diag_init(c));
     if (rc == LC3D_OK) {
         if (p->fp64_transform == LC3D_FP64_FFT && !c->fft_ok) rc = LC3D_ERR_PARAM;
         c->use_fft = c->fft_ok && p->fp64_transform != LC3D_FP64_DENSE;
@@ -508,6 +530,18 @@ int lc3d_step_arrays(lc3d_ctx* c, const lc3d_state_ptrs* prev, const lc3d_state_
     return run_step(c, *prev, *out, beam_ro ? beam_ro : c->zeros, S(stream));
 }
 
+int lc3d_step_arrays_host_beam(lc3d_ctx* c, const lc3d_state_ptrs* prev, const lc3d_state_ptrs* out,
+                               const double* beam_host, void* stream) {
+    if (!c || !state_complete(prev) || !state_complete(out)) return LC3D_ERR_PARAM;
+    if (c->const_set != 3) return LC3D_ERR_STATE;
+    DeviceGuard g(c->device);
+    if (!beam_host) return run_step(c, *prev, *out, c->zeros, S(stream));
+    // the previous call's copy has finished reading its host buffer
+    LC3D_CUDA_TRY(cudaEventSynchronize(c->ev_copy));
+    StepExtras x{nullptr, nullptr, nullptr, beam_host};
+    return run_step(c, *prev, *out, c->zeros, S(stream), &x);
+}
+
 int lc3d_step_arrays_first_pass(lc3d_ctx* c, const lc3d_state_ptrs* prev, const lc3d_state_ptrs* out,
                                 const double* beam_ro, double* const* first, void* stream) {
     if (!c || !state_complete(prev) || !state_complete(out) || !first) return LC3D_ERR_PARAM;
@@ -515,7 +549,7 @@ int lc3d_step_arrays_first_pass(lc3d_ctx* c, const lc3d_state_ptrs* prev, const 
         if (!first[f]) return LC3D_ERR_PARAM;
     if (c->const_set != 3) return LC3D_ERR_STATE;
     DeviceGuard g(c->device);
-    StepExtras x{first, nullptr, nullptr};
+    StepExtras x{first, nullptr, nullptr, nullptr};
     return run_step(c, *prev, *out, beam_ro ? beam_ro : c->zeros, S(stream), &x);
 }
 
@@ -526,7 +560,7 @@ int lc3d_step_arrays_predicted(lc3d_ctx* c, const lc3d_state_ptrs* prev, const l
         if (!pred[f]) return LC3D_ERR_PARAM;
     if (c->const_set != 3) return LC3D_ERR_STATE;
     DeviceGuard g(c->device);
-    StepExtras x{nullptr, pred, residual};
+    StepExtras x{nullptr, pred, residual, nullptr};
     return run_step(c, *prev, *out, beam_ro ? beam_ro : c->zeros, S(stream), &x);
 }
 

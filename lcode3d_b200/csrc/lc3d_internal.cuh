@@ -161,6 +161,8 @@ int mixed_stage(lc3d_ctx* ctx, const MixedStageDesc* d, int count, cudaStream_t 
 int particles_prepare();
 int fft_prepare(int P);
 int fields_init(lc3d_ctx* ctx);           // transform matrices, workspaces
+int diag_init(lc3d_ctx* ctx);             // diagnostics.cu
+void diag_free(lc3d_ctx* ctx);
 void fields_free(lc3d_ctx* ctx);
 
 // ---------------------------------------------------------------------------
@@ -189,6 +191,12 @@ struct lc3d_ctx {
     unsigned* err;                        // device error flag
     double* zeros;                        // N x N zeros (absent beam)
     unsigned long long* resid;            // predicted-step residual maxima (2 words, double bits)
+    double* diag_w;                       // zn diagnostic: Gaussian weights, then partial sums
+    double* diag_buf;                     // zn diagnostic: two N x N blur planes
+    int diag_r;                           // Gaussian radius
+    double* beam_dev;                     // device copy of a host beam (lc3d_step_arrays_host_beam)
+    cudaStream_t copy_stream;             // its host-to-device copies
+    cudaEvent_t ev_main, ev_copy;         // ordering of those copies with the step's stream
     // field-solver workspaces (fields.cu)
     double *S2, *C, *CT;                  // 2*DST-I (M x M), DCT-I (N x N), its transpose
     double *lam_dir, *lam_mix, *lam_mixT, *lam_neu;

@@ -389,21 +389,47 @@ def _beam(config, beam_ro):
     return _f64(beam_ro, _grid(config))
 
 
+def _host_beam(config, beam_ro):
+    """The beam as a contiguous float64 host array of N x N (None for a
+    device array or the scalar 0)."""
+    if isinstance(beam_ro, (int, float)) and beam_ro == 0:
+        return None
+    if isinstance(beam_ro, torch.Tensor):
+        if beam_ro.is_cuda:
+            return None
+        t = beam_ro.to(torch.float64)
+    else:
+        t = torch.from_numpy(np.asarray(beam_ro, dtype=np.float64))
+    g = _grid(config)
+    if tuple(t.shape) != g:
+        t = t.expand(g)
+    return t.contiguous()
+
+
 def step(config, const, virt_params, prev, beam_ro):
     """One xi step: estimate, predictor, corrector, final move and deposit
-    (lcode.py:828-931). Returns a new GPUArrays; ``prev`` is not modified."""
+    (lcode.py:828-931). Returns a new GPUArrays; ``prev`` is not modified.
+    A beam given in host memory (the reference's loop evaluates it with
+    numpy) is copied to the device during the step's first deposition
+    (lc3d_step_arrays_host_beam)."""
     s = solver_for(config)
     s.set_virt(virt_params)
     s.set_const(const)
-    beam = _beam(config, beam_ro)
+    hb = _host_beam(config, beam_ro)
+    beam = None if hb is not None else _beam(config, beam_ro)
     shape_p = tuple(prev.x_offt.shape)
     g = _grid(config)
     prev_t = [_f64(getattr(prev, n), shape_p if k < 5 else g) for k, n in enumerate(_lib.STATE_NAMES)]
     out = {n: _empty(shape_p if k < 5 else g) for k, n in enumerate(_lib.STATE_NAMES)}
     sp = _lib.StatePtrs(*[t.data_ptr() for t in prev_t])
     so = _lib.StatePtrs(*[out[n].data_ptr() for n in _lib.STATE_NAMES])
-    check(lib.lc3d_step_arrays(s.ctx, ctypes.byref(sp), ctypes.byref(so), _ptr(beam), _stream()),
-          'step')
+    if hb is not None:
+        check(lib.lc3d_step_arrays_host_beam(s.ctx, ctypes.byref(sp), ctypes.byref(so),
+                                             ctypes.c_void_p(hb.data_ptr()), _stream()), 'step')
+        s._host_beam_keep = hb   # read by the copy until the next call on this context
+    else:
+        check(lib.lc3d_step_arrays(s.ctx, ctypes.byref(sp), ctypes.byref(so), _ptr(beam), _stream()),
+              'step')
     s.check_device_flag('step')
     new = GPUArrays.__new__(GPUArrays)
     for n in _lib.STATE_NAMES:
@@ -493,9 +519,27 @@ def init(config):
 
 
 # ---------------------------------------------------------------------------
-# CLI loop (lcode.py:1032-1051) with the on-axis Ez report of
-# lcode.py:992-1002, 1016-1026 (PNG slices and the zn figure are omitted)
+# CLI loop (lcode.py:1032-1051) with the diagnostics line of
+# lcode.py:979-1026: on-axis Ez, its peak drift and the zn noise figure (the
+# PNG slices of lcode.py:1005-1013 are omitted: no plotting stack)
 # ---------------------------------------------------------------------------
+
+max_zn = 0.0
+
+
+def diags_ro_zn(config, ro):
+    """The running maximum of the density-noise figure (lcode.py:979-987):
+    mean |ro - gaussian_filter(ro, sigma = 0.25 / h)| / 4.23045376e-04,
+    computed on the device (lc3d_diag_zn); one scalar is read back."""
+    global max_zn
+    s = solver_for(config)
+    g = _grid(config)
+    r = _f64(ro, g)
+    out = _empty((1,))
+    check(lib.lc3d_diag_zn(s.ctx, _ptr(r), _ptr(out), _stream()), 'lc3d_diag_zn')
+    max_zn = max(max_zn, float(out.item()))
+    return max_zn
+
 
 def diags_peak_msg(Ez_00_history):
     """Last on-axis Ez peak and its drift from the first peak
@@ -525,7 +569,8 @@ def main():
             Ez_00_history.append(ez)
             if xi_i % config.diagnostics_each_N_steps == 0 or xi_i == config.xi_steps - 1:
                 xi = -xi_i * config.xi_step_size
-                print(f'xi={xi:+.4f} {ez:+.4e}|{diags_peak_msg(Ez_00_history)}')
+                zn = diags_ro_zn(config, state.ro)
+                print(f'xi={xi:+.4f} {ez:+.4e}|{diags_peak_msg(Ez_00_history)}|zn={zn:.3f}')
                 sys.stdout.flush()
 
 

@@ -97,3 +97,45 @@ def test_autotuner_picks_a_form(L):
     choice, timings = B.autotune_transform([161], steps=3)
     assert choice[161] in ('fft', 'dense')
     assert set(timings[161]) == {'fft', 'dense'} and all(v > 0 for v in timings[161].values())
+
+
+def test_diag_zn_matches_scipy(L):
+    """lc3d_diag_zn against the reference's own zn expression (scipy.ndimage
+    gaussian_filter, oracle restatement) on a state from a real run and on
+    a noisy field; the running maximum is kept like the reference's."""
+    cfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    xs, ys, const, virt, st = L.init(cfg)
+    for i in range(40):
+        st = L.step(cfg, const, virt, st, beam_array(cfg, i, xs, ys))
+    ro = st.ro.cpu().numpy()
+    rng = np.random.default_rng(3)
+    noisy = ro + 1e-3 * rng.normal(size=ro.shape)
+    L.lcode.max_zn = 0.0
+    a = L.lcode.diags_ro_zn(cfg, st.ro)
+    assert a == pytest.approx(O.diags_ro_zn_value(cfg, ro), rel=1e-12)
+    b = L.lcode.diags_ro_zn(cfg, torch.from_numpy(noisy).cuda())
+    assert b == pytest.approx(max(a, O.diags_ro_zn_value(cfg, noisy)), rel=1e-12)
+    assert L.lcode.diags_ro_zn(cfg, st.ro) == b       # running maximum
+    # a 641 grid (sigma = 10 cells, 81 taps)
+    cfg6 = make_config(641, 0.025, 0.005, 10, amplitude=0.5)
+    L.lcode.max_zn = 0.0
+    z = rng.normal(size=(641, 641))
+    assert L.lcode.diags_ro_zn(cfg6, torch.from_numpy(z).cuda()) == pytest.approx(
+        O.diags_ro_zn_value(cfg6, z), rel=1e-12)
+
+
+def test_host_beam_step_is_device_beam_step(L):
+    """lcode.step with the beam in host memory (copied during the first
+    deposition, lc3d_step_arrays_host_beam) gives the same bits as with the
+    beam already on the device, for pageable and pinned host arrays."""
+    cfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    xs, ys, const, virt, st = L.init(cfg)
+    a = b = c = st
+    for i in range(12):
+        beam = beam_array(cfg, i, xs, ys)
+        a = L.step(cfg, const, virt, a, beam)                                   # numpy, pageable
+        b = L.step(cfg, const, virt, b, torch.from_numpy(beam).cuda())          # device
+        c = L.step(cfg, const, virt, c, torch.from_numpy(beam).pin_memory())    # pinned
+    for k in STATE:
+        assert torch.equal(getattr(a, k), getattr(b, k)), k
+        assert torch.equal(getattr(c, k), getattr(b, k)), k
