@@ -11,7 +11,9 @@
 // and DCT-I = C x of the dense-transform form). The FFT is an
 // in-place decimation-in-frequency FFT with mixed radices 8, 4, 2, 3, 5 in
 // shared memory (P = 1280: 8, 8, 4, 5), read out in digit-reversed order
-// through a position-sorted list. Every launch transforms rows, optionally
+// through a position-sorted list. The kernel is persistent: a CTA loops over
+// groups of rows and copies the next group's rows into a staging area with
+// cp.async while the current group's passes run. Every launch transforms rows, optionally
 // scaled on input by Lambda[r][j], and writes its output TRANSPOSED
 // (out[k][r]); the 2-D solve F = L (Lambda o (L X R)) R is then four such
 // passes:
@@ -66,6 +68,8 @@ struct FftBatch {
     int count, P, N;
     int nrad;
     int rad[MAX_RADICES];
+    int ngroups;                         // row groups (ROWS_PER_CTA rows) over all fields
+    int stage_lam;                       // the staging area also holds Lambda rows
     const double2* tw;                   // tw[m] = exp(-2 pi i m / P)
     const int* rd;                       // readout lists: DCT-I (N entries), then DST-I (N - 2)
 };
@@ -215,59 +219,94 @@ __device__ __forceinline__ void fft_pass(double2* A, int span, int P, const doub
     }
 }
 
-__global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_kernel(const __grid_constant__ FftBatch b) {
-    extern __shared__ double2 sm[];      // FFT q at sm + q (P + FFT_PAD), transformed in place
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+__device__ __forceinline__ int field_of(const FftBatch& b, int g) {
     int fi = 0;
 #pragma unroll 1
     for (int q = 1; q < b.count; ++q)
-        if ((int)blockIdx.x >= b.f[q].cta_start) fi = q;
-    const FftField& F = b.f[fi];
-    const int P = b.P, L = P / 2, PS = P + FFT_PAD;
-    const int r0 = ((int)blockIdx.x - F.cta_start) * ROWS_PER_CTA;
-    const int n = F.type ? b.N - 2 : b.N;     // input / output length
-    double2* A = sm;
+        if (g >= b.f[q].cta_start) fi = q;
+    return fi;
+}
 
-    // symmetric / antisymmetric extensions, rows 2q and 2q + 1 of the CTA
-    // as the real and imaginary parts of FFT q, each input element (scaled
-    // by Lambda[row][j] when given) loaded once and written to its one or
-    // two positions. All loads of a batch are issued before the first use.
-    constexpr int LU = 2;
-    for (int j0 = 0; j0 < n; j0 += LU * FFT_THREADS) {
-        double x[ROWS_PER_CTA][LU];
+// Start copying row group g (ROWS_PER_CTA rows, and their Lambda rows) into
+// the staging area, one 8-byte cp.async per element (rows need not be
+// 16-byte aligned); rows past the field are not copied (the reader uses 0).
+__device__ __forceinline__ void stage_group(const FftBatch& b, int g, double* stg, double* stgL) {
+    const FftField& F = b.f[field_of(b, g)];
+    const int n = F.type ? b.N - 2 : b.N;
+    const int r0 = (g - F.cta_start) * ROWS_PER_CTA;
 #pragma unroll
-        for (int rr = 0; rr < ROWS_PER_CTA; ++rr) {
-            const int row = r0 + rr;
-            const double* rp = F.in + (size_t)row * F.ld_in;
-            const double* lp = F.lam ? F.lam + (size_t)row * F.ld_lam : nullptr;
-#pragma unroll
-            for (int u = 0; u < LU; ++u) {
-                const int j = j0 + u * FFT_THREADS + (int)threadIdx.x;
-                const bool ok = row < F.rows && j < n;
-                x[rr][u] = ok ? __ldg(rp + j) : 0.0;
-                if (F.lam) x[rr][u] *= ok ? __ldg(lp + j) : 0.0;
-            }
+    for (int rr = 0; rr < ROWS_PER_CTA; ++rr) {
+        const int row = r0 + rr;
+        if (row >= F.rows) continue;
+        const double* rp = F.in + (size_t)row * F.ld_in;
+        const double* lp = F.lam ? F.lam + (size_t)row * F.ld_lam : nullptr;
+        for (int j = threadIdx.x; j < n; j += FFT_THREADS) {
+            cp_async8(stg + rr * b.N + j, rp + j);
+            if (lp) cp_async8(stgL + rr * b.N + j, lp + j);
         }
+    }
+    cp_async_commit();
+}
+
+// Persistent: CTA i transforms row groups i, i + gridDim.x, ...; the rows
+// of the next group are copied into the staging area (cp.async) while the
+// current group's FFT passes run, so the global-load latency of a group is
+// hidden behind the previous group's work.
+__global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_kernel(const __grid_constant__ FftBatch b) {
+    extern __shared__ double2 sm[];      // FFT q at sm + q (P + FFT_PAD); then the staging rows
+    const int P = b.P, L = P / 2, PS = P + FFT_PAD;
+    double2* A = sm;
+    double* stg = reinterpret_cast<double*>(sm + FFT_PER_CTA * PS);   // [ROWS_PER_CTA][N]
+    double* stgL = stg + ROWS_PER_CTA * b.N;                          // [ROWS_PER_CTA][N] if stage_lam
+    int g = blockIdx.x;
+    if (g < b.ngroups) stage_group(b, g, stg, stgL);
+#pragma unroll 1
+    for (; g < b.ngroups; g += gridDim.x) {
+    const FftField& F = b.f[field_of(b, g)];
+    const int r0 = (g - F.cta_start) * ROWS_PER_CTA;
+    const int n = F.type ? b.N - 2 : b.N;     // input / output length
+    cp_async_wait_all();
+    __syncthreads();                     // the staging area holds group g
+
+    // symmetric / antisymmetric extensions, rows 2q and 2q + 1 of the group
+    // as the real and imaginary parts of FFT q, each staged element (scaled
+    // by Lambda[row][j] when given) written to its one or two positions
 #pragma unroll
-        for (int q = 0; q < FFT_PER_CTA; ++q) {
-            double2* a = A + q * PS;
-#pragma unroll
-            for (int u = 0; u < LU; ++u) {
-                const int j = j0 + u * FFT_THREADS + (int)threadIdx.x;
-                if (j >= n) continue;
-                const double2 z = make_double2(x[2 * q][u], x[2 * q + 1][u]);
-                if (F.type == 0) {           // m = j and P - j
-                    a[j] = z;
-                    if (j > 0 && j < L) a[P - j] = z;
-                } else {                     // m = j + 1 and P - j - 1, negated
-                    a[j + 1] = z;
-                    a[P - j - 1] = make_double2(-z.x, -z.y);
-                }
+    for (int q = 0; q < FFT_PER_CTA; ++q) {
+        double2* a = A + q * PS;
+        const bool ok0 = r0 + 2 * q < F.rows, ok1 = r0 + 2 * q + 1 < F.rows;
+        const double* s0 = stg + (2 * q) * b.N;
+        const double* s1 = s0 + b.N;
+        const double* l0 = stgL + (2 * q) * b.N;
+        const double* l1 = l0 + b.N;
+        for (int j = threadIdx.x; j < n; j += FFT_THREADS) {
+            double x0 = ok0 ? s0[j] : 0.0, x1 = ok1 ? s1[j] : 0.0;
+            if (F.lam) {
+                x0 *= ok0 ? l0[j] : 0.0;
+                x1 *= ok1 ? l1[j] : 0.0;
+            }
+            const double2 z = make_double2(x0, x1);
+            if (F.type == 0) {           // m = j and P - j
+                a[j] = z;
+                if (j > 0 && j < L) a[P - j] = z;
+            } else {                     // m = j + 1 and P - j - 1, negated
+                a[j + 1] = z;
+                a[P - j - 1] = make_double2(-z.x, -z.y);
             }
         }
     }
     if (F.type == 1 && threadIdx.x < 2 * FFT_PER_CTA)   // DST-I: zeros at m = 0 and m = L
         A[(threadIdx.x >> 1) * PS + (threadIdx.x & 1) * L] = make_double2(0.0, 0.0);
-    __syncthreads();
+    __syncthreads();                     // the staging area is free: start the next group
+    if (g + (int)gridDim.x < b.ngroups) stage_group(b, g + gridDim.x, stg, stgL);
     int span = P;
     for (int p = 0; p < b.nrad; ++p) {
         const int R = b.rad[p];
@@ -323,8 +362,11 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
             if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
             __syncthreads();
         }
-        if (threadIdx.x == 0) F.partial[blockIdx.x - F.cta_start] = red[0];
+        if (threadIdx.x == 0) F.partial[g - F.cta_start] = red[0];
     }
+    __syncthreads();                     // the FFT buffer is free for the next group
+    }
+    cp_async_wait_all();                 // nothing left in flight (no group was started past the end)
 }
 
 double sin_pi_frac(long long r, long long L) {
@@ -353,12 +395,18 @@ int fft_plan(int P, int* rad) {
 
 int fft_cta_rows() { return ROWS_PER_CTA; }
 
-size_t fft_smem_bytes(int P) { return ((size_t)FFT_PER_CTA * P + (FFT_PER_CTA - 1) * FFT_PAD) * sizeof(double2); }
+// Dynamic shared memory of fft_rows_kernel, the layout the kernel uses: the
+// FFT buffers at a pitch of P + FFT_PAD double2 words, then the staging rows
+// (ROWS_PER_CTA x N doubles, twice when Lambda rows are staged too).
+size_t fft_cta_smem_bytes(int P, int N, int stage_lam) {
+    return (size_t)FFT_PER_CTA * (P + FFT_PAD) * sizeof(double2) +
+           (size_t)ROWS_PER_CTA * N * sizeof(double) * (1 + stage_lam);
+}
 
 int fft_init(lc3d_ctx* c) {
     const int N = c->N, P = 2 * (N - 1);
     int rad[MAX_RADICES];
-    c->fft_ok = fft_plan(P, rad) > 0 && fft_smem_bytes(P) <= 200 * 1024;
+    c->fft_ok = fft_plan(P, rad) > 0 && fft_cta_smem_bytes(P, N, 1) <= 200 * 1024;
     if (!c->fft_ok) return LC3D_OK;
     LC3D_TRY(fft_prepare(P));
     const int nrad = fft_plan(P, rad);
@@ -425,11 +473,19 @@ int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, cudaStream_t s) {
         f.partial = desc[q].partial;
         f.cta_start = ctas;
         ctas += (f.rows + ROWS_PER_CTA - 1) / ROWS_PER_CTA;
+        if (f.lam) b.stage_lam = 1;
     }
     if (!ctas) return LC3D_OK;
-    const size_t smem = fft_smem_bytes(b.P);
+    b.ngroups = ctas;
+    const size_t smem = fft_cta_smem_bytes(b.P, b.N, b.stage_lam);
+    // persistent grid: as many CTAs as fit on the device at once
+    int dev = 0, sms = 0, per_sm = 0;
+    LC3D_CUDA_TRY(cudaGetDevice(&dev));
+    LC3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    LC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_rows_kernel, FFT_THREADS, smem));
+    const int grid = std::max(1, std::min(ctas, sms * std::max(per_sm, 1)));
     ProfScope ps(c, LC3D_STAGE_TRANSFORM, s);
-    fft_rows_kernel<<<ctas, FFT_THREADS, smem, s>>>(b);
+    fft_rows_kernel<<<grid, FFT_THREADS, smem, s>>>(b);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
