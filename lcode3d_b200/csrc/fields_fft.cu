@@ -42,7 +42,7 @@ constexpr int FFT_THREADS = LC3D_FFT_THREADS;
 constexpr int FFT_PER_CTA = LC3D_FFT_PER_CTA;   // complex FFTs per CTA (1 or 2; two rows each)
 constexpr int ROWS_PER_CTA = 2 * FFT_PER_CTA;
 static_assert(FFT_PER_CTA == 1 || FFT_PER_CTA == 2, "one or two FFTs per CTA");
-static_assert((FFT_THREADS & (FFT_THREADS - 1)) == 0, "the partial-sum tree assumes a power-of-two CTA");
+static_assert(FFT_THREADS % 32 == 0 && FFT_THREADS <= 1024, "whole warps");
 #ifndef LC3D_FFT_MAX_RADIX
 #define LC3D_FFT_MAX_RADIX 8              // largest power-of-two butterfly in a plan (8 or 4)
 #endif
@@ -356,13 +356,16 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
     if (F.partial) {   // uniform per CTA: fixed-order sum of everything this CTA wrote
         __syncthreads();   // the FFT buffer is free
         double* red = reinterpret_cast<double*>(sm);
-        red[threadIdx.x] = psum;
+        double v = psum;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
         __syncthreads();
-        for (int h = FFT_THREADS / 2; h > 0; h >>= 1) {
-            if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
-            __syncthreads();
+        if (threadIdx.x == 0) {   // the warps' sums in warp order
+            double t = 0.0;
+            for (int w = 0; w < FFT_THREADS / 32; ++w) t += red[w];
+            F.partial[g - F.cta_start] = t;
         }
-        if (threadIdx.x == 0) F.partial[g - F.cta_start] = red[0];
     }
     __syncthreads();                     // the FFT buffer is free for the next group
     }
