@@ -432,7 +432,11 @@ def run_scan(args, rank, world, dist):
     mine = B.partition(specs, world)[rank]
     grids = sorted({specs[i]['grid_steps'] for i in mine})
     choice, timings = B.autotune_transform(grids, steps=4)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter()
     bt = B.Batch([specs[i] for i in mine], transform=choice)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t_setup
     K, W = args.steps, args.warmup
     bt.run(W)
     from lcode3d_b200 import _lib
@@ -476,6 +480,7 @@ def run_scan(args, rank, world, dist):
                      'ms_per_step': {str(k): v for k, v in timings.items()}},
         'gpu_launches': launches,
         'launches_per_batch_step': launches / K,
+        'setup_s': t_setup,
         'all_final_Ez00_finite': bool(all(np.isfinite(v).all() for v in last.values())),
         'clocks': clk,
     }

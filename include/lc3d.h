@@ -109,6 +109,18 @@ const char* lc3d_strerror(int code);
 int lc3d_set_const(lc3d_ctx* ctx, const lc3d_const_ptrs* c,
                    const lc3d_virt_ptrs* v, void* stream);
 
+/* init() on the device (lcode.py:936-975 with make_plasma, lcode.py:490-573,
+ * and initial_deposition, lcode.py:692-699): builds the context's const and
+ * virt_params and its state at xi = 0 (zero offsets, momenta and fields)
+ * from the parameters alone, bit-identical to the host layout of init().
+ * lc3d_get_const copies the context's const and virt_params out (device
+ * arrays, any may be NULL); the state comes out with lc3d_get_state. */
+int lc3d_init_plasma(lc3d_ctx* ctx, void* stream);
+int lc3d_get_const(lc3d_ctx* ctx, double* m, double* q, double* x_init, double* y_init,
+                   double* ro_initial, double* influence_prev, double* influence_next,
+                   int32_t* indices_prev, int32_t* indices_next, double* fine_grid,
+                   void* stream);
+
 /* Context-owned state (double-buffered): copy in / copy out. */
 int lc3d_set_state(lc3d_ctx* ctx, const lc3d_state_ptrs* s, void* stream);
 int lc3d_get_state(lc3d_ctx* ctx, lc3d_state_ptrs* s, void* stream);

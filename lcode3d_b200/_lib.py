@@ -85,6 +85,8 @@ SIGNATURES = [
     ('lc3d_batch_destroy', c_int, [P]),
     ('lc3d_beam_eval', c_int, [P, c_int, P, P]),
     ('lc3d_diag_zn', c_int, [P, P, P, P]),
+    ('lc3d_init_plasma', c_int, [P, P]),
+    ('lc3d_get_const', c_int, [P] * 12),
     ('lc3d_step_arrays_first_pass', c_int, [P, ctypes.POINTER(StatePtrs), ctypes.POINTER(StatePtrs), P, P, P]),
     ('lc3d_step_arrays_predicted', c_int, [P, ctypes.POINTER(StatePtrs), ctypes.POINTER(StatePtrs), P, P, P, P]),
     ('lc3d_fields_rel_diff', c_int, [P, P, P, P, P]),

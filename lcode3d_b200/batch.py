@@ -81,20 +81,15 @@ def make_config(spec, precision='fp64', transform='auto', slices=0):
 
 class Sim:
     """One scan member: its own context (not shared through the per-config
-    cache of ``lcode``), constants and state."""
+    cache of ``lcode``) with its plasma, ion background and initial state
+    built on the device (lc3d_init_plasma)."""
 
     def __init__(self, spec, precision='fp64', transform='auto', slices=0):
         self.spec = spec
         self.config = make_config(spec, precision, transform, slices)
-        self.xs, self.ys, self.const, self.virt, state = L.init(self.config)
+        L.init_config_checks(self.config)
         self.solver = L.Solver(L.params_of(self.config), L._device().index)
-        self.solver.set_virt(self.virt)
-        self.solver.set_const(self.const)
-        shape_p = tuple(state.x_offt.shape)
-        g = (spec['grid_steps'],) * 2
-        src = [L._f64(getattr(state, n), shape_p if k < 5 else g) for k, n in enumerate(_lib.STATE_NAMES)]
-        check(lib.lc3d_set_state(self.solver.ctx, ctypes.byref(_lib.StatePtrs(*[t.data_ptr() for t in src])),
-                                 L._stream()), 'lc3d_set_state')
+        check(lib.lc3d_init_plasma(self.solver.ctx, L._stream()), 'lc3d_init_plasma')
         bp = _lib.BeamParams(spec['amplitude'], spec['sigma_r'], spec['length_factor'])
         check(lib.lc3d_set_beam(self.solver.ctx, ctypes.byref(bp)), 'lc3d_set_beam')
         self.xi = 0
@@ -102,7 +97,7 @@ class Sim:
     def state(self):
         """The current state as device arrays (a copy)."""
         N = self.spec['grid_steps']
-        shape_p = tuple(self.const.m.shape)
+        shape_p = (self.solver.Nc, self.solver.Nc)
         out = {n: L._empty(shape_p if k < 5 else (N, N)) for k, n in enumerate(_lib.STATE_NAMES)}
         check(lib.lc3d_get_state(self.solver.ctx,
                                  ctypes.byref(_lib.StatePtrs(*[out[n].data_ptr() for n in _lib.STATE_NAMES])),

@@ -359,6 +359,72 @@ void destroy(lc3d_ctx* c) {
 
 inline cudaStream_t S(void* p) { return reinterpret_cast<cudaStream_t>(p); }
 
+// ---------------------------------------------------------------------------
+// Plasma layout on the device (lcode.py:454-573, make_coarse_plasma_grid,
+// make_fine_plasma_grid, make_plasma): the same float64 expressions as the
+// host layout, element by element, so the arrays are bit-identical.
+// ---------------------------------------------------------------------------
+struct PlasmaArgs {
+    double *m, *q, *x_init, *y_init;      // Nc x Nc
+    double *inf_prev, *inf_next, *fine;   // Nf
+    int32_t *idx_prev, *idx_next;         // Nf
+    int Nc, Nf, R, Rf, f;                 // R = Nc half-width + 1, Rf fine half count
+    double hc, d, m0, q0;                 // h * coarseness, h / fineness, particle mass and charge
+};
+
+// coarse lattice: -(R-1) .. R-1 times h c, the negative half as negated
+// products. __dmul_rn: a rounded product that the compiler may not contract
+// into an FMA with the subtraction that uses it (numpy rounds it first).
+__device__ __forceinline__ double coarse_at(const PlasmaArgs& a, int i) {
+    const int j = i - (a.R - 1);
+    return j < 0 ? -__dmul_rn((double)(-j), a.hc) : __dmul_rn((double)j, a.hc);
+}
+
+__device__ __forceinline__ double fine_at(const PlasmaArgs& a, int i) {
+    if (a.f % 2) {
+        const int j = i - (a.Rf - 1);
+        return j < 0 ? -__dmul_rn((double)(-j), a.d) : __dmul_rn((double)j, a.d);
+    }
+    return i < a.Rf ? -__dmul_rn(.5 + (double)(a.Rf - 1 - i), a.d) : __dmul_rn(.5 + (double)(i - a.Rf), a.d);
+}
+
+__global__ void plasma_coarse_kernel(const __grid_constant__ PlasmaArgs a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.Nc * a.Nc) return;
+    const int i = k / a.Nc, j = k - i * a.Nc;
+    a.x_init[k] = coarse_at(a, i);
+    a.y_init[k] = coarse_at(a, j);
+    a.m[k] = a.m0;
+    a.q[k] = a.q0;
+}
+
+__global__ void plasma_fine_kernel(const __grid_constant__ PlasmaArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.Nf) return;
+    const double x = fine_at(a, i);
+    // searchsorted(coarse, x), side left: the first index with coarse >= x
+    int lo = 0, hi = a.Nc;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (coarse_at(a, mid) < x) lo = mid + 1;
+        else hi = mid;
+    }
+    const int nxt = min(max(lo, 0), a.Nc - 1), prv = min(max(lo - 1, 0), a.Nc - 1);
+    double ip = (coarse_at(a, nxt) - x) / a.hc, in = (x - coarse_at(a, prv)) / a.hc;
+    if (nxt == 0) { ip = 0; in = 1; }
+    if (prv == a.Nc - 1) { in = 0; ip = 1; }
+    a.fine[i] = x;
+    a.idx_prev[i] = prv;
+    a.idx_next[i] = nxt;
+    a.inf_prev[i] = ip;
+    a.inf_next[i] = in;
+}
+
+__global__ void negate_kernel(const double* __restrict__ a, double* __restrict__ out, int n) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) out[k] = -a[k];
+}
+
 }  // namespace
 
 int step_schedule(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& out, const double* beam,
@@ -494,6 +560,62 @@ int lc3d_set_const(lc3d_ctx* c, const lc3d_const_ptrs* k, const lc3d_virt_ptrs* 
         LC3D_CUDA_TRY(cudaMemcpyAsync(c->idx_next, v->indices_next, ni, cudaMemcpyDeviceToDevice, s));
         c->const_set |= 2;
     }
+    return LC3D_OK;
+}
+
+int lc3d_init_plasma(lc3d_ctx* c, void* stream) {
+    if (!c) return LC3D_ERR_PARAM;
+    DeviceGuard g(c->device);
+    const cudaStream_t s = S(stream);
+    const int N = c->N, co = c->p.plasma_coarseness, fi = c->p.plasma_fineness;
+    const int steps = N - 2 * c->p.plasma_padding_steps;
+    PlasmaArgs a;
+    a.m = c->m; a.q = c->q; a.x_init = c->x_init; a.y_init = c->y_init;
+    a.inf_prev = c->inf_prev; a.inf_next = c->inf_next; a.fine = c->fine_grid;
+    a.idx_prev = c->idx_prev; a.idx_next = c->idx_next;
+    a.Nc = c->Nc; a.Nf = c->Nf;
+    a.R = steps / (2 * co);
+    a.Rf = steps / 2 * fi;
+    a.f = fi;
+    a.hc = c->p.grid_step_size * co;
+    a.d = c->p.grid_step_size / fi;
+    a.m0 = (double)(1 * co * co);      // electron mass 1, charge -1 (lcode.py:494-495)
+    a.q0 = (double)(-1 * co * co);
+    const size_t np = (size_t)c->Nc * c->Nc, ng = (size_t)N * N;
+    plasma_coarse_kernel<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(a);
+    plasma_fine_kernel<<<(c->Nf + 255) / 256, 256, 0, s>>>(a);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    c->const_set = 3;
+    // state at the start: zero offsets, momenta, fields, densities and currents
+    lc3d_state_ptrs& st = c->st[c->cur];
+    double* parts[] = {st.x_offt, st.y_offt, st.px, st.py, st.pz};
+    double* grids[] = {st.Ex, st.Ey, st.Ez, st.Bx, st.By, st.Bz, st.ro, st.jx, st.jy, st.jz};
+    for (double* p : parts) LC3D_CUDA_TRY(cudaMemsetAsync(p, 0, np * sizeof(double), s));
+    for (double* p : grids) LC3D_CUDA_TRY(cudaMemsetAsync(p, 0, ng * sizeof(double), s));
+    // ion background = minus the initial electron deposition (lcode.py:692-699)
+    LC3D_TRY(deposit_into(c, nullptr, st.x_offt, st.y_offt, c->m, c->q, st.px, st.py, st.pz, c->dens[0],
+                          c->dens[1], c->dens[2], c->dens[3], s));
+    negate_kernel<<<(unsigned)((ng + 255) / 256), 256, 0, s>>>(c->dens[0], c->ro_initial, (int)ng);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    c->state_set = 1;
+    return LC3D_OK;
+}
+
+int lc3d_get_const(lc3d_ctx* c, double* m, double* q, double* x_init, double* y_init, double* ro_initial,
+                   double* influence_prev, double* influence_next, int32_t* indices_prev, int32_t* indices_next,
+                   double* fine_grid, void* stream) {
+    if (!c) return LC3D_ERR_PARAM;
+    if (c->const_set != 3) return LC3D_ERR_STATE;
+    DeviceGuard g(c->device);
+    const cudaStream_t s = S(stream);
+    const size_t np = (size_t)c->Nc * c->Nc * sizeof(double), ng = (size_t)c->N * c->N * sizeof(double);
+    const size_t nf = (size_t)c->Nf * sizeof(double), ni = (size_t)c->Nf * sizeof(int32_t);
+    struct { void* dst; const void* src; size_t n; } cp[] = {
+        {m, c->m, np}, {q, c->q, np}, {x_init, c->x_init, np}, {y_init, c->y_init, np},
+        {ro_initial, c->ro_initial, ng}, {influence_prev, c->inf_prev, nf}, {influence_next, c->inf_next, nf},
+        {indices_prev, c->idx_prev, ni}, {indices_next, c->idx_next, ni}, {fine_grid, c->fine_grid, nf}};
+    for (auto& e : cp)
+        if (e.dst) LC3D_CUDA_TRY(cudaMemcpyAsync(e.dst, e.src, e.n, cudaMemcpyDeviceToDevice, s));
     return LC3D_OK;
 }
 

@@ -518,6 +518,46 @@ def init(config):
     return xs, ys, const, virt_params, state
 
 
+def init_config_checks(config):
+    """The configuration checks of init() and config.reflect_boundary
+    (lcode.py:941-949)."""
+    assert config.grid_steps % 2 == 1
+    assert config.reflect_padding_steps > config.plasma_coarseness + 1
+    config.reflect_boundary = config.grid_step_size * (
+        config.grid_steps / 2 - config.reflect_padding_steps)
+
+
+def init_device(config):
+    """init(config) with the plasma layout, the ion background and the
+    initial state built on the device (lc3d_init_plasma); returns the same
+    (xs, ys, const, virt_params, state), bit-identical to init()."""
+    init_config_checks(config)
+    N = config.grid_steps
+    grid = (np.arange(N) - N // 2) * config.grid_step_size
+    xs, ys = grid[:, None], grid[None, :]
+    s = solver_for(config)
+    check(lib.lc3d_init_plasma(s.ctx, _stream()), 'lc3d_init_plasma')
+    Nc, Nf = s.Nc, s.Nf
+    const = GPUArrays(m=_empty((Nc, Nc)), q=_empty((Nc, Nc)), x_init=_empty((Nc, Nc)), y_init=_empty((Nc, Nc)),
+                      ro_initial=_empty((N, N)))
+    ip = torch.empty(Nf, dtype=torch.int32, device=_device())
+    inn = torch.empty(Nf, dtype=torch.int32, device=_device())
+    virt = GPUArrays(influence_prev=_empty((Nf,)), influence_next=_empty((Nf,)), fine_grid=_empty((Nf,)))
+    check(lib.lc3d_get_const(s.ctx, *[_ptr(t) for t in (const.m, const.q, const.x_init, const.y_init,
+                                                         const.ro_initial, virt.influence_prev,
+                                                         virt.influence_next, ip, inn, virt.fine_grid)],
+                             _stream()), 'lc3d_get_const')
+    virt.indices_prev = ip.to(torch.int64)
+    virt.indices_next = inn.to(torch.int64)
+    out = {n: _empty((Nc, Nc) if k < 5 else (N, N)) for k, n in enumerate(_lib.STATE_NAMES)}
+    check(lib.lc3d_get_state(s.ctx, ctypes.byref(_lib.StatePtrs(*[out[n].data_ptr() for n in _lib.STATE_NAMES])),
+                             _stream()), 'lc3d_get_state')
+    state = GPUArrays.__new__(GPUArrays)
+    for n in _lib.STATE_NAMES:
+        setattr(state, n, out[n])
+    return xs, ys, const, virt, state
+
+
 # ---------------------------------------------------------------------------
 # CLI loop (lcode.py:1032-1051) with the diagnostics line of
 # lcode.py:979-1026: on-axis Ez, its peak drift and the zn noise figure (the

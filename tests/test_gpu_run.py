@@ -139,3 +139,24 @@ def test_host_beam_step_is_device_beam_step(L):
     for k in STATE:
         assert torch.equal(getattr(a, k), getattr(b, k)), k
         assert torch.equal(getattr(c, k), getattr(b, k)), k
+
+
+@pytest.mark.parametrize('N,h,c,f', [(41, 0.1, 3, 2), (61, 0.1, 2, 3), (81, 0.1, 4, 1), (161, 0.05, 3, 2),
+                                     (641, 0.025, 3, 2)])
+def test_init_on_device_matches_host_init(L, N, h, c, f):
+    """lc3d_init_plasma (plasma layout, ion background, initial state built
+    on the device) against the host layout of init(): bit-identical."""
+    cfg = make_config(N, h, 0.05, 10, amplitude=0.1)
+    cfg.plasma_coarseness, cfg.plasma_fineness = c, f
+    cfg.reflect_padding_steps = max(cfg.reflect_padding_steps, c + 2)
+    xs, ys, const, virt, st = L.init(cfg)
+    xs2, ys2, const2, virt2, st2 = L.lcode.init_device(cfg)
+    assert np.array_equal(xs, xs2) and np.array_equal(ys, ys2)
+    for k in ('m', 'q', 'x_init', 'y_init', 'ro_initial'):
+        assert torch.equal(L.lcode._f64(getattr(const, k)), getattr(const2, k)), k
+    for k in ('influence_prev', 'influence_next', 'fine_grid'):
+        assert torch.equal(L.lcode._f64(getattr(virt, k)), getattr(virt2, k)), k
+    for k in ('indices_prev', 'indices_next'):
+        assert torch.equal(torch.as_tensor(getattr(virt, k)).cuda().long(), getattr(virt2, k)), k
+    for k in STATE:
+        assert torch.equal(L.lcode._f64(getattr(st, k)), getattr(st2, k)), k
