@@ -485,9 +485,9 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
                 e.ld_out = N;
                 switch (stage) {
                     case 0: e.in = c->rhs[f] + g.off; e.rows = g.rows; e.type = g.type1; e.out = c->t1[f]; break;
-                    case 1: e.in = c->t1[f]; e.rows = g.cols; e.type = g.type0; e.out = c->t2[f]; break;
-                    case 2: e.in = c->t2[f]; e.rows = g.rows; e.type = g.type1; e.out = c->t1[f];
-                            e.lam = g.Lam; e.ld_lam = g.ldLam; break;   // Lambda o Z, row by row
+                    case 1: e.in = c->t1[f]; e.rows = g.cols; e.type = g.type0; e.out = c->t2[f];
+                            e.lam = g.Lam; e.ld_lam = g.ldLam; break;   // Lambda o Z as Z is written
+                    case 2: e.in = c->t2[f]; e.rows = g.rows; e.type = g.type1; e.out = c->t1[f]; break;
                     default: e.in = c->t1[f]; e.rows = g.cols; e.type = g.type0; e.out = dst[f] + g.off;
                              if (f == 5) {   // Bz: the mean's partial sums come with the last pass
                                  e.partial = c->red;

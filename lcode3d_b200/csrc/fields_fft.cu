@@ -13,14 +13,16 @@
 // shared memory (P = 1280: 8, 8, 4, 5), read out in digit-reversed order
 // through a position-sorted list. The kernel is persistent: a CTA loops over
 // groups of rows and copies the next group's rows into a staging area with
-// cp.async while the current group's passes run. Every launch transforms rows, optionally
-// scaled on input by Lambda[r][j], and writes its output TRANSPOSED
-// (out[k][r]); the 2-D solve F = L (Lambda o (L X R)) R is then four such
-// passes:
+// cp.async while the current group's passes run. Every launch transforms rows
+// and writes its output TRANSPOSED (out[k][r]), optionally scaled on output
+// by Lambda[k][r]; the 2-D solve F = L (Lambda o (L X R)) R is then four
+// such passes:
 //     A: rows of X by the axis-1 transform                 -> T1^T
-//     B: rows of T1^T by the axis-0 transform              -> Z
+//     B: rows of T1^T by the axis-0 transform, times Lambda -> Lambda o Z
 //     C: rows of Lambda o Z by the axis-1 transform        -> T3^T
 //     D: rows of T3^T by the axis-0 transform              -> F
+// (Lambda on B's output rather than C's input: the multiply is the same,
+// and no Lambda rows take staging space, which keeps 3 CTAs per SM.)
 // One launch covers all fields of a solve.
 
 #include <algorithm>
@@ -57,7 +59,7 @@ struct FftField {
     int ld_in, rows, type;               // type: 0 DCT-I (n = N), 1 DST-I (n = N - 2)
     double* out;
     int ld_out;
-    const double* lam;
+    const double* lam;                   // out[k][r] *= lam[k ld_lam + r], or NULL
     int ld_lam;
     double* partial;                     // per-CTA sums of the written values, or NULL
     int cta_start;
@@ -69,7 +71,6 @@ struct FftBatch {
     int nrad;
     int rad[MAX_RADICES];
     int ngroups;                         // row groups (ROWS_PER_CTA rows) over all fields
-    int stage_lam;                       // the staging area also holds Lambda rows
     const double2* tw;                   // tw[m] = exp(-2 pi i m / P)
     const int* rd;                       // readout lists: DCT-I (N entries), then DST-I (N - 2)
 };
@@ -155,13 +156,19 @@ __device__ __forceinline__ void dft<4>(double2 (&v)[4], const double2*, int) {
 // (X_0 X_2 X_4 X_6 X_1 X_3 X_5 X_7); dft_out<8> maps register -> frequency.
 template <>
 __device__ __forceinline__ void dft<8>(double2 (&v)[8], const double2* tw, int P) {
-    double2 a[4], b[4];
+    // W8 = sqrt(1/2) (1 - i), W8^2 = -i, W8^3 = -sqrt(1/2) (1 + i): no
+    // table loads, two real products each for j = 1, 3
+    constexpr double h = 0.70710678118654752440;
+    double2 a[4], b[4], d[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         a[j] = cadd(v[j], v[j + 4]);
-        const double2 d = csub(v[j], v[j + 4]);
-        b[j] = j ? cmul(d, __ldg(tw + j * (P / 8))) : d;
+        d[j] = csub(v[j], v[j + 4]);
     }
+    b[0] = d[0];
+    b[1] = make_double2(h * (d[1].x + d[1].y), h * (d[1].y - d[1].x));
+    b[2] = mul_mi(d[2]);
+    b[3] = make_double2(h * (d[3].y - d[3].x), -h * (d[3].x + d[3].y));
     dft<4>(a, tw, P);
     dft<4>(b, tw, P);
 #pragma unroll
@@ -235,10 +242,10 @@ __device__ __forceinline__ int field_of(const FftBatch& b, int g) {
     return fi;
 }
 
-// Start copying row group g (ROWS_PER_CTA rows, and their Lambda rows) into
-// the staging area, one 8-byte cp.async per element (rows need not be
-// 16-byte aligned); rows past the field are not copied (the reader uses 0).
-__device__ __forceinline__ void stage_group(const FftBatch& b, int g, double* stg, double* stgL) {
+// Start copying row group g (ROWS_PER_CTA rows) into the staging area, one
+// 8-byte cp.async per element (rows need not be 16-byte aligned); rows past
+// the field are not copied (the reader uses 0).
+__device__ __forceinline__ void stage_group(const FftBatch& b, int g, double* stg) {
     const FftField& F = b.f[field_of(b, g)];
     const int n = F.type ? b.N - 2 : b.N;
     const int r0 = (g - F.cta_start) * ROWS_PER_CTA;
@@ -247,11 +254,7 @@ __device__ __forceinline__ void stage_group(const FftBatch& b, int g, double* st
         const int row = r0 + rr;
         if (row >= F.rows) continue;
         const double* rp = F.in + (size_t)row * F.ld_in;
-        const double* lp = F.lam ? F.lam + (size_t)row * F.ld_lam : nullptr;
-        for (int j = threadIdx.x; j < n; j += FFT_THREADS) {
-            cp_async8(stg + rr * b.N + j, rp + j);
-            if (lp) cp_async8(stgL + rr * b.N + j, lp + j);
-        }
+        for (int j = threadIdx.x; j < n; j += FFT_THREADS) cp_async8(stg + rr * b.N + j, rp + j);
     }
     cp_async_commit();
 }
@@ -265,9 +268,8 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
     const int P = b.P, L = P / 2, PS = P + FFT_PAD;
     double2* A = sm;
     double* stg = reinterpret_cast<double*>(sm + FFT_PER_CTA * PS);   // [ROWS_PER_CTA][N]
-    double* stgL = stg + ROWS_PER_CTA * b.N;                          // [ROWS_PER_CTA][N] if stage_lam
     int g = blockIdx.x;
-    if (g < b.ngroups) stage_group(b, g, stg, stgL);
+    if (g < b.ngroups) stage_group(b, g, stg);
 #pragma unroll 1
     for (; g < b.ngroups; g += gridDim.x) {
     const FftField& F = b.f[field_of(b, g)];
@@ -277,22 +279,16 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
     __syncthreads();                     // the staging area holds group g
 
     // symmetric / antisymmetric extensions, rows 2q and 2q + 1 of the group
-    // as the real and imaginary parts of FFT q, each staged element (scaled
-    // by Lambda[row][j] when given) written to its one or two positions
+    // as the real and imaginary parts of FFT q, each staged element written
+    // to its one or two positions
 #pragma unroll
     for (int q = 0; q < FFT_PER_CTA; ++q) {
         double2* a = A + q * PS;
         const bool ok0 = r0 + 2 * q < F.rows, ok1 = r0 + 2 * q + 1 < F.rows;
         const double* s0 = stg + (2 * q) * b.N;
         const double* s1 = s0 + b.N;
-        const double* l0 = stgL + (2 * q) * b.N;
-        const double* l1 = l0 + b.N;
         for (int j = threadIdx.x; j < n; j += FFT_THREADS) {
-            double x0 = ok0 ? s0[j] : 0.0, x1 = ok1 ? s1[j] : 0.0;
-            if (F.lam) {
-                x0 *= ok0 ? l0[j] : 0.0;
-                x1 *= ok1 ? l1[j] : 0.0;
-            }
+            const double x0 = ok0 ? s0[j] : 0.0, x1 = ok1 ? s1[j] : 0.0;
             const double2 z = make_double2(x0, x1);
             if (F.type == 0) {           // m = j and P - j
                 a[j] = z;
@@ -306,7 +302,7 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
     if (F.type == 1 && threadIdx.x < 2 * FFT_PER_CTA)   // DST-I: zeros at m = 0 and m = L
         A[(threadIdx.x >> 1) * PS + (threadIdx.x & 1) * L] = make_double2(0.0, 0.0);
     __syncthreads();                     // the staging area is free: start the next group
-    if (g + (int)gridDim.x < b.ngroups) stage_group(b, g + gridDim.x, stg, stgL);
+    if (g + (int)gridDim.x < b.ngroups) stage_group(b, g + gridDim.x, stg);
     int span = P;
     for (int p = 0; p < b.nrad; ++p) {
         const int R = b.rad[p];
@@ -325,7 +321,8 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
     // transposed output: out[k][row] for the CTA's rows. The readout list
     // holds (position, k) for the wanted frequencies sorted by position, so
     // a warp reads nearly consecutive shared-memory words; the threads of
-    // one entry (one per FFT) write the CTA's consecutive rows of out[k].
+    // one entry (one per FFT) write the CTA's consecutive rows of out[k]
+    // (and read the same places of Lambda, when given).
     const int* rl = b.rd + (F.type ? b.N : 0);
     const int total = n * FFT_PER_CTA;
     double psum = 0.0;
@@ -337,19 +334,39 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
             const int t = t0 + u * FFT_THREADS + (int)threadIdx.x;
             e[u] = t < total ? __ldg(rl + t / FFT_PER_CTA) : 0;
         }
+        // two halves, so that the Lambda values of only SU / 2 entries are
+        // held in registers at a time
 #pragma unroll
-        for (int u = 0; u < SU; ++u) {
-            const int t = t0 + u * FFT_THREADS + (int)threadIdx.x;
-            const int q = t % FFT_PER_CTA, row = r0 + 2 * q;
-            if (t >= total || row >= F.rows) continue;
-            const double2 z = A[q * PS + (e[u] >> 16)];
-            double* o = F.out + (size_t)(e[u] & 0xffff) * F.ld_out + row;
-            const double x0 = F.type == 0 ? z.x : -z.y, x1 = F.type == 0 ? z.y : z.x;
-            o[0] = x0;
-            psum += x0;
-            if (row + 1 < F.rows) {
-                o[1] = x1;
-                psum += x1;
+        for (int h = 0; h < SU; h += SU / 2) {
+            double la[SU / 2][2];
+            if (F.lam) {
+#pragma unroll
+                for (int u = 0; u < SU / 2; ++u) {
+                    const int t = t0 + (h + u) * FFT_THREADS + (int)threadIdx.x;
+                    const int row = r0 + 2 * (t % FFT_PER_CTA);
+                    const double* lp = F.lam + (size_t)(e[h + u] & 0xffff) * F.ld_lam + row;
+                    la[u][0] = t < total && row < F.rows ? __ldg(lp) : 0.0;
+                    la[u][1] = t < total && row + 1 < F.rows ? __ldg(lp + 1) : 0.0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < SU / 2; ++u) {
+                const int t = t0 + (h + u) * FFT_THREADS + (int)threadIdx.x;
+                const int q = t % FFT_PER_CTA, row = r0 + 2 * q;
+                if (t >= total || row >= F.rows) continue;
+                const double2 z = A[q * PS + (e[h + u] >> 16)];
+                double* o = F.out + (size_t)(e[h + u] & 0xffff) * F.ld_out + row;
+                double x0 = F.type == 0 ? z.x : -z.y, x1 = F.type == 0 ? z.y : z.x;
+                if (F.lam) {
+                    x0 *= la[u][0];
+                    x1 *= la[u][1];
+                }
+                o[0] = x0;
+                psum += x0;
+                if (row + 1 < F.rows) {
+                    o[1] = x1;
+                    psum += x1;
+                }
             }
         }
     }
@@ -400,16 +417,15 @@ int fft_cta_rows() { return ROWS_PER_CTA; }
 
 // Dynamic shared memory of fft_rows_kernel, the layout the kernel uses: the
 // FFT buffers at a pitch of P + FFT_PAD double2 words, then the staging rows
-// (ROWS_PER_CTA x N doubles, twice when Lambda rows are staged too).
-size_t fft_cta_smem_bytes(int P, int N, int stage_lam) {
-    return (size_t)FFT_PER_CTA * (P + FFT_PAD) * sizeof(double2) +
-           (size_t)ROWS_PER_CTA * N * sizeof(double) * (1 + stage_lam);
+// (ROWS_PER_CTA x N doubles).
+size_t fft_cta_smem_bytes(int P, int N) {
+    return (size_t)FFT_PER_CTA * (P + FFT_PAD) * sizeof(double2) + (size_t)ROWS_PER_CTA * N * sizeof(double);
 }
 
 int fft_init(lc3d_ctx* c) {
     const int N = c->N, P = 2 * (N - 1);
     int rad[MAX_RADICES];
-    c->fft_ok = fft_plan(P, rad) > 0 && fft_cta_smem_bytes(P, N, 1) <= 200 * 1024;
+    c->fft_ok = fft_plan(P, rad) > 0 && fft_cta_smem_bytes(P, N) <= 200 * 1024;
     if (!c->fft_ok) return LC3D_OK;
     LC3D_TRY(fft_prepare(P));
     const int nrad = fft_plan(P, rad);
@@ -476,11 +492,10 @@ int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, cudaStream_t s) {
         f.partial = desc[q].partial;
         f.cta_start = ctas;
         ctas += (f.rows + ROWS_PER_CTA - 1) / ROWS_PER_CTA;
-        if (f.lam) b.stage_lam = 1;
     }
     if (!ctas) return LC3D_OK;
     b.ngroups = ctas;
-    const size_t smem = fft_cta_smem_bytes(b.P, b.N, b.stage_lam);
+    const size_t smem = fft_cta_smem_bytes(b.P, b.N);
     // persistent grid: as many CTAs as fit on the device at once
     int dev = 0, sms = 0, per_sm = 0;
     LC3D_CUDA_TRY(cudaGetDevice(&dev));

@@ -124,8 +124,8 @@ int solve_fields(lc3d_ctx* ctx, int which, const SolveInputs& in,
                  const SolveOutputs& o, cudaStream_t s);
 
 // FFT row transforms (fields_fft.cu): rows of `in` (length N for DCT-I,
-// N - 2 for DST-I), optionally multiplied element-wise by lam[r][j] on
-// input, are transformed and written transposed, out[k][r].
+// N - 2 for DST-I) are transformed and written transposed, out[k][r],
+// optionally multiplied element-wise by lam[k][r] as they are written.
 struct FftRowsDesc {
     const double* in;
     int ld_in, rows, type;                // type: 0 DCT-I, 1 DST-I

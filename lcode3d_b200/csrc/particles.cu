@@ -11,9 +11,9 @@
 //     c = hi * 2^-24 + lo * 2^-76 + (rounding below 2^-77),
 // which are summed with 64-bit integer adds; integer addition is associative,
 // so the sums do not depend on the order in which threads add them, and the
-// final conversion rounds once. Each CTA owns a 32x32 patch of the fine
-// lattice and accumulates into a shared-memory window placed on the bounding
-// box of its particles' cells; particles whose stencil falls outside the
+// final conversion rounds once. Each CTA owns a 16x32 patch of the fine
+// lattice and accumulates into a 32x32-cell shared-memory window placed on
+// the bounding box of its particles' cells; particles whose stencil falls outside the
 // window (strongly displaced plasma) add straight to the global accumulators.
 // The window is then flushed with 64-bit integer reductions into global
 // memory, and a finalize pass converts to float64, adds the ion background
