@@ -12,7 +12,7 @@ LIB_PATH = os.path.join(HERE, 'liblc3d.so')
 c_int, c_double, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
 OK, ERR_PARAM, ERR_CUDA, ERR_WINDOW, ERR_NONFINITE, ERR_STATE, ERR_SIZE, ERR_TIMEOUT = range(8)
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FFT32 = 0, 1, 2
 FP64_AUTO, FP64_FFT, FP64_DENSE = 0, 1, 2
 
 
@@ -123,7 +123,7 @@ class LC3DError(RuntimeError):
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f'{LIB_PATH} is missing: build it with `python -m lcode3d_b200.build` '
+            f'{LIB_PATH} is missing: build it with `python lcode3d_b200/build.py` '
             '(nvcc, sm_100a). There is no CPU fallback.')
     lib = ctypes.CDLL(LIB_PATH)
     for name, res, args in SIGNATURES:

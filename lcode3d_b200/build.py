@@ -1,6 +1,6 @@
 """Build liblc3d.so (the C-ABI CUDA library) in-tree for sm_100a.
 
-    python -m lcode3d_b200.build          # or: python lcode3d_b200/build.py
+    python lcode3d_b200/build.py          # (importing the package needs the library)
 
 The library is written next to this file so that it travels with the source
 tree; nothing is installed into site-packages.
