@@ -2,7 +2,7 @@
 """Throughput of the LCODE 3D xi step on B200: xi-steps/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|mixed] [--grid 641]
+                    [--precision fp64|mixed|fft32] [--grid 641]
 
 Workload (default): the production grid of the reference's example config,
 641 x 641 cells, h = 0.025 (window +-8), plasma coarseness 3 / fineness 2
@@ -183,14 +183,19 @@ def transform_flops_per_launch(N):
     return sum(4 * r * c * (r + c) for r, c in dims) / 4
 
 
-def fft_bytes_per_launch(N):
-    """Algorithmic bytes of one FFT row pass over the 6 fields of a solve:
-    every field's r x c array is read once and written once (8 bytes per
-    element); one of the 4 passes also reads the eigenvalue matrix, counted
-    as a quarter per launch."""
+def fft_bytes_per_launch(N, fp32=False):
+    """Algorithmic bytes of one FFT row pass over the 6 fields of a solve,
+    averaged over the 4 passes: every field's r x c array is read once and
+    written once per pass, and one pass also reads the eigenvalue matrix.
+    float64: 8 bytes per element everywhere (8 + 8, plus 8 / 4 for the
+    eigenvalues). float32 transforms: the first pass reads float64 and
+    writes float32, the last reads float32 and writes float64, the
+    intermediates and eigenvalues are float32 (44 bytes per element over
+    the 4 passes)."""
     M = N - 2
     dims = [(N, M), (M, N), (M, M), (M, N), (N, M), (N, N)]
-    return sum(8 * r * c * (2 + 0.25) for r, c in dims)
+    per = 44 / 4 if fp32 else 8 * (2 + 0.25)
+    return sum(per * r * c for r, c in dims)
 
 
 def deposit_bytes_per_launch(N, Nc, Nf):
@@ -221,8 +226,12 @@ def run_ours(args, rank, world, dist):
 
     # advance (untimed) into the beam with the public API
     t_pre = time.time()
+    ez_pre = []   # reduced precisions: Ez(N/2, N/2) of the pre-steps, for the float64 comparison
     for i in range(args.pre):
         st = L.step(cfg, const, virt, st, beam_np(cfg, i, xs, ys))
+        if args.precision != 'fp64':
+            ez_pre.append(st.Ez[N // 2, N // 2].clone())
+    ez_field_pre = st.Ez.clone() if args.precision != 'fp64' and args.pre else None
     torch.cuda.synchronize()
     t_pre = time.time() - t_pre
     x0 = args.pre
@@ -334,11 +343,13 @@ def run_ours(args, rank, world, dist):
         roof = {'kernel': f'oz_gemm_kernel (tcgen05 split-BF16 transforms, {S} slices, {S * (S + 1) // 2} products)',
                 'bound': 'tensor', 'achieved': ach, 'peak': pk, 'unit': 'TFLOP/s', 'frac': ach / pk,
                 'peak_source': src, 'algorithmic_per_launch': fl, 'avg_launch_ms': avg_ms, 'traffic': None}
-    elif dom == 'transform' and stage[dom]['timed'] and use_fft:
+    elif dom == 'transform' and stage[dom]['timed'] and (use_fft or args.precision == 'fft32'):
         avg_ms = stage[dom]['ms'] / stage[dom]['timed']
-        by = fft_bytes_per_launch(N)
+        f32 = args.precision == 'fft32'
+        by = fft_bytes_per_launch(N, f32)
         ach = by / (avg_ms * 1e-3) / 1e9
-        roof = {'kernel': 'fft_rows_kernel (FP64 DST/DCT row-FFT pass, 6 fields)', 'bound': 'hbm',
+        roof = {'kernel': f'fft_rows_kernel ({"FP32" if f32 else "FP64"} DST/DCT row-FFT pass, 6 fields)',
+                'bound': 'hbm',
                 'achieved': ach, 'peak': hbm, 'unit': 'GB/s', 'frac': ach / hbm,
                 'peak_source': hbm_src, 'algorithmic_per_launch': by, 'avg_launch_ms': avg_ms,
                 'traffic': None}
@@ -367,7 +378,8 @@ def run_ours(args, rank, world, dist):
     out = {
         'metric': METRIC, 'value': value, 'unit': 'xi-steps/s', 'n_gpus': world,
         'steps': K, 'warmup': W, 'ms_per_step': total_ms / K, 'higher_is_better': True,
-        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64' if args.precision == 'fp64' else 'f64+bf16',
+        'scaling': 'weak', 'vs_baseline': None,
+        'dtype': {'fp64': 'f64', 'mixed': 'f64+bf16', 'fft32': 'f64+f32'}[args.precision],
         'data': 'synthetic (generated cold uniform plasma + axisymmetric beam; no dataset)',
         'config': {'workload': f'LCODE 3D xi step, {N}x{N} grid, h={cfg.grid_step_size}, '
                                f'xi_step={cfg.xi_step_size}, coarseness 3 / fineness 2, A={GRIDS[N][2]}, '
@@ -391,7 +403,32 @@ def run_ours(args, rank, world, dist):
                   'how': 'the same K steps as one lc3d_run: CUDA-graph replay per step, beam evaluated '
                          'on the device, Ez(0,0) recorded on the device, no L2 flush between steps'},
     }
+    if ez_field_pre is not None:
+        out['accuracy_vs_fp64'] = accuracy_vs_fp64(args, ez_pre, ez_field_pre)
     return out
+
+
+def accuracy_vs_fp64(args, ez_pre, ez_field_pre):
+    """Ez of the reduced-precision pre-steps against the same steps in
+    float64 from the same initial state: the on-axis Ez(N/2, N/2) history
+    and the final Ez field, each as max |difference| / max |float64|."""
+    import torch
+    import lcode3d_b200 as L
+    cfg = make_config(args.grid, 'fp64')
+    N = cfg.grid_steps
+    xs, ys, const, virt, st = L.init(cfg)
+    ez = []
+    for i in range(args.pre):
+        st = L.step(cfg, const, virt, st, beam_np(cfg, i, xs, ys))
+        ez.append(st.Ez[N // 2, N // 2].clone())
+    h64 = torch.stack(ez).cpu().numpy()
+    h = torch.stack(ez_pre).cpu().numpy()
+    f64 = st.Ez.cpu().numpy()
+    f = ez_field_pre.cpu().numpy()
+    e_h = float(np.abs(h - h64).max() / max(np.abs(h64).max(), 1e-300))
+    e_f = float(np.abs(f - f64).max() / max(np.abs(f64).max(), 1e-300))
+    return {'steps': args.pre, 'ez_axis_history_max_rel': e_h, 'ez_field_max_rel': e_f,
+            'within_1e-6': bool(max(e_h, e_f) <= 1e-6)}
 
 
 # ---------------------------------------------------------------------------
@@ -587,7 +624,7 @@ def main():
     ap.add_argument('--steps', type=int, default=100)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--precision', default='fp64', choices=['fp64', 'mixed'])
+    ap.add_argument('--precision', default='fp64', choices=['fp64', 'mixed', 'fft32'])
     ap.add_argument('--fp64-transform', default='auto', choices=['auto', 'fft', 'dense'])
     ap.add_argument('--slices', type=int, default=4, help='bf16 slices per operand (mixed precision)')
     ap.add_argument('--grid', type=int, default=641, choices=sorted(GRIDS))

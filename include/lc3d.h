@@ -47,12 +47,16 @@ extern "C" {
 #define LC3D_ERR_TIMEOUT 7      /* device flag: a bounded wait in a kernel ran out */
 
 /* Precision of the field solvers. */
-#define LC3D_PREC_FP64 0        /* float64 dense-transform (DGEMM-form) solvers */
+#define LC3D_PREC_FP64 0        /* float64 solvers (transform form: fp64_transform) */
 #define LC3D_PREC_MIXED 1       /* split-BF16 tcgen05 transforms, fp32 accumulate,
                                    float64 combination; grid_steps <= 1000 */
+#define LC3D_PREC_FFT32 2       /* float32 FFT transforms (float32 intermediates and
+                                   eigenvalues); right-hand sides, field outputs,
+                                   averaging and particles stay float64; needs
+                                   2(N-1) to factor into 2, 3 and 5 */
 
 /* Float64 transform method (lc3d_params.fp64_transform). */
-#define LC3D_FP64_AUTO 0        /* FFT when 2(N-1) factors into 2, 3, 5, 7; else dense */
+#define LC3D_FP64_AUTO 0        /* FFT when 2(N-1) factors into 2, 3, 5; else dense */
 #define LC3D_FP64_FFT 1         /* shared-memory FFT DST-I / DCT-I */
 #define LC3D_FP64_DENSE 2       /* dense transform matrices (DGEMM form) */
 

@@ -293,6 +293,14 @@ int upload(double** dst, const std::vector<double>& v) {
     return LC3D_OK;
 }
 
+// float copy of an eigenvalue matrix (float32-transform precision)
+int upload32(float** dst, const std::vector<double>& v) {
+    std::vector<float> f(v.begin(), v.end());
+    LC3D_CUDA_TRY(cudaMalloc(dst, f.size() * sizeof(float)));
+    LC3D_CUDA_TRY(cudaMemcpy(*dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return LC3D_OK;
+}
+
 }  // namespace
 
 int fields_init(lc3d_ctx* c) {
@@ -334,6 +342,12 @@ int fields_init(lc3d_ctx* c) {
     LC3D_TRY(upload(&c->lam_mix, lm));
     LC3D_TRY(upload(&c->lam_mixT, lmT));
     LC3D_TRY(upload(&c->lam_neu, ln));
+    if (c->p.precision == LC3D_PREC_FFT32) {
+        LC3D_TRY(upload32(&c->lam32_dir, ld));
+        LC3D_TRY(upload32(&c->lam32_mix, lm));
+        LC3D_TRY(upload32(&c->lam32_mixT, lmT));
+        LC3D_TRY(upload32(&c->lam32_neu, ln));
+    }
     const size_t plane = (size_t)N * N * sizeof(double);
     for (int f = 0; f < 6; ++f) {
         LC3D_CUDA_TRY(cudaMalloc(&c->rhs[f], plane));
@@ -352,6 +366,11 @@ int fields_init(lc3d_ctx* c) {
 void fields_free(lc3d_ctx* c) {
     double** ps[] = {&c->S2, &c->C, &c->CT, &c->lam_dir, &c->lam_mix, &c->lam_mixT, &c->lam_neu, &c->red};
     for (double** p : ps) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    float** ps32[] = {&c->lam32_dir, &c->lam32_mix, &c->lam32_mixT, &c->lam32_neu};
+    for (float** p : ps32) {
         if (*p) cudaFree(*p);
         *p = nullptr;
     }
@@ -392,6 +411,16 @@ FieldGeom geom(const lc3d_ctx* c, int f) {
             break;
     }
     return g;
+}
+
+// The float copy of field f's eigenvalue matrix (float32-transform precision).
+const float* lam32(const lc3d_ctx* c, int f) {
+    switch (f) {
+        case 0: case 4: return c->lam32_mixT;
+        case 1: case 3: return c->lam32_mix;
+        case 2: return c->lam32_dir;
+        default: return c->lam32_neu;
+    }
 }
 
 }  // namespace
@@ -471,8 +500,13 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
             }
             LC3D_TRY(mixed_stage(c, d, cnt, s));
         }
-    } else if (c->use_fft) {
-        // four FFT row passes, each writing its output transposed
+    } else if (c->use_fft || c->p.precision == LC3D_PREC_FFT32) {
+        // four FFT row passes, each writing its output transposed; with the
+        // float32-transform precision the passes compute in float32 and the
+        // two intermediates (in the t1 / t2 planes) are float32
+        const bool f32 = c->p.precision == LC3D_PREC_FFT32;
+        const int types[4] = {f32 ? FFT_F64_F32 : FFT_F64, f32 ? FFT_F32 : FFT_F64, f32 ? FFT_F32 : FFT_F64,
+                              f32 ? FFT_F32_F64 : FFT_F64};
         for (int stage = 0; stage < 4; ++stage) {
             FftRowsDesc d[6];
             int cnt = 0;
@@ -486,7 +520,8 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
                 switch (stage) {
                     case 0: e.in = c->rhs[f] + g.off; e.rows = g.rows; e.type = g.type1; e.out = c->t1[f]; break;
                     case 1: e.in = c->t1[f]; e.rows = g.cols; e.type = g.type0; e.out = c->t2[f];
-                            e.lam = g.Lam; e.ld_lam = g.ldLam; break;   // Lambda o Z as Z is written
+                            e.lam = f32 ? static_cast<const void*>(lam32(c, f)) : g.Lam;
+                            e.ld_lam = g.ldLam; break;   // Lambda o Z as Z is written
                     case 2: e.in = c->t2[f]; e.rows = g.rows; e.type = g.type1; e.out = c->t1[f]; break;
                     default: e.in = c->t1[f]; e.rows = g.cols; e.type = g.type0; e.out = dst[f] + g.off;
                              if (f == 5) {   // Bz: the mean's partial sums come with the last pass
@@ -496,7 +531,7 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
                              break;
                 }
             }
-            LC3D_TRY(fft_rows(c, d, cnt, s));
+            LC3D_TRY(fft_rows(c, d, cnt, types[stage], s));
         }
     } else {
         // the four GEMM stages

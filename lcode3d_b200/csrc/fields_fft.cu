@@ -49,17 +49,20 @@ static_assert(FFT_THREADS % 32 == 0 && FFT_THREADS <= 1024, "whole warps");
 #define LC3D_FFT_MAX_RADIX 8              // largest power-of-two butterfly in a plan (8 or 4)
 #endif
 #ifndef LC3D_FFT_MIN_BLOCKS
-#define LC3D_FFT_MIN_BLOCKS 3             // resident CTAs per SM the registers allow
+#define LC3D_FFT_MIN_BLOCKS 3             // resident CTAs per SM the registers allow (float64)
+#endif
+#ifndef LC3D_FFT32_MIN_BLOCKS
+#define LC3D_FFT32_MIN_BLOCKS 4           // ... (float32 transforms)
 #endif
 constexpr int MAX_RADICES = 24;
-constexpr int FFT_PAD = 4;               // double2 words between the CTA's two FFTs (bank offset)
+constexpr int FFT_PAD = 4;               // complex words between the CTA's two FFTs (bank offset)
 
 struct FftField {
-    const double* in;
+    const void* in;                      // Tin rows
     int ld_in, rows, type;               // type: 0 DCT-I (n = N), 1 DST-I (n = N - 2)
-    double* out;
+    void* out;                           // Tout
     int ld_out;
-    const double* lam;                   // out[k][r] *= lam[k ld_lam + r], or NULL
+    const void* lam;                     // T: out[k][r] *= lam[k ld_lam + r], or NULL
     int ld_lam;
     double* partial;                     // per-CTA sums of the written values, or NULL
     int cta_start;
@@ -72,109 +75,108 @@ struct FftBatch {
     int rad[MAX_RADICES];
     int ngroups;                         // row groups (ROWS_PER_CTA rows) over all fields
     const double2* tw;                   // tw[m] = exp(-2 pi i m / P)
+    const float2* tw32;                  // the same rounded to float
     const int* rd;                       // readout lists: DCT-I (N entries), then DST-I (N - 2)
 };
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// Complex values of the transform arithmetic: double2 (float64 solves) or
+// float2 (float32-transform solves).
+template <typename V> struct ReOf;
+template <> struct ReOf<double2> { using type = double; };
+template <> struct ReOf<float2> { using type = float; };
+template <typename T> struct CxOf;
+template <> struct CxOf<double> { using type = double2; };
+template <> struct CxOf<float> { using type = float2; };
 
-// Small DFTs in registers, forward sign.
-template <int R>
-__device__ __forceinline__ void dft(double2 (&v)[R], const double2* __restrict__ tw, int P) {
-    double2 o[R];
-#pragma unroll
-    for (int m = 0; m < R; ++m) {
-        double2 s = v[0];
-#pragma unroll
-        for (int r = 1; r < R; ++r) s = cadd(s, cmul(v[r], __ldg(tw + ((r * m) % R) * (P / R))));
-        o[m] = s;
-    }
-#pragma unroll
-    for (int m = 0; m < R; ++m) v[m] = o[m];
+template <typename V>
+__device__ __forceinline__ V cmk(typename ReOf<V>::type a, typename ReOf<V>::type b) {
+    V r;
+    r.x = a;
+    r.y = b;
+    return r;
 }
-
-template <>
-__device__ __forceinline__ void dft<2>(double2 (&v)[2], const double2*, int) {
-    const double2 a = v[0], b = v[1];
-    v[0] = cadd(a, b);
-    v[1] = csub(a, b);
+template <typename V>
+__device__ __forceinline__ V cmul(V a, V b) {
+    return cmk<V>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-
+template <typename V>
+__device__ __forceinline__ V cadd(V a, V b) { return cmk<V>(a.x + b.x, a.y + b.y); }
+template <typename V>
+__device__ __forceinline__ V csub(V a, V b) { return cmk<V>(a.x - b.x, a.y - b.y); }
 // x -> -i x
-__device__ __forceinline__ double2 mul_mi(double2 a) { return make_double2(a.y, -a.x); }
-__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+template <typename V>
+__device__ __forceinline__ V mul_mi(V a) { return cmk<V>(a.y, -a.x); }
+template <typename V>
+__device__ __forceinline__ V cscale(V a, typename ReOf<V>::type s) { return cmk<V>(a.x * s, a.y * s); }
 
-// 3-point DFT: W = exp(-2 pi i / 3) = (c, -s) read from the twiddle table.
-template <>
-__device__ __forceinline__ void dft<3>(double2 (&v)[3], const double2* tw, int P) {
-    const double2 w = __ldg(tw + P / 3);
-    const double2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
-    const double2 a = cadd(v[0], cscale(t1, w.x));
-    const double2 bb = cscale(t2, -w.y);
-    v[0] = cadd(v[0], t1);
-    v[1] = cadd(a, mul_mi(bb));
-    v[2] = csub(a, mul_mi(bb));
-}
-
-// 5-point DFT with W = (c1, -s1), W^2 = (c2, -s2) from the twiddle table:
-// X1,4 = v0 + c1 t1 + c2 t2 -+ i (s1 t3 + s2 t4),
-// X2,3 = v0 + c2 t1 + c1 t2 -+ i (s2 t3 - s1 t4),
-// t1 = v1 + v4, t2 = v2 + v3, t3 = v1 - v4, t4 = v2 - v3.
-template <>
-__device__ __forceinline__ void dft<5>(double2 (&v)[5], const double2* tw, int P) {
-    const double2 w1 = __ldg(tw + P / 5), w2 = __ldg(tw + 2 * (P / 5));
-    const double c1 = w1.x, s1 = -w1.y, c2 = w2.x, s2 = -w2.y;
-    const double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
-    const double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
-    const double2 a1 = cadd(v[0], cadd(cscale(t1, c1), cscale(t2, c2)));
-    const double2 a2 = cadd(v[0], cadd(cscale(t1, c2), cscale(t2, c1)));
-    const double2 b1 = cadd(cscale(t3, s1), cscale(t4, s2));
-    const double2 b2 = csub(cscale(t3, s2), cscale(t4, s1));
-    v[0] = cadd(v[0], cadd(t1, t2));
-    v[1] = cadd(a1, mul_mi(b1));
-    v[4] = csub(a1, mul_mi(b1));
-    v[2] = cadd(a2, mul_mi(b2));
-    v[3] = csub(a2, mul_mi(b2));
-}
-
-template <>
-__device__ __forceinline__ void dft<4>(double2 (&v)[4], const double2*, int) {
-    const double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-    const double2 a2 = cadd(v[1], v[3]), d = csub(v[1], v[3]);
-    const double2 a3 = make_double2(d.y, -d.x);   // -i (v1 - v3)
-    v[0] = cadd(a0, a2);
-    v[2] = csub(a0, a2);
-    v[1] = cadd(a1, a3);
-    v[3] = csub(a1, a3);
-}
-
-// 8-point DFT as 2 x 4: a_j = v_j + v_{j+4}, b_j = (v_j - v_{j+4}) W8^j,
-// X_2k = DFT4(a)_k, X_2k+1 = DFT4(b)_k. Outputs are left in register order
-// (X_0 X_2 X_4 X_6 X_1 X_3 X_5 X_7); dft_out<8> maps register -> frequency.
-template <>
-__device__ __forceinline__ void dft<8>(double2 (&v)[8], const double2* tw, int P) {
-    // W8 = sqrt(1/2) (1 - i), W8^2 = -i, W8^3 = -sqrt(1/2) (1 + i): no
-    // table loads, two real products each for j = 1, 3
-    constexpr double h = 0.70710678118654752440;
-    double2 a[4], b[4], d[4];
+// Small DFTs in registers, forward sign, R = 2, 3, 4, 5, 8.
+//  3: W = exp(-2 pi i / 3) = (c, -s) from the twiddle table.
+//  5: W = (c1, -s1), W^2 = (c2, -s2) from the twiddle table;
+//     X1,4 = v0 + c1 t1 + c2 t2 -+ i (s1 t3 + s2 t4),
+//     X2,3 = v0 + c2 t1 + c1 t2 -+ i (s2 t3 - s1 t4),
+//     t1 = v1 + v4, t2 = v2 + v3, t3 = v1 - v4, t4 = v2 - v3.
+//  8: 2 x 4, a_j = v_j + v_{j+4}, b_j = (v_j - v_{j+4}) W8^j,
+//     X_2k = DFT4(a)_k, X_2k+1 = DFT4(b)_k. Outputs are left in register
+//     order (X_0 X_2 X_4 X_6 X_1 X_3 X_5 X_7); dft_out<8> maps register ->
+//     frequency. W8 = sqrt(1/2) (1 - i), W8^2 = -i, W8^3 = -sqrt(1/2) (1 + i):
+//     no table loads, two real products each for j = 1, 3.
+template <int R, typename V>
+__device__ __forceinline__ void dft(V (&v)[R], const V* __restrict__ tw, int P) {
+    using T = typename ReOf<V>::type;
+    static_assert(R == 2 || R == 3 || R == 4 || R == 5 || R == 8, "radix 2, 3, 4, 5 or 8");
+    if constexpr (R == 2) {
+        const V a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 3) {
+        const V w = __ldg(tw + P / 3);
+        const V t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+        const V a = cadd(v[0], cscale(t1, w.x));
+        const V bb = cscale(t2, -w.y);
+        v[0] = cadd(v[0], t1);
+        v[1] = cadd(a, mul_mi(bb));
+        v[2] = csub(a, mul_mi(bb));
+    } else if constexpr (R == 4) {
+        const V a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+        const V a2 = cadd(v[1], v[3]);
+        const V a3 = mul_mi(csub(v[1], v[3]));   // -i (v1 - v3)
+        v[0] = cadd(a0, a2);
+        v[2] = csub(a0, a2);
+        v[1] = cadd(a1, a3);
+        v[3] = csub(a1, a3);
+    } else if constexpr (R == 5) {
+        const V w1 = __ldg(tw + P / 5), w2 = __ldg(tw + 2 * (P / 5));
+        const T c1 = w1.x, s1 = -w1.y, c2 = w2.x, s2 = -w2.y;
+        const V t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        const V t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        const V a1 = cadd(v[0], cadd(cscale(t1, c1), cscale(t2, c2)));
+        const V a2 = cadd(v[0], cadd(cscale(t1, c2), cscale(t2, c1)));
+        const V b1 = cadd(cscale(t3, s1), cscale(t4, s2));
+        const V b2 = csub(cscale(t3, s2), cscale(t4, s1));
+        v[0] = cadd(v[0], cadd(t1, t2));
+        v[1] = cadd(a1, mul_mi(b1));
+        v[4] = csub(a1, mul_mi(b1));
+        v[2] = cadd(a2, mul_mi(b2));
+        v[3] = csub(a2, mul_mi(b2));
+    } else {
+        constexpr T h = (T)0.70710678118654752440;
+        V a[4], b[4], d[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        a[j] = cadd(v[j], v[j + 4]);
-        d[j] = csub(v[j], v[j + 4]);
-    }
-    b[0] = d[0];
-    b[1] = make_double2(h * (d[1].x + d[1].y), h * (d[1].y - d[1].x));
-    b[2] = mul_mi(d[2]);
-    b[3] = make_double2(h * (d[3].y - d[3].x), -h * (d[3].x + d[3].y));
-    dft<4>(a, tw, P);
-    dft<4>(b, tw, P);
+        for (int j = 0; j < 4; ++j) {
+            a[j] = cadd(v[j], v[j + 4]);
+            d[j] = csub(v[j], v[j + 4]);
+        }
+        b[0] = d[0];
+        b[1] = cmk<V>(h * (d[1].x + d[1].y), h * (d[1].y - d[1].x));
+        b[2] = mul_mi(d[2]);
+        b[3] = cmk<V>(h * (d[3].y - d[3].x), -h * (d[3].x + d[3].y));
+        dft<4>(a, tw, P);
+        dft<4>(b, tw, P);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        v[j] = a[j];
-        v[j + 4] = b[j];
+        for (int j = 0; j < 4; ++j) {
+            v[j] = a[j];
+            v[j + 4] = b[j];
+        }
     }
 }
 
@@ -193,17 +195,17 @@ __device__ __forceinline__ constexpr int dft_out(int r) {
 // The twiddles w^m, w = exp(-2 pi i k / Lr), are one table load and a
 // product tree w^m = w^(m/2) w^(m - m/2) (at most three roundings deep for
 // R <= 8), which keeps the R - 1 scattered table loads off the L1 pipe.
-template <int R>
-__device__ __forceinline__ void dif_butterfly(double2* A, int b, int span, float inv_span, int tstep, int P,
-                                              const double2* __restrict__ tw) {
+template <int R, typename V>
+__device__ __forceinline__ void dif_butterfly(V* A, int b, int span, float inv_span, int tstep, int P,
+                                              const V* __restrict__ tw) {
     // g = b / span: (b + 0.5) / span lies at least 0.5 / span from an
     // integer, far more than the float rounding for b, span < 2^16
     const int g = __float2int_rz(((float)b + 0.5f) * inv_span), k = b - g * span;
     const int base = g * span * R + k;
-    double2 v[R];
+    V v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = A[base + r * span];
-    double2 w[R];
+    V w[R];
     w[1] = __ldg(tw + k * tstep);
 #pragma unroll
     for (int m = 2; m < R; ++m) w[m] = cmul(w[m / 2], w[m - m / 2]);
@@ -215,8 +217,8 @@ __device__ __forceinline__ void dif_butterfly(double2* A, int b, int span, float
     }
 }
 
-template <int R>
-__device__ __forceinline__ void fft_pass(double2* A, int span, int P, const double2* tw) {
+template <int R, typename V>
+__device__ __forceinline__ void fft_pass(V* A, int span, int P, const V* tw) {
     const int nb = P / R;
     const float inv_span = 1.0f / (float)span;
     const int tstep = P / (span * R);   // twiddle stride of this pass
@@ -226,10 +228,14 @@ __device__ __forceinline__ void fft_pass(double2* A, int span, int P, const doub
     }
 }
 
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-                 "l"(src)
-                 : "memory");
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+    static_assert(BYTES == 4 || BYTES == 8, "4- or 8-byte copies");
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    if constexpr (BYTES == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
@@ -243,9 +249,10 @@ __device__ __forceinline__ int field_of(const FftBatch& b, int g) {
 }
 
 // Start copying row group g (ROWS_PER_CTA rows) into the staging area, one
-// 8-byte cp.async per element (rows need not be 16-byte aligned); rows past
-// the field are not copied (the reader uses 0).
-__device__ __forceinline__ void stage_group(const FftBatch& b, int g, double* stg) {
+// cp.async per element (rows need not be 16-byte aligned); rows past the
+// field are not copied (the reader uses 0).
+template <typename Tin>
+__device__ __forceinline__ void stage_group(const FftBatch& b, int g, Tin* stg) {
     const FftField& F = b.f[field_of(b, g)];
     const int n = F.type ? b.N - 2 : b.N;
     const int r0 = (g - F.cta_start) * ROWS_PER_CTA;
@@ -253,21 +260,31 @@ __device__ __forceinline__ void stage_group(const FftBatch& b, int g, double* st
     for (int rr = 0; rr < ROWS_PER_CTA; ++rr) {
         const int row = r0 + rr;
         if (row >= F.rows) continue;
-        const double* rp = F.in + (size_t)row * F.ld_in;
-        for (int j = threadIdx.x; j < n; j += FFT_THREADS) cp_async8(stg + rr * b.N + j, rp + j);
+        const Tin* rp = static_cast<const Tin*>(F.in) + (size_t)row * F.ld_in;
+        for (int j = threadIdx.x; j < n; j += FFT_THREADS) cp_async<sizeof(Tin)>(stg + rr * b.N + j, rp + j);
     }
     cp_async_commit();
 }
 
+// Resident CTAs per SM the register budget is sized for: float64 butterflies
+// need twice the registers of float32 ones.
+template <typename T>
+constexpr int fft_min_blocks() { return sizeof(T) == 8 ? LC3D_FFT_MIN_BLOCKS : LC3D_FFT32_MIN_BLOCKS; }
+
 // Persistent: CTA i transforms row groups i, i + gridDim.x, ...; the rows
 // of the next group are copied into the staging area (cp.async) while the
 // current group's FFT passes run, so the global-load latency of a group is
-// hidden behind the previous group's work.
-__global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_kernel(const __grid_constant__ FftBatch b) {
-    extern __shared__ double2 sm[];      // FFT q at sm + q (P + FFT_PAD); then the staging rows
+// hidden behind the previous group's work. Arithmetic in T; rows read as
+// Tin and written as Tout.
+template <typename T, typename Tin, typename Tout>
+__global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_kernel(const __grid_constant__ FftBatch b) {
+    using V = typename CxOf<T>::type;
+    extern __shared__ __align__(16) unsigned char fft_smem[];   // FFT q at q (P + FFT_PAD); then the staging rows
     const int P = b.P, L = P / 2, PS = P + FFT_PAD;
-    double2* A = sm;
-    double* stg = reinterpret_cast<double*>(sm + FFT_PER_CTA * PS);   // [ROWS_PER_CTA][N]
+    V* A = reinterpret_cast<V*>(fft_smem);
+    Tin* stg = reinterpret_cast<Tin*>(A + FFT_PER_CTA * PS);   // [ROWS_PER_CTA][N]
+    const V* tw = reinterpret_cast<const V*>(sizeof(T) == 8 ? static_cast<const void*>(b.tw)
+                                                            : static_cast<const void*>(b.tw32));
     int g = blockIdx.x;
     if (g < b.ngroups) stage_group(b, g, stg);
 #pragma unroll 1
@@ -283,24 +300,24 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
     // to its one or two positions
 #pragma unroll
     for (int q = 0; q < FFT_PER_CTA; ++q) {
-        double2* a = A + q * PS;
+        V* a = A + q * PS;
         const bool ok0 = r0 + 2 * q < F.rows, ok1 = r0 + 2 * q + 1 < F.rows;
-        const double* s0 = stg + (2 * q) * b.N;
-        const double* s1 = s0 + b.N;
+        const Tin* s0 = stg + (2 * q) * b.N;
+        const Tin* s1 = s0 + b.N;
         for (int j = threadIdx.x; j < n; j += FFT_THREADS) {
-            const double x0 = ok0 ? s0[j] : 0.0, x1 = ok1 ? s1[j] : 0.0;
-            const double2 z = make_double2(x0, x1);
+            const T x0 = ok0 ? (T)s0[j] : (T)0, x1 = ok1 ? (T)s1[j] : (T)0;
+            const V z = cmk<V>(x0, x1);
             if (F.type == 0) {           // m = j and P - j
                 a[j] = z;
                 if (j > 0 && j < L) a[P - j] = z;
             } else {                     // m = j + 1 and P - j - 1, negated
                 a[j + 1] = z;
-                a[P - j - 1] = make_double2(-z.x, -z.y);
+                a[P - j - 1] = cmk<V>(-z.x, -z.y);
             }
         }
     }
     if (F.type == 1 && threadIdx.x < 2 * FFT_PER_CTA)   // DST-I: zeros at m = 0 and m = L
-        A[(threadIdx.x >> 1) * PS + (threadIdx.x & 1) * L] = make_double2(0.0, 0.0);
+        A[(threadIdx.x >> 1) * PS + (threadIdx.x & 1) * L] = cmk<V>((T)0, (T)0);
     __syncthreads();                     // the staging area is free: start the next group
     if (g + (int)gridDim.x < b.ngroups) stage_group(b, g + gridDim.x, stg);
     int span = P;
@@ -309,12 +326,12 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
         span /= R;
         switch (R) {
 #if LC3D_FFT_MAX_RADIX >= 8
-            case 8: fft_pass<8>(A, span, P, b.tw); break;
+            case 8: fft_pass<8>(A, span, P, tw); break;
 #endif
-            case 4: fft_pass<4>(A, span, P, b.tw); break;
-            case 2: fft_pass<2>(A, span, P, b.tw); break;
-            case 3: fft_pass<3>(A, span, P, b.tw); break;
-            default: fft_pass<5>(A, span, P, b.tw); break;
+            case 4: fft_pass<4>(A, span, P, tw); break;
+            case 2: fft_pass<2>(A, span, P, tw); break;
+            case 3: fft_pass<3>(A, span, P, tw); break;
+            default: fft_pass<5>(A, span, P, tw); break;
         }
         __syncthreads();
     }
@@ -324,6 +341,8 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
     // one entry (one per FFT) write the CTA's consecutive rows of out[k]
     // (and read the same places of Lambda, when given).
     const int* rl = b.rd + (F.type ? b.N : 0);
+    const T* lam = static_cast<const T*>(F.lam);
+    Tout* out = static_cast<Tout*>(F.out);
     const int total = n * FFT_PER_CTA;
     double psum = 0.0;
     constexpr int SU = 8;
@@ -338,15 +357,15 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
         // held in registers at a time
 #pragma unroll
         for (int h = 0; h < SU; h += SU / 2) {
-            double la[SU / 2][2];
-            if (F.lam) {
+            T la[SU / 2][2];
+            if (lam) {
 #pragma unroll
                 for (int u = 0; u < SU / 2; ++u) {
                     const int t = t0 + (h + u) * FFT_THREADS + (int)threadIdx.x;
                     const int row = r0 + 2 * (t % FFT_PER_CTA);
-                    const double* lp = F.lam + (size_t)(e[h + u] & 0xffff) * F.ld_lam + row;
-                    la[u][0] = t < total && row < F.rows ? __ldg(lp) : 0.0;
-                    la[u][1] = t < total && row + 1 < F.rows ? __ldg(lp + 1) : 0.0;
+                    const T* lp = lam + (size_t)(e[h + u] & 0xffff) * F.ld_lam + row;
+                    la[u][0] = t < total && row < F.rows ? __ldg(lp) : (T)0;
+                    la[u][1] = t < total && row + 1 < F.rows ? __ldg(lp + 1) : (T)0;
                 }
             }
 #pragma unroll
@@ -354,25 +373,26 @@ __global__ void __launch_bounds__(FFT_THREADS, LC3D_FFT_MIN_BLOCKS) fft_rows_ker
                 const int t = t0 + (h + u) * FFT_THREADS + (int)threadIdx.x;
                 const int q = t % FFT_PER_CTA, row = r0 + 2 * q;
                 if (t >= total || row >= F.rows) continue;
-                const double2 z = A[q * PS + (e[h + u] >> 16)];
-                double* o = F.out + (size_t)(e[h + u] & 0xffff) * F.ld_out + row;
-                double x0 = F.type == 0 ? z.x : -z.y, x1 = F.type == 0 ? z.y : z.x;
-                if (F.lam) {
+                const V z = A[q * PS + (e[h + u] >> 16)];
+                Tout* o = out + (size_t)(e[h + u] & 0xffff) * F.ld_out + row;
+                T x0 = F.type == 0 ? z.x : -z.y, x1 = F.type == 0 ? z.y : z.x;
+                if (lam) {
                     x0 *= la[u][0];
                     x1 *= la[u][1];
                 }
-                o[0] = x0;
-                psum += x0;
+                const Tout y0 = (Tout)x0, y1 = (Tout)x1;
+                o[0] = y0;
+                psum += (double)y0;
                 if (row + 1 < F.rows) {
-                    o[1] = x1;
-                    psum += x1;
+                    o[1] = y1;
+                    psum += (double)y1;
                 }
             }
         }
     }
     if (F.partial) {   // uniform per CTA: fixed-order sum of everything this CTA wrote
         __syncthreads();   // the FFT buffer is free
-        double* red = reinterpret_cast<double*>(sm);
+        double* red = reinterpret_cast<double*>(fft_smem);
         double v = psum;
 #pragma unroll
         for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -416,16 +436,37 @@ int fft_plan(int P, int* rad) {
 int fft_cta_rows() { return ROWS_PER_CTA; }
 
 // Dynamic shared memory of fft_rows_kernel, the layout the kernel uses: the
-// FFT buffers at a pitch of P + FFT_PAD double2 words, then the staging rows
-// (ROWS_PER_CTA x N doubles).
-size_t fft_cta_smem_bytes(int P, int N) {
-    return (size_t)FFT_PER_CTA * (P + FFT_PAD) * sizeof(double2) + (size_t)ROWS_PER_CTA * N * sizeof(double);
+// FFT buffers at a pitch of P + FFT_PAD complex words, then the staging rows
+// (ROWS_PER_CTA x N input elements).
+size_t fft_cta_smem_bytes(int P, int N, int types) {
+    const size_t cx = types == FFT_F64 ? sizeof(double2) : sizeof(float2);
+    const size_t in = (types == FFT_F64 || types == FFT_F64_F32) ? sizeof(double) : sizeof(float);
+    return (size_t)FFT_PER_CTA * (P + FFT_PAD) * cx + (size_t)ROWS_PER_CTA * N * in;
+}
+
+// Layout of the twiddle buffer (in doubles): P double2 twiddles, the two
+// readout lists (2 N - 2 int32), then the P float2 twiddles.
+size_t fft_tw32_offset(int P, int N) { return 2 * (size_t)P + (size_t)(2 * N - 2 + 1) / 2; }
+
+template <typename T, typename Tin, typename Tout>
+int fft_launch(const FftBatch& b, cudaStream_t s) {
+    const int types = sizeof(T) == 8 ? FFT_F64 : sizeof(Tin) == 8 ? FFT_F64_F32 : sizeof(Tout) == 8 ? FFT_F32_F64 : FFT_F32;
+    const size_t smem = fft_cta_smem_bytes(b.P, b.N, types);
+    // persistent grid: as many CTAs as fit on the device at once
+    int dev = 0, sms = 0, per_sm = 0;
+    LC3D_CUDA_TRY(cudaGetDevice(&dev));
+    LC3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    LC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_rows_kernel<T, Tin, Tout>, FFT_THREADS, smem));
+    const int grid = std::max(1, std::min(b.ngroups, sms * std::max(per_sm, 1)));
+    fft_rows_kernel<T, Tin, Tout><<<grid, FFT_THREADS, smem, s>>>(b);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
 }
 
 int fft_init(lc3d_ctx* c) {
     const int N = c->N, P = 2 * (N - 1);
     int rad[MAX_RADICES];
-    c->fft_ok = fft_plan(P, rad) > 0 && fft_cta_smem_bytes(P, N) <= 200 * 1024;
+    c->fft_ok = fft_plan(P, rad) > 0 && fft_cta_smem_bytes(P, N, FFT_F64) <= 200 * 1024;
     if (!c->fft_ok) return LC3D_OK;
     LC3D_TRY(fft_prepare(P));
     const int nrad = fft_plan(P, rad);
@@ -454,10 +495,14 @@ int fft_init(lc3d_ctx* c) {
         std::sort(l.begin(), l.end());
         rd.insert(rd.end(), l.begin(), l.end());
     }
-    std::vector<double> buf(2 * (size_t)P + (rd.size() + 1) / 2);
+    const size_t o32 = fft_tw32_offset(P, N);
+    std::vector<double> buf(o32 + (size_t)P);
+    float* tw32 = reinterpret_cast<float*>(buf.data() + o32);
     for (int m = 0; m < P; ++m) {
         buf[2 * m] = sin_pi_frac(4LL * m + P, 2LL * P);      // cos(pi (2m) / P)
         buf[2 * m + 1] = -sin_pi_frac(2LL * m, (long long)P);
+        tw32[2 * m] = (float)buf[2 * m];
+        tw32[2 * m + 1] = (float)buf[2 * m + 1];
     }
     memcpy(buf.data() + 2 * (size_t)P, rd.data(), rd.size() * sizeof(int32_t));
     LC3D_CUDA_TRY(cudaMalloc(&c->fft_tw, buf.size() * sizeof(double)));
@@ -469,14 +514,19 @@ int fft_prepare(int P) {
     // the limit is per kernel, not per context: always the largest size any
     // context may use (contexts of different grid sizes coexist in batches)
     (void)P;
-    LC3D_CUDA_TRY(cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(fft_rows_kernel<double, double, double>, a, 200 * 1024));
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(fft_rows_kernel<float, double, float>, a, 200 * 1024));
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(fft_rows_kernel<float, float, float>, a, 200 * 1024));
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(fft_rows_kernel<float, float, double>, a, 200 * 1024));
     return LC3D_OK;
 }
 
 // One transform pass over up to 6 fields: desc[f] = {in, ld_in, rows, type,
 // out, ld_out, lam, ld_lam}; rows of `in` are transformed and written
-// transposed into `out`.
-int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, cudaStream_t s) {
+// transposed into `out`. `types` (FFT_*) gives the element types of the
+// rows read and written and of the arithmetic.
+int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, int types, cudaStream_t s) {
     FftBatch b;
     memset(&b, 0, sizeof(b));
     b.P = 2 * (c->N - 1);
@@ -484,6 +534,7 @@ int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, cudaStream_t s) {
     b.nrad = fft_plan(b.P, b.rad);
     b.tw = reinterpret_cast<const double2*>(c->fft_tw);
     b.rd = reinterpret_cast<const int*>(c->fft_tw + 2 * (size_t)b.P);
+    b.tw32 = reinterpret_cast<const float2*>(c->fft_tw + fft_tw32_offset(b.P, b.N));
     int ctas = 0;
     for (int q = 0; q < count; ++q) {
         FftField& f = b.f[b.count++];
@@ -495,15 +546,12 @@ int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, cudaStream_t s) {
     }
     if (!ctas) return LC3D_OK;
     b.ngroups = ctas;
-    const size_t smem = fft_cta_smem_bytes(b.P, b.N);
-    // persistent grid: as many CTAs as fit on the device at once
-    int dev = 0, sms = 0, per_sm = 0;
-    LC3D_CUDA_TRY(cudaGetDevice(&dev));
-    LC3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    LC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_rows_kernel, FFT_THREADS, smem));
-    const int grid = std::max(1, std::min(ctas, sms * std::max(per_sm, 1)));
     ProfScope ps(c, LC3D_STAGE_TRANSFORM, s);
-    fft_rows_kernel<<<grid, FFT_THREADS, smem, s>>>(b);
-    LC3D_CUDA_TRY(cudaGetLastError());
-    return LC3D_OK;
+    switch (types) {
+        case FFT_F64: return fft_launch<double, double, double>(b, s);
+        case FFT_F64_F32: return fft_launch<float, double, float>(b, s);
+        case FFT_F32: return fft_launch<float, float, float>(b, s);
+        case FFT_F32_F64: return fft_launch<float, float, double>(b, s);
+        default: return LC3D_ERR_PARAM;
+    }
 }

@@ -57,7 +57,8 @@ int check_params(const lc3d_params* p, int* Nc, int* Nf, double* rb) {
     if (!(p->grid_step_size > 0) || !(p->xi_step_size > 0)) return LC3D_ERR_PARAM;
     if (c < 1 || f < 1) return LC3D_ERR_PARAM;
     if (!(p->reflect_padding_steps > c + 1)) return LC3D_ERR_PARAM;       // lcode.py:944
-    if (p->precision != LC3D_PREC_FP64 && p->precision != LC3D_PREC_MIXED) return LC3D_ERR_PARAM;
+    if (p->precision != LC3D_PREC_FP64 && p->precision != LC3D_PREC_MIXED && p->precision != LC3D_PREC_FFT32)
+        return LC3D_ERR_PARAM;
     if (p->fp64_transform < LC3D_FP64_AUTO || p->fp64_transform > LC3D_FP64_DENSE) return LC3D_ERR_PARAM;
     if (p->mixed_slices < 0 || p->mixed_slices > 6) return LC3D_ERR_PARAM;
     if (p->precision == LC3D_PREC_MIXED && N > 1000) return LC3D_ERR_SIZE;
@@ -510,6 +511,7 @@ int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out) {
     LC3D_STEP(diag_init(c));
     if (rc == LC3D_OK) {
         if (p->fp64_transform == LC3D_FP64_FFT && !c->fft_ok) rc = LC3D_ERR_PARAM;
+        if (p->precision == LC3D_PREC_FFT32 && !c->fft_ok) rc = LC3D_ERR_PARAM;   // no dense float32 form
         c->use_fft = c->fft_ok && p->fp64_transform != LC3D_FP64_DENSE;
     }
     if (rc == LC3D_OK && p->precision == LC3D_PREC_MIXED)

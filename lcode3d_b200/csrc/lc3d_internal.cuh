@@ -126,18 +126,26 @@ int solve_fields(lc3d_ctx* ctx, int which, const SolveInputs& in,
 // FFT row transforms (fields_fft.cu): rows of `in` (length N for DCT-I,
 // N - 2 for DST-I) are transformed and written transposed, out[k][r],
 // optionally multiplied element-wise by lam[k][r] as they are written.
+// Element types of a pass: the rows read, the arithmetic (and Lambda), the
+// rows written.
+enum FftTypes {
+    FFT_F64 = 0,       // double -> double arithmetic -> double
+    FFT_F64_F32 = 1,   // double -> float -> float
+    FFT_F32 = 2,       // float -> float -> float
+    FFT_F32_F64 = 3,   // float -> float -> double
+};
 struct FftRowsDesc {
-    const double* in;
+    const void* in;
     int ld_in, rows, type;                // type: 0 DCT-I, 1 DST-I
-    double* out;
+    void* out;
     int ld_out;
-    const double* lam;
+    const void* lam;                      // in the arithmetic's type
     int ld_lam;
     double* partial;                      // optional: per-CTA sums of the written values
 };
 int fft_init(lc3d_ctx* ctx);
 int fft_cta_rows();                       // rows per CTA: partial sums per field = ceil(rows / this)
-int fft_rows(lc3d_ctx* ctx, const FftRowsDesc* desc, int count, cudaStream_t s);
+int fft_rows(lc3d_ctx* ctx, const FftRowsDesc* desc, int count, int types, cudaStream_t s);
 int fft_plan(int P, int* rad);
 
 // Mixed-precision transform stages (fields_mixed.cu): C = A B^T with one
@@ -200,6 +208,7 @@ struct lc3d_ctx {
     // field-solver workspaces (fields.cu)
     double *S2, *C, *CT;                  // 2*DST-I (M x M), DCT-I (N x N), its transpose
     double *lam_dir, *lam_mix, *lam_mixT, *lam_neu;
+    float *lam32_dir, *lam32_mix, *lam32_mixT, *lam32_neu;   // float32-transform precision only
     double* rhs[6];                       // right-hand sides, N x N planes
     double* t1[6];                        // transform scratch
     double* t2[6];

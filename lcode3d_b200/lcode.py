@@ -15,7 +15,9 @@ attribute access like the reference's. All device work runs in liblc3d.so
 (include/lc3d.h) on the current torch stream; there is no CPU fallback.
 
 Extra, optional config attributes (absent in the reference's config):
-``lc3d_precision`` = 'fp64' (default) or 'mixed';
+``lc3d_precision`` = 'fp64' (default), 'mixed' (split-bf16 tensor-core
+transforms) or 'fft32' (float32 FFT transforms; right-hand sides, fields,
+averaging and particles in float64);
 ``lc3d_fp64_transform`` = 'auto' (default: FFT where 2(N-1) factors into
 2, 3, 5), 'fft' or 'dense' (DGEMM-form transform matrices);
 ``lc3d_mixed_slices`` = bf16 slices per operand of the mixed-precision
@@ -104,7 +106,9 @@ def _precision(config):
         return _lib.PREC_FP64
     if p in ('mixed', _lib.PREC_MIXED):
         return _lib.PREC_MIXED
-    raise ValueError(f'lc3d_precision must be "fp64" or "mixed", not {p!r}')
+    if p in ('fft32', _lib.PREC_FFT32):
+        return _lib.PREC_FFT32
+    raise ValueError(f'lc3d_precision must be "fp64", "mixed" or "fft32", not {p!r}')
 
 
 def _fp64_transform(config):
