@@ -51,8 +51,11 @@ static_assert(FFT_THREADS % 32 == 0 && FFT_THREADS <= 1024, "whole warps");
 #ifndef LC3D_FFT_MIN_BLOCKS
 #define LC3D_FFT_MIN_BLOCKS 3             // resident CTAs per SM the registers allow (float64)
 #endif
+#ifndef LC3D_FFT32_SU
+#define LC3D_FFT32_SU 8                   // readout entries per thread and round (float32 transforms)
+#endif
 #ifndef LC3D_FFT32_MIN_BLOCKS
-#define LC3D_FFT32_MIN_BLOCKS 4           // ... (float32 transforms)
+#define LC3D_FFT32_MIN_BLOCKS 5           // ... (float32 transforms)
 #endif
 constexpr int MAX_RADICES = 24;
 constexpr int FFT_PAD = 4;               // complex words between the CTA's two FFTs (bank offset)
@@ -345,7 +348,7 @@ __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_ker
     Tout* out = static_cast<Tout*>(F.out);
     const int total = n * FFT_PER_CTA;
     double psum = 0.0;
-    constexpr int SU = 8;
+    constexpr int SU = sizeof(T) == 8 ? 8 : LC3D_FFT32_SU;   // readout entries in flight per thread
     for (int t0 = 0; t0 < total; t0 += SU * FFT_THREADS) {
         int e[SU];
 #pragma unroll
