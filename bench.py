@@ -18,6 +18,8 @@ deposit: 3 pushes, 3 depositions, 2 field solves of 6 fields).
 value: device-resident inputs (beam arrays already in HBM), context-owned
 state, each step timed with CUDA events on the launching stream; L2 is
 flushed (a 256 MiB write) between timed steps, outside the timed events.
+stages_ms_per_step and the roofline's kernel time come from K further steps
+with every kernel launch bracketed by CUDA events (kept out of `value`).
 e2e: the same metric through the public drop-in API (lcode3d_b200.step) with
 the beam copied host->device from pinned memory and Ez(0,0) read back
 device->host every step, like the reference's CLI loop.
@@ -240,14 +242,14 @@ def run_ours(args, rank, world, dist):
     ptrs = _lib.StatePtrs(*[getattr(st, n).data_ptr() for n in names])
     _lib.check(lib.lc3d_set_state(s.ctx, ctypes.byref(ptrs), sp), 'set_state')
     K, W = args.steps, args.warmup
-    beams = [torch.from_numpy(beam_np(cfg, x0 + i, xs, ys)).cuda() for i in range(W + K)]
+    beams = [torch.from_numpy(beam_np(cfg, x0 + i, xs, ys)).cuda() for i in range(W + 2 * K)]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
     for i in range(W):
         _lib.check(lib.lc3d_step(s.ctx, ctypes.c_void_p(beams[i].data_ptr()), sp), 'step')
     torch.cuda.synchronize()
     _lib.check(lib.lc3d_check_error(s.ctx, sp), 'warmup')
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-    _lib.check(lib.lc3d_profile(s.ctx, 1), 'profile')
+    _lib.check(lib.lc3d_profile(s.ctx, 0), 'profile reset')   # count launches, no per-launch events
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -265,18 +267,27 @@ def run_ours(args, rank, world, dist):
     ms_steps = [a.elapsed_time(b) for a, b in ev]
     nst = len(_lib.STAGES)
     launches = (ctypes.c_longlong * nst)()
+    lib.lc3d_profile_read(s.ctx, launches, None, None)
+    _lib.check(lib.lc3d_check_error(s.ctx, sp), 'timed steps')
+
+    # ---- stage breakdown: K further steps, every launch bracketed by CUDA events ----
+    _lib.check(lib.lc3d_profile(s.ctx, 1), 'profile')
+    for i in range(K):
+        flush.fill_(float(i))
+        _lib.check(lib.lc3d_step(s.ctx, ctypes.c_void_p(beams[W + K + i].data_ptr()), sp), 'step')
+    plaunches = (ctypes.c_longlong * nst)()
     kms = (ctypes.c_double * nst)()
     timed = (ctypes.c_longlong * nst)()
-    rc = lib.lc3d_profile_read(s.ctx, launches, kms, timed)
+    lib.lc3d_profile_read(s.ctx, plaunches, kms, timed)
     lib.lc3d_profile(s.ctx, 0)
-    _lib.check(lib.lc3d_check_error(s.ctx, sp), 'timed steps')
+    _lib.check(lib.lc3d_check_error(s.ctx, sp), 'profiled steps')
     total_ms = sum(ms_steps)
     if dist:
         t = torch.tensor([total_ms], dtype=torch.float64, device='cuda')
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t)
     value = world * K / (total_ms * 1e-3)
-    stage = {n: {'launches': int(launches[k]), 'ms': kms[k], 'timed': int(timed[k])}
+    stage = {n: {'launches': int(plaunches[k]), 'ms': kms[k], 'timed': int(timed[k])}
              for k, n in enumerate(_lib.STAGES)}
 
     # ---- e2e through the public API, host beam in pinned memory ----
@@ -310,7 +321,7 @@ def run_ours(args, rank, world, dist):
     bp = _lib.BeamParams(GRIDS[args.grid][2], 1.0, 1.0)
     _lib.check(lib.lc3d_set_beam(s.ctx, ctypes.byref(bp)), 'set_beam')
     ezh = torch.empty(W + K, dtype=torch.float64, device='cuda')
-    xg = x0 + W + K   # the context state has advanced by W + K steps
+    xg = x0 + W + 2 * K   # the context state has advanced by W + 2K steps
     _lib.check(lib.lc3d_run(s.ctx, xg, W, ctypes.c_void_p(ezh.data_ptr()), sp), 'graph warmup')
     torch.cuda.synchronize()
     if dist:

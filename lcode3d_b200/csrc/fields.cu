@@ -51,6 +51,7 @@ __device__ __forceinline__ double div_by(double x, double d, double inv_d) {
 }
 
 __global__ void __launch_bounds__(256) rhs_kernel(const __grid_constant__ RhsArgs a) {
+    pdl_wait();
     const int N = a.N;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= N * N) return;
@@ -220,6 +221,7 @@ __device__ __forceinline__ double block_sum_fixed(double v, double* sh) {
 
 __global__ void __launch_bounds__(RED_THREADS) partial_sum_kernel(const double* __restrict__ a, int n,
                                                                   double* __restrict__ partial) {
+    pdl_wait();
     __shared__ double sh[RED_THREADS];
     double v = 0;
     for (int k = blockIdx.x * RED_THREADS + threadIdx.x; k < n; k += gridDim.x * RED_THREADS) v += a[k];
@@ -244,6 +246,7 @@ struct FinalizeArgs {
 };
 
 __global__ void __launch_bounds__(RED_THREADS) finalize_step_kernel(const __grid_constant__ FinalizeArgs a) {
+    pdl_wait();
     __shared__ double sh[RED_THREADS];
     const double mean = a.has_bz ? mean_from_partials(a.partial, a.nblocks, a.inv_n, sh) : 0.0;
     const int k = blockIdx.x * RED_THREADS + threadIdx.x;
@@ -261,6 +264,7 @@ __global__ void __launch_bounds__(RED_THREADS) finalize_step_kernel(const __grid
 
 __global__ void __launch_bounds__(RED_THREADS) subtract_mean_kernel(double* a, int n, const double* partial,
                                                                     int nblocks, double inv_n) {
+    pdl_wait();
     __shared__ double sh[RED_THREADS];
     const double mean = mean_from_partials(partial, nblocks, inv_n, sh);
     const int k = blockIdx.x * RED_THREADS + threadIdx.x;
@@ -445,7 +449,7 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
     for (int f = 0; f < 6; ++f) ra.out[f] = on[f] ? c->rhs[f] : nullptr;
     {
         ProfScope ps(c, LC3D_STAGE_RHS, s);
-        rhs_kernel<<<(n + 255) / 256, 256, 0, s>>>(ra);
+        LC3D_CUDA_TRY(launch_pdl(rhs_kernel, dim3((n + 255) / 256), dim3(256), 0, s, ra));
         LC3D_CUDA_TRY(cudaGetLastError());
     }
 
@@ -576,15 +580,17 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
     const double inv_n = 1.0 / n;
     if (on[5] && !bz_partials) {
         ProfScope ps(c, LC3D_STAGE_FIELD_FIN, s);
-        partial_sum_kernel<<<c->red_blocks, RED_THREADS, 0, s>>>(dst[5], n, c->red);
+        LC3D_CUDA_TRY(launch_pdl(partial_sum_kernel, dim3(c->red_blocks), dim3(RED_THREADS), 0, s,
+                                 static_cast<const double*>(dst[5]), n, c->red));
         LC3D_CUDA_TRY(cudaGetLastError());
     }
     const int nred = bz_partials ? bz_partials : c->red_blocks;
     if (o.mode == 0) {
         if (on[5]) {
             ProfScope ps(c, LC3D_STAGE_FIELD_FIN, s);
-            subtract_mean_kernel<<<(n + RED_THREADS - 1) / RED_THREADS, RED_THREADS, 0, s>>>(
-                dst[5], n, c->red, nred, inv_n);
+            LC3D_CUDA_TRY(launch_pdl(subtract_mean_kernel, dim3((n + RED_THREADS - 1) / RED_THREADS),
+                                     dim3(RED_THREADS), 0, s, dst[5], n, static_cast<const double*>(c->red),
+                                     nred, inv_n));
             LC3D_CUDA_TRY(cudaGetLastError());
         }
         return LC3D_OK;
@@ -605,7 +611,8 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
     fa.has_bz = on[5];
     fa.inv_n = inv_n;
     ProfScope ps(c, LC3D_STAGE_FIELD_FIN, s);
-    finalize_step_kernel<<<(n + RED_THREADS - 1) / RED_THREADS, RED_THREADS, 0, s>>>(fa);
+    LC3D_CUDA_TRY(launch_pdl(finalize_step_kernel, dim3((n + RED_THREADS - 1) / RED_THREADS), dim3(RED_THREADS), 0,
+                             s, fa));
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }

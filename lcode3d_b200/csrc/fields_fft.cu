@@ -288,6 +288,7 @@ __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_ker
     Tin* stg = reinterpret_cast<Tin*>(A + FFT_PER_CTA * PS);   // [ROWS_PER_CTA][N]
     const V* tw = reinterpret_cast<const V*>(sizeof(T) == 8 ? static_cast<const void*>(b.tw)
                                                             : static_cast<const void*>(b.tw32));
+    pdl_wait();
     int g = blockIdx.x;
     if (g < b.ngroups) stage_group(b, g, stg);
 #pragma unroll 1
@@ -461,7 +462,7 @@ int fft_launch(const FftBatch& b, cudaStream_t s) {
     LC3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     LC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_rows_kernel<T, Tin, Tout>, FFT_THREADS, smem));
     const int grid = std::max(1, std::min(b.ngroups, sms * std::max(per_sm, 1)));
-    fft_rows_kernel<T, Tin, Tout><<<grid, FFT_THREADS, smem, s>>>(b);
+    LC3D_CUDA_TRY(launch_pdl(fft_rows_kernel<T, Tin, Tout>, dim3(grid), dim3(FFT_THREADS), smem, s, b));
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }

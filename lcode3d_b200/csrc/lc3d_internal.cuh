@@ -30,6 +30,38 @@
 void lc3d_set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line);
 
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch of the xi-step kernels. They are launched
+// with programmatic stream serialization: the launch of a kernel is
+// processed while its predecessor in the stream is still running, and its
+// CTAs start as soon as the predecessor has exited. Every such kernel calls
+// pdl_wait() before its first global-memory access, read or write: the wait
+// returns once the preceding grid has completed and its writes are visible,
+// so stream order holds for all data, and transitively, since every kernel
+// in the chain waits. No kernel triggers its successor early
+// (griddepcontrol.launch_dependents): resident, waiting successor CTAs
+// measured slower. pdl_wait() is a no-op for a kernel launched without the
+// attribute. Step loops launched from the host gain 4-7 % from this; CUDA
+// graph replays are unchanged.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args&&>(args)...);
+}
+
+// ---------------------------------------------------------------------------
 // Particle kernels (particles.cu)
 // ---------------------------------------------------------------------------
 

@@ -105,6 +105,7 @@ __device__ __forceinline__ void estimate_one(double m, double xi0, double yi0, d
 }
 
 __global__ void __launch_bounds__(256) move_estimate_kernel(EstimateArgs a) {
+    pdl_wait();
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.n) return;
     double ex, ey;
@@ -120,6 +121,7 @@ __global__ void __launch_bounds__(256) move_estimate_kernel(EstimateArgs a) {
 // predictor pass of step()).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) move_smart_kernel(MoveArgs a) {
+    pdl_wait();
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.n) return;
     const double m = a.m[k], q = a.q[k];
@@ -307,6 +309,7 @@ __global__ void __launch_bounds__(DEP_THREADS, 1024 / DEP_THREADS) deposit_kerne
     }
     for (int w = t; w < 4 * DEP_WIN; w += DEP_THREADS) fwin[w] = 0.0;
     for (int w = t; w < DEP_WIN; w += DEP_THREADS) s_claim[w] = -1;
+    pdl_wait();   // global memory from here on
 
     // ---- phase 1: one fine particle per thread ----
     {
@@ -332,15 +335,11 @@ __global__ void __launch_bounds__(DEP_THREADS, 1024 / DEP_THREADS) deposit_kerne
             s_v[3 * DEP_THREADS + t] = f.djz;
         }
         s_cell[t] = cell;
-        int imin = cell >= 0 ? i : 1 << 30, imax = cell >= 0 ? i : -(1 << 30);
-        int jmin = cell >= 0 ? j : 1 << 30, jmax = cell >= 0 ? j : -(1 << 30);
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            imin = min(imin, __shfl_xor_sync(0xffffffffu, imin, o));
-            imax = max(imax, __shfl_xor_sync(0xffffffffu, imax, o));
-            jmin = min(jmin, __shfl_xor_sync(0xffffffffu, jmin, o));
-            jmax = max(jmax, __shfl_xor_sync(0xffffffffu, jmax, o));
-        }
+        // warp bounding box of the cells (one redux instruction each)
+        const int imin = __reduce_min_sync(0xffffffffu, cell >= 0 ? i : 1 << 30);
+        const int imax = __reduce_max_sync(0xffffffffu, cell >= 0 ? i : -(1 << 30));
+        const int jmin = __reduce_min_sync(0xffffffffu, cell >= 0 ? j : 1 << 30);
+        const int jmax = __reduce_max_sync(0xffffffffu, cell >= 0 ? j : -(1 << 30));
         __syncthreads();   // s_bb initialised, window and claims cleared
         if ((t & 31) == 0 && imin <= imax) {
             atomicMin(&s_bb[0], imin);
@@ -453,6 +452,7 @@ __global__ void __launch_bounds__(DEP_THREADS, 1024 / DEP_THREADS) deposit_kerne
 // could alias later loads for the compiler otherwise, serialising them);
 // the float64 side uses 16-byte accesses when every array allows it.
 __global__ void __launch_bounds__(256) deposit_finalize_kernel(DepositFinalizeArgs f) {
+    pdl_wait();
     const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     if (k >= f.n) return;
     const size_t P = f.plane;
@@ -514,14 +514,14 @@ __global__ void __launch_bounds__(256) deposit_finalize_kernel(DepositFinalizeAr
 
 int launch_move_estimate(const EstimateArgs& a, cudaStream_t s) {
     if (a.n <= 0) return LC3D_OK;
-    move_estimate_kernel<<<(a.n + 255) / 256, 256, 0, s>>>(a);
+    LC3D_CUDA_TRY(launch_pdl(move_estimate_kernel, dim3((a.n + 255) / 256), dim3(256), 0, s, a));
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
 
 int launch_move_smart(const MoveArgs& a, cudaStream_t s) {
     if (a.n <= 0) return LC3D_OK;
-    move_smart_kernel<<<(a.n + 255) / 256, 256, 0, s>>>(a);
+    LC3D_CUDA_TRY(launch_pdl(move_smart_kernel, dim3((a.n + 255) / 256), dim3(256), 0, s, a));
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
@@ -534,7 +534,7 @@ int particles_prepare() {
 int launch_deposit_main(const DepositArgs& a, cudaStream_t s) {
     if (a.Nf <= 0) return LC3D_OK;
     dim3 grid((a.Nf + DEP_TJ - 1) / DEP_TJ, (a.Nf + DEP_TI - 1) / DEP_TI);
-    deposit_kernel<<<grid, DEP_THREADS, DEP_SMEM, s>>>(a);
+    LC3D_CUDA_TRY(launch_pdl(deposit_kernel, grid, dim3(DEP_THREADS), DEP_SMEM, s, a));
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
@@ -545,7 +545,7 @@ int launch_deposit_finalize(const DepositFinalizeArgs& f_in, cudaStream_t s) {
                          reinterpret_cast<uintptr_t>(f.jy) | reinterpret_cast<uintptr_t>(f.jz) |
                          reinterpret_cast<uintptr_t>(f.ro_initial);
     f.vec = (al & 15) == 0;
-    deposit_finalize_kernel<<<((f.n + 1) / 2 + 255) / 256, 256, 0, s>>>(f);
+    LC3D_CUDA_TRY(launch_pdl(deposit_finalize_kernel, dim3(((f.n + 1) / 2 + 255) / 256), dim3(256), 0, s, f));
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }

@@ -36,6 +36,7 @@ __device__ __forceinline__ double beam_value(int k, int N, double h, double xi, 
 
 __global__ void __launch_bounds__(256) beam_kernel(double* out, int N, double h, double dxi, double A, double sr,
                                                    double lf, const RunCtl* ctl) {
+    pdl_wait();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= N * N) return;
     out[k] = beam_value(k, N, h, ctl->xi * dxi, A, sr, lf);
@@ -49,6 +50,7 @@ __global__ void __launch_bounds__(256) beam_at_kernel(double* out, int N, double
 }
 
 __global__ void record_kernel(const double* Ez, int center, RunCtl* ctl) {
+    pdl_wait();
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         if (ctl->ez) ctl->ez[ctl->xi - ctl->xi0] = Ez[center];
         ctl->xi += 1;
@@ -77,14 +79,15 @@ int enqueue_step(lc3d_ctx* c, int par, cudaStream_t s) {
     const int N = c->N;
     {
         ProfScope ps(c, LC3D_STAGE_OTHER, s);
-        beam_kernel<<<(N * N + 255) / 256, 256, 0, s>>>(c->beam_buf, N, c->p.grid_step_size, c->p.xi_step_size,
-                                                         c->beam_A, c->beam_sr, c->beam_lf,
-                                                         static_cast<const RunCtl*>(c->run_ctl));
+        LC3D_CUDA_TRY(launch_pdl(beam_kernel, dim3((N * N + 255) / 256), dim3(256), 0, s, c->beam_buf, N,
+                                 c->p.grid_step_size, c->p.xi_step_size, c->beam_A, c->beam_sr, c->beam_lf,
+                                 static_cast<const RunCtl*>(c->run_ctl)));
         LC3D_CUDA_TRY(cudaGetLastError());
     }
     LC3D_TRY(step_schedule(c, c->st[par], c->st[par ^ 1], c->beam_buf, s));
     ProfScope ps(c, LC3D_STAGE_OTHER, s);
-    record_kernel<<<1, 32, 0, s>>>(c->st[par ^ 1].Ez, (N / 2) * N + N / 2, static_cast<RunCtl*>(c->run_ctl));
+    LC3D_CUDA_TRY(launch_pdl(record_kernel, dim3(1), dim3(32), 0, s, static_cast<const double*>(c->st[par ^ 1].Ez),
+                             (N / 2) * N + N / 2, static_cast<RunCtl*>(c->run_ctl)));
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
