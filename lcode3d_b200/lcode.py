@@ -200,16 +200,33 @@ class Solver:
 
 
 _solvers = {}
+_solvers_raw = {}   # (raw config attribute values, device) -> Solver: skips params_of per call
+_CFG_ATTRS = ('grid_steps', 'grid_step_size', 'xi_step_size', 'plasma_coarseness', 'plasma_fineness',
+              'reflect_padding_steps', 'plasma_padding_steps', 'field_solver_subtraction_trick',
+              'field_solver_variant_A')
+_CFG_OPTIONAL = (('lc3d_precision', 'fp64'), ('lc3d_fp64_transform', 'auto'), ('lc3d_mixed_slices', 0))
 
 
 def solver_for(config):
     """The cached Solver of this configuration on the current device."""
+    raw = None
+    if torch.cuda.is_available():
+        raw = (tuple(getattr(config, n, None) for n in _CFG_ATTRS) +
+               tuple(getattr(config, n, d) for n, d in _CFG_OPTIONAL) + (torch.cuda.current_device(),))
+        try:
+            s = _solvers_raw.get(raw)
+        except TypeError:   # an unhashable attribute value: take the full path
+            raw, s = None, None
+        if s is not None:
+            return s
     p = params_of(config)
     dev = _device().index
     k = _key(p, dev)
     s = _solvers.get(k)
     if s is None:
         s = _solvers[k] = Solver(p, dev)
+    if raw is not None:
+        _solvers_raw[raw] = s
     return s
 
 
@@ -231,6 +248,32 @@ def _f64(a, shape=None):
     if shape is not None and tuple(t.shape) != tuple(shape):
         t = t.expand(shape).contiguous()
     return t
+
+
+def _state_arrays(state, shape_p, g, dev):
+    """The 15 state arrays of ``state`` as contiguous float64 tensors on
+    ``dev``; arrays that already are (the usual case: the previous step's
+    output) are used as they are, without a conversion call."""
+    out = []
+    for k, n in enumerate(_lib.STATE_NAMES):
+        t = getattr(state, n)
+        shape = shape_p if k < 5 else g
+        if not (isinstance(t, torch.Tensor) and t.dtype == torch.float64 and t.device == dev and
+                t.is_contiguous() and tuple(t.shape) == shape):
+            t = _f64(t, shape)
+        out.append(t)
+    return out
+
+
+def _new_state_arrays(shape_p, g, dev):
+    """Uninitialised output arrays of one step: views of ONE allocation (one
+    allocator call instead of 15), each starting on a 256-byte boundary.
+    The allocation lives while any of its arrays does."""
+    n_p, n_g = shape_p[0] * shape_p[1], g[0] * g[1]
+    pad = lambda n: (n + 31) // 32 * 32   # float64 words to a 256-byte multiple
+    sizes = [pad(n_p)] * 5 + [pad(n_g)] * 10
+    parts = torch.empty(sum(sizes), dtype=torch.float64, device=dev).split(sizes)
+    return [p[:n_p].view(shape_p) if k < 5 else p[:n_g].view(g) for k, p in enumerate(parts)]
 
 
 # ---------------------------------------------------------------------------
@@ -423,10 +466,12 @@ def step(config, const, virt_params, prev, beam_ro):
     beam = None if hb is not None else _beam(config, beam_ro)
     shape_p = tuple(prev.x_offt.shape)
     g = _grid(config)
-    prev_t = [_f64(getattr(prev, n), shape_p if k < 5 else g) for k, n in enumerate(_lib.STATE_NAMES)]
-    out = {n: _empty(shape_p if k < 5 else g) for k, n in enumerate(_lib.STATE_NAMES)}
+    dev = _device()
+    prev_t = _state_arrays(prev, shape_p, g, dev)
+    out_t = _new_state_arrays(shape_p, g, dev)
+    out = dict(zip(_lib.STATE_NAMES, out_t))
     sp = _lib.StatePtrs(*[t.data_ptr() for t in prev_t])
-    so = _lib.StatePtrs(*[out[n].data_ptr() for n in _lib.STATE_NAMES])
+    so = _lib.StatePtrs(*[t.data_ptr() for t in out_t])
     if hb is not None:
         check(lib.lc3d_step_arrays_host_beam(s.ctx, ctypes.byref(sp), ctypes.byref(so),
                                              ctypes.c_void_p(hb.data_ptr()), _stream()), 'step')
