@@ -453,15 +453,27 @@ size_t fft_cta_smem_bytes(int P, int N, int types) {
 size_t fft_tw32_offset(int P, int N) { return 2 * (size_t)P + (size_t)(2 * N - 2 + 1) / 2; }
 
 template <typename T, typename Tin, typename Tout>
-int fft_launch(const FftBatch& b, cudaStream_t s) {
-    const int types = sizeof(T) == 8 ? FFT_F64 : sizeof(Tin) == 8 ? FFT_F64_F32 : sizeof(Tout) == 8 ? FFT_F32_F64 : FFT_F32;
-    const size_t smem = fft_cta_smem_bytes(b.P, b.N, types);
-    // persistent grid: as many CTAs as fit on the device at once
+constexpr int fft_types() {
+    return sizeof(T) == 8 ? FFT_F64 : sizeof(Tin) == 8 ? FFT_F64_F32 : sizeof(Tout) == 8 ? FFT_F32_F64 : FFT_F32;
+}
+
+// Persistent grid of an instantiation: as many CTAs as fit on the device at
+// once (queried once per context, at set-up).
+template <typename T, typename Tin, typename Tout>
+int fft_grid_size(int P, int N, int* grid) {
     int dev = 0, sms = 0, per_sm = 0;
     LC3D_CUDA_TRY(cudaGetDevice(&dev));
     LC3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    LC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_rows_kernel<T, Tin, Tout>, FFT_THREADS, smem));
-    const int grid = std::max(1, std::min(b.ngroups, sms * std::max(per_sm, 1)));
+    LC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_rows_kernel<T, Tin, Tout>, FFT_THREADS,
+                                                                fft_cta_smem_bytes(P, N, fft_types<T, Tin, Tout>())));
+    *grid = std::max(1, sms * std::max(per_sm, 1));
+    return LC3D_OK;
+}
+
+template <typename T, typename Tin, typename Tout>
+int fft_launch(const FftBatch& b, int G, cudaStream_t s) {
+    const size_t smem = fft_cta_smem_bytes(b.P, b.N, fft_types<T, Tin, Tout>());
+    const int grid = std::max(1, std::min(b.ngroups, G));
     LC3D_CUDA_TRY(launch_pdl(fft_rows_kernel<T, Tin, Tout>, dim3(grid), dim3(FFT_THREADS), smem, s, b));
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
@@ -473,6 +485,10 @@ int fft_init(lc3d_ctx* c) {
     c->fft_ok = fft_plan(P, rad) > 0 && fft_cta_smem_bytes(P, N, FFT_F64) <= 200 * 1024;
     if (!c->fft_ok) return LC3D_OK;
     LC3D_TRY(fft_prepare(P));
+    LC3D_TRY((fft_grid_size<double, double, double>(P, N, &c->fft_grid[FFT_F64])));
+    LC3D_TRY((fft_grid_size<float, double, float>(P, N, &c->fft_grid[FFT_F64_F32])));
+    LC3D_TRY((fft_grid_size<float, float, float>(P, N, &c->fft_grid[FFT_F32])));
+    LC3D_TRY((fft_grid_size<float, float, double>(P, N, &c->fft_grid[FFT_F32_F64])));
     const int nrad = fft_plan(P, rad);
     // P twiddles exp(-2 pi i m / P), then the two readout lists. Frequency k
     // of the in-place DIF output sits at pos(k) = sum_s m_s P / (R0..Rs) for
@@ -552,10 +568,10 @@ int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, int types, cudaStr
     b.ngroups = ctas;
     ProfScope ps(c, LC3D_STAGE_TRANSFORM, s);
     switch (types) {
-        case FFT_F64: return fft_launch<double, double, double>(b, s);
-        case FFT_F64_F32: return fft_launch<float, double, float>(b, s);
-        case FFT_F32: return fft_launch<float, float, float>(b, s);
-        case FFT_F32_F64: return fft_launch<float, float, double>(b, s);
+        case FFT_F64: return fft_launch<double, double, double>(b, c->fft_grid[FFT_F64], s);
+        case FFT_F64_F32: return fft_launch<float, double, float>(b, c->fft_grid[FFT_F64_F32], s);
+        case FFT_F32: return fft_launch<float, float, float>(b, c->fft_grid[FFT_F32], s);
+        case FFT_F32_F64: return fft_launch<float, float, double>(b, c->fft_grid[FFT_F32_F64], s);
         default: return LC3D_ERR_PARAM;
     }
 }

@@ -249,6 +249,7 @@ struct lc3d_ctx {
     int red_blocks;
     int fft_ok, use_fft;                  // FFT transforms available / selected
     double* fft_tw;                       // FFT twiddles, P complex
+    int fft_grid[4];                      // persistent FFT grid per FftTypes instantiation
     void* mixed;                          // mixed-precision solver state (fields_mixed.cu)
     // launch accounting / profiling
     long long launches[LC3D_NSTAGES];

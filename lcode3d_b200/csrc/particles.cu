@@ -218,7 +218,10 @@ constexpr int DEP_TI = LC3D_DEP_ROWS;     // ... along i (16: two CTAs share an 
 constexpr int DEP_THREADS = DEP_TI * DEP_TJ; // phase 1: one fine particle per thread
 constexpr int DEP_BLOCKS = DEP_THREADS / 4;  // phase 2: 2 x 2 blocks of the patch
 static_assert(DEP_TI % 2 == 0 && DEP_THREADS % 4 == 0, "the patch is tiled by 2 x 2 blocks");
-constexpr int DEP_W = 32;                 // shared window side (cells)
+#ifndef LC3D_DEP_W
+#define LC3D_DEP_W 32
+#endif
+constexpr int DEP_W = LC3D_DEP_W;         // shared window side (cells)
 constexpr int DEP_WIN = DEP_W * DEP_W;
 // shared memory: float64 window (4 fields), anchor claims, per-particle
 // staging (cell, xl, yl, 4 values)
