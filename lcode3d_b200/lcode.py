@@ -162,6 +162,7 @@ class Solver:
         check(lib.lc3d_sizes(ctypes.byref(params), ctypes.byref(nc), ctypes.byref(nf),
                              ctypes.byref(rb)), 'lc3d_sizes')
         self.N, self.Nc, self.Nf, self.reflect_boundary = params.grid_steps, nc.value, nf.value, rb.value
+        self.out_pool = _StatePool()
         self._const_key = None
         self._virt_key = None
         self._keep = ()
@@ -263,6 +264,42 @@ def _state_arrays(state, shape_p, g, dev):
             t = _f64(t, shape)
         out.append(t)
     return out
+
+
+class _StatePool:
+    """Output states of ``step`` kept for reuse (per Solver). An entry (a
+    GPUArrays, its 15 arrays and their StatePtrs) is handed out again only
+    when nothing outside the pool refers to the object or to any of its
+    arrays: their CPython reference counts are back at the values taken
+    when the entry was made. That is the state before last in the
+    reference's loop (``state = step(..., state, ...)``), which the caller
+    has dropped. A reused state is the same Python object, with the new
+    step's values; states the caller keeps are never touched. Saves the
+    allocation and the 15 array objects of a step."""
+
+    SIZE = 3
+
+    def __init__(self):
+        self.entries = []
+
+    @staticmethod
+    def _counts(e):
+        return [sys.getrefcount(e[0])] + [sys.getrefcount(t) for t in e[1]]
+
+    def take(self, shape_p, g, dev):
+        for e in self.entries:
+            if e[4] == (shape_p, g, dev) and self._counts(e) == e[3]:
+                return e
+        arrays = tuple(_new_state_arrays(shape_p, g, dev))
+        obj = GPUArrays.__new__(GPUArrays)
+        for n, t in zip(_lib.STATE_NAMES, arrays):
+            setattr(obj, n, t)
+        e = [obj, arrays, _lib.StatePtrs(*[t.data_ptr() for t in arrays]), None, (shape_p, g, dev)]
+        del obj, arrays, n, t
+        if len(self.entries) < self.SIZE:
+            self.entries.append(e)
+            e[3] = self._counts(e)
+        return e
 
 
 def _new_state_arrays(shape_p, g, dev):
@@ -468,10 +505,9 @@ def step(config, const, virt_params, prev, beam_ro):
     g = _grid(config)
     dev = _device()
     prev_t = _state_arrays(prev, shape_p, g, dev)
-    out_t = _new_state_arrays(shape_p, g, dev)
-    out = dict(zip(_lib.STATE_NAMES, out_t))
+    e = s.out_pool.take(shape_p, g, dev)
     sp = _lib.StatePtrs(*[t.data_ptr() for t in prev_t])
-    so = _lib.StatePtrs(*[t.data_ptr() for t in out_t])
+    so = e[2]
     if hb is not None:
         check(lib.lc3d_step_arrays_host_beam(s.ctx, ctypes.byref(sp), ctypes.byref(so),
                                              ctypes.c_void_p(hb.data_ptr()), _stream()), 'step')
@@ -480,10 +516,7 @@ def step(config, const, virt_params, prev, beam_ro):
         check(lib.lc3d_step_arrays(s.ctx, ctypes.byref(sp), ctypes.byref(so), _ptr(beam), _stream()),
               'step')
     s.check_device_flag('step')
-    new = GPUArrays.__new__(GPUArrays)
-    for n in _lib.STATE_NAMES:
-        setattr(new, n, out[n])
-    return new
+    return e[0]
 
 
 def run(config, const, virt_params, state, xi0, nsteps, beam=None):
