@@ -133,9 +133,10 @@ MoveArgs move_base(lc3d_ctx* c) {
 
 int deposit_into(lc3d_ctx* c, const double* ro_initial, const double* x, const double* y, const double* m,
                  const double* q, const double* px, const double* py, const double* pz, double* ro, double* jx,
-                 double* jy, double* jz, cudaStream_t s) {
+                 double* jy, double* jz, cudaStream_t s, const double* packed = nullptr) {
     DepositArgs a;
     a.x_offt = x; a.y_offt = y; a.m = m; a.q = q; a.px = px; a.py = py; a.pz = pz;
+    a.packed = packed;   // the same values, packed by the move just before
     a.inf_prev = c->inf_prev; a.inf_next = c->inf_next; a.fine_grid = c->fine_grid;
     a.idx_prev = c->idx_prev; a.idx_next = c->idx_next;
     a.acc = c->acc;
@@ -224,6 +225,7 @@ int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& ou
     mv.m = c->m; mv.q = c->q; mv.x_init = c->x_init; mv.y_init = c->y_init;
     mv.x_prev = prev.x_offt; mv.y_prev = prev.y_offt;
     mv.px_prev = prev.px; mv.py_prev = prev.py; mv.pz_prev = prev.pz;
+    mv.out_packed = c->packed;            // each deposition below follows a move
 
     SolveInputs in;
     memset(&in, 0, sizeof(in));
@@ -279,7 +281,7 @@ int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& ou
             continue;
         }
         LC3D_TRY(deposit_into(c, c->ro_initial, pw[0], pw[1], c->m, c->q, pw[2], pw[3], pw[4], c->dens[0],
-                              c->dens[1], c->dens[2], c->dens[3], s));
+                              c->dens[1], c->dens[2], c->dens[3], s, c->packed));
         if (pass == 0) {
             in.Ex_sub = prev.Ex; in.Ey_sub = prev.Ey; in.Bx_sub = prev.Bx; in.By_sub = prev.By;
             for (int f = 0; f < 6; ++f) so.out[f] = (x && x->first) ? x->first[f] : nullptr;
@@ -317,7 +319,7 @@ int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& ou
         LC3D_TRY(launch_move_smart(mv, s));
     }
     LC3D_TRY(deposit_into(c, c->ro_initial, out.x_offt, out.y_offt, c->m, c->q, out.px, out.py, out.pz, out.ro,
-                          out.jx, out.jy, out.jz, s));
+                          out.jx, out.jy, out.jz, s, c->packed));
     return LC3D_OK;
 }
 
@@ -342,6 +344,7 @@ void destroy(lc3d_ctx* c) {
     if (c->zeros) cudaFree(c->zeros);
     if (c->resid) cudaFree(c->resid);
     if (c->beam_dev) cudaFree(c->beam_dev);
+    if (c->packed) cudaFree(c->packed);
     if (c->ev_main) cudaEventDestroy(c->ev_main);
     if (c->ev_copy) cudaEventDestroy(c->ev_copy);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
@@ -501,6 +504,7 @@ int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out) {
     LC3D_STEP(dalloc(&c->zeros, ng));
     LC3D_STEP(dalloc(&c->resid, (size_t)2));
     LC3D_STEP(dalloc(&c->beam_dev, ng));
+    LC3D_STEP(dalloc(&c->packed, 8 * np));
     if (rc == LC3D_OK && cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = LC3D_ERR_CUDA;
     if (rc == LC3D_OK && cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming) != cudaSuccess) rc = LC3D_ERR_CUDA;
     if (rc == LC3D_OK && cudaEventCreateWithFlags(&c->ev_copy, cudaEventDisableTiming) != cudaSuccess) rc = LC3D_ERR_CUDA;

@@ -72,6 +72,7 @@ struct MoveArgs {
     const double *px_prev, *py_prev, *pz_prev;
     const double *F[6];                   // Ex Ey Ez Bx By Bz (averaged)
     double *out_x, *out_y, *out_px, *out_py, *out_pz;
+    double* out_packed;                   // optional: [n][8] = x_offt y_offt m q px py pz, pad
     int n;                                // coarse particles
     int N;                                // grid_steps
     double h, inv_h, dxi, rb;
@@ -89,6 +90,7 @@ struct DepositArgs {
     const double *x_offt, *y_offt, *m, *q, *px, *py, *pz;   // coarse, Nc x Nc
     const double *inf_prev, *inf_next, *fine_grid;            // Nf
     const int32_t *idx_prev, *idx_next;                       // Nf
+    const double* packed;                                     // optional: the 7 coarse arrays as [Nc*Nc][8]
     unsigned long long* acc;                                  // 8 planes of fixed-point words
     size_t plane;                                             // plane stride (>= N*N, 256-byte multiple)
     int Nc, Nf, N;
@@ -235,6 +237,7 @@ struct lc3d_ctx {
     double* diag_buf;                     // zn diagnostic: two N x N blur planes
     int diag_r;                           // Gaussian radius
     double* beam_dev;                     // device copy of a host beam (lc3d_step_arrays_host_beam)
+    double* packed;                       // coarse particles of the last move, [Nc*Nc][8] (x y m q px py pz -)
     cudaStream_t copy_stream;             // its host-to-device copies
     cudaEvent_t ev_main, ev_copy;         // ordering of those copies with the step's stream
     // field-solver workspaces (fields.cu)
