@@ -47,10 +47,16 @@ check_errors = True
 # Array groups (lcode.py:52-119)
 # ---------------------------------------------------------------------------
 
+_cuda_seen = False   # a CUDA device was found once; availability does not go away
+
+
 def _device():
-    if not torch.cuda.is_available():
-        raise RuntimeError('lcode3d_b200 needs a CUDA device (B200, sm_100a); '
-                           'there is no CPU fallback')
+    global _cuda_seen
+    if not _cuda_seen:
+        if not torch.cuda.is_available():
+            raise RuntimeError('lcode3d_b200 needs a CUDA device (B200, sm_100a); '
+                               'there is no CPU fallback')
+        _cuda_seen = True
     return torch.device('cuda', torch.cuda.current_device())
 
 
@@ -211,7 +217,7 @@ _CFG_OPTIONAL = (('lc3d_precision', 'fp64'), ('lc3d_fp64_transform', 'auto'), ('
 def solver_for(config):
     """The cached Solver of this configuration on the current device."""
     raw = None
-    if torch.cuda.is_available():
+    if _cuda_seen or torch.cuda.is_available():
         raw = (tuple(getattr(config, n, None) for n in _CFG_ATTRS) +
                tuple(getattr(config, n, d) for n, d in _CFG_OPTIONAL) + (torch.cuda.current_device(),))
         try:
@@ -285,6 +291,17 @@ class _StatePool:
     @staticmethod
     def _counts(e):
         return [sys.getrefcount(e[0])] + [sys.getrefcount(t) for t in e[1]]
+
+    def ptrs_of(self, state):
+        """The StatePtrs of `state` if it is one of the pool's states with
+        all 15 arrays still its own (else None)."""
+        for e in self.entries:
+            if e[0] is state:
+                for n, t in zip(_lib.STATE_NAMES, e[1]):
+                    if getattr(state, n) is not t:
+                        return None
+                return e[2]
+        return None
 
     def take(self, shape_p, g, dev):
         for e in self.entries:
@@ -504,9 +521,11 @@ def step(config, const, virt_params, prev, beam_ro):
     shape_p = tuple(prev.x_offt.shape)
     g = _grid(config)
     dev = _device()
-    prev_t = _state_arrays(prev, shape_p, g, dev)
+    sp = s.out_pool.ptrs_of(prev)   # the previous step's output: its arrays are known
+    if sp is None:
+        prev_t = _state_arrays(prev, shape_p, g, dev)
+        sp = _lib.StatePtrs(*[t.data_ptr() for t in prev_t])
     e = s.out_pool.take(shape_p, g, dev)
-    sp = _lib.StatePtrs(*[t.data_ptr() for t in prev_t])
     so = e[2]
     if hb is not None:
         check(lib.lc3d_step_arrays_host_beam(s.ctx, ctypes.byref(sp), ctypes.byref(so),

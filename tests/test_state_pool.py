@@ -44,3 +44,15 @@ def test_the_reference_loop_cycles_through_two_entries():
         seen.add(id(state))
     assert len(seen) <= lcode._StatePool.SIZE
     assert len(pool.entries) <= lcode._StatePool.SIZE
+
+
+def test_ptrs_of_knows_only_unmodified_pool_states():
+    pool = lcode._StatePool()
+    s0 = take(pool)
+    assert pool.ptrs_of(s0) is pool.entries[0][2]
+    s0.Ez = torch.zeros(5, 5, dtype=torch.float64)   # the caller swapped an array
+    assert pool.ptrs_of(s0) is None
+
+    class Other:
+        pass
+    assert pool.ptrs_of(Other()) is None
