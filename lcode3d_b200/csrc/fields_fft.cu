@@ -1,4 +1,7 @@
-// Float64 DST-I / DCT-I row transforms through a shared-memory FFT.
+// DST-I / DCT-I row transforms through a shared-memory FFT, in float64, or
+// in float32 for the float32-transform precision (one kernel template,
+// fft_rows_kernel<T, Tin, Tout>: arithmetic in T, rows read as Tin and
+// written as Tout).
 //
 // The reference realises its transforms with padded real FFTs
 // (lcode.py:124-141 dst2d, 190-212 mix2d, 295-313 dct2d). Here every 1-D
@@ -23,7 +26,8 @@
 //     D: rows of T3^T by the axis-0 transform              -> F
 // (Lambda on B's output rather than C's input: the multiply is the same,
 // and no Lambda rows take staging space, which keeps 3 CTAs per SM.)
-// One launch covers all fields of a solve.
+// One launch covers all fields of a solve; launches are programmatic
+// dependent launches (the kernel waits for its predecessor on the device).
 
 #include <algorithm>
 #include <cmath>
