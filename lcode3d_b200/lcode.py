@@ -171,8 +171,6 @@ class Solver:
         self.out_pool = _StatePool()
         self._const_arrays = None
         self._virt_arrays = None
-        self._const_key = None
-        self._virt_key = None
         self._keep = ()
 
     def __del__(self):
@@ -183,12 +181,10 @@ class Solver:
 
     # -- constants ----------------------------------------------------------
     def set_virt(self, virt):
+        # the same array objects as last time: nothing to copy (the solver
+        # holds them, so their storage cannot have been freed and reused)
         arrays = tuple(getattr(virt, n) for n in _lib.VIRT_NAMES)
         if self._virt_arrays is not None and all(a is b for a, b in zip(arrays, self._virt_arrays)):
-            return   # the same array objects as last time (their storage cannot have moved)
-        key = tuple(a.data_ptr() for a in arrays)
-        if key == self._virt_key:
-            self._virt_arrays = arrays
             return
         ip = getattr(virt, 'indices_prev').to(torch.int32).contiguous()
         inn = getattr(virt, 'indices_next').to(torch.int32).contiguous()
@@ -197,20 +193,14 @@ class Solver:
         check(lib.lc3d_set_const(self.ctx, None, ctypes.byref(v), _stream()), 'lc3d_set_const')
         self._keep = (ip, inn)   # alive until the stream-ordered copy ran
         torch.cuda.current_stream().synchronize()
-        self._virt_key = key
         self._virt_arrays = arrays
 
     def set_const(self, const):
         arrays = tuple(getattr(const, n) for n in _lib.CONST_NAMES)
         if self._const_arrays is not None and all(a is b for a, b in zip(arrays, self._const_arrays)):
             return   # the same array objects as last time
-        key = tuple(a.data_ptr() for a in arrays)
-        if key == self._const_key:
-            self._const_arrays = arrays
-            return
         c = _lib.ConstPtrs(*[getattr(const, n).data_ptr() for n in _lib.CONST_NAMES])
         check(lib.lc3d_set_const(self.ctx, ctypes.byref(c), None, _stream()), 'lc3d_set_const')
-        self._const_key = key
         self._const_arrays = arrays
 
     def check_device_flag(self, where):
