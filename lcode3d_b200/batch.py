@@ -10,8 +10,6 @@ the device). Across GPUs the simulations are partitioned by cost with no
 exchange during the run; only the Ez(0,0) histories are gathered at the end.
 """
 import ctypes
-import math
-import time
 import types
 
 import numpy as np

@@ -24,8 +24,6 @@ averaging and particles in float64);
 transforms (1..6, default 4).
 """
 import ctypes
-import math
-import os
 import sys
 
 import numpy as np

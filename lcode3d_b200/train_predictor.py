@@ -19,7 +19,6 @@ import time
 import types
 
 import numpy as np
-import torch
 
 from . import predictor as P
 

@@ -5,7 +5,6 @@ import glob
 import os
 import re
 
-import numpy as np
 import pytest
 
 from conftest import ROOT

@@ -1,7 +1,6 @@
 """Host logic of batched scans: seeded draws, cost-balanced partition across
 ranks, and the end-of-run gather / max-over-ranks timing, the multi-rank
 parts on 2 gloo ranks (CPU)."""
-import os
 import socket
 
 import numpy as np

@@ -2,13 +2,12 @@
 tests/golden/make_golden.py from the reference lcode.py) and against
 known answers from mathematics. CPU only."""
 import os
-import sys
 import types
 
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, ROOT
+from conftest import GOLDEN
 
 from make_golden import beam_array, make_config  # noqa: E402
 from oracle import lcode_oracle as O  # noqa: E402
