@@ -399,7 +399,7 @@ struct FieldGeom {
 
 FieldGeom geom(const lc3d_ctx* c, int f) {
     const int N = c->N, M = c->M;
-    FieldGeom g;
+    FieldGeom g{};
     switch (f) {
         case 0: case 4:   // Ex, By: solved transposed
             g = {N, M, 1, c->C, c->S2, c->lam_mixT, N, M, M, 0, 1};
@@ -437,7 +437,7 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
     if (which & LC3D_F_EZ) on[2] = true;
     if (which & LC3D_F_BZ) on[5] = true;
 
-    RhsArgs ra;
+    RhsArgs ra{};
     memset(&ra, 0, sizeof(ra));
     ra.in = in;
     ra.st = c->p.field_solver_subtraction_trick;
@@ -469,7 +469,7 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
     if (c->p.precision == LC3D_PREC_MIXED) {
         // four split-BF16 tensor-core GEMM stages (fields_mixed.cu)
         for (int stage = 0; stage < 4; ++stage) {
-            MixedStageDesc d[6];
+            MixedStageDesc d[6]{};
             int cnt = 0;
             for (int f = 0; f < 6; ++f) {
                 if (!on[f]) continue;
@@ -512,7 +512,7 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
         const int types[4] = {f32 ? FFT_F64_F32 : FFT_F64, f32 ? FFT_F32 : FFT_F64, f32 ? FFT_F32 : FFT_F64,
                               f32 ? FFT_F32_F64 : FFT_F64};
         for (int stage = 0; stage < 4; ++stage) {
-            FftRowsDesc d[6];
+            FftRowsDesc d[6]{};
             int cnt = 0;
             for (int f = 0; f < 6; ++f) {
                 if (!on[f]) continue;
@@ -540,7 +540,7 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
     } else {
         // the four GEMM stages
         for (int stage = 0; stage < 4; ++stage) {
-            GemmBatch b;
+            GemmBatch b{};
             memset(&b, 0, sizeof(b));
             for (int f = 0; f < 6; ++f) {
                 if (!on[f]) continue;
@@ -595,7 +595,7 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
         }
         return LC3D_OK;
     }
-    FinalizeArgs fa;
+    FinalizeArgs fa{};
     memset(&fa, 0, sizeof(fa));
     for (int f = 0; f < 6; ++f) {
         if (!on[f]) continue;

@@ -551,7 +551,7 @@ int fft_prepare(int P) {
 // transposed into `out`. `types` (FFT_*) gives the element types of the
 // rows read and written and of the arithmetic.
 int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, int types, cudaStream_t s) {
-    FftBatch b;
+    FftBatch b{};
     memset(&b, 0, sizeof(b));
     b.P = 2 * (c->N - 1);
     b.N = c->N;

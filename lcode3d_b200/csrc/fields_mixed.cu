@@ -435,7 +435,7 @@ int mixed_stage(lc3d_ctx* c, const MixedStageDesc* d, int count, cudaStream_t s)
     MixedState* ms = static_cast<MixedState*>(c->mixed);
     if (!ms) return LC3D_ERR_STATE;
     // 1. slice the data operands
-    SliceArgs sa;
+    SliceArgs sa{};
     memset(&sa, 0, sizeof(sa));
     sa.count = count;
     sa.S = ms->S;
@@ -459,7 +459,7 @@ int mixed_stage(lc3d_ctx* c, const MixedStageDesc* d, int count, cudaStream_t s)
         LC3D_CUDA_TRY(cudaGetLastError());
     }
     // 2. the GEMMs
-    OzBatch b;
+    OzBatch b{};
     memset(&b, 0, sizeof(b));
     b.count = count;
     b.S = ms->S;

@@ -119,7 +119,7 @@ bool state_complete(const lc3d_state_ptrs* s) {
 }
 
 MoveArgs move_base(lc3d_ctx* c) {
-    MoveArgs a;
+    MoveArgs a{};
     memset(&a, 0, sizeof(a));
     a.n = c->Nc * c->Nc;
     a.N = c->N;
@@ -134,7 +134,7 @@ MoveArgs move_base(lc3d_ctx* c) {
 int deposit_into(lc3d_ctx* c, const double* ro_initial, const double* x, const double* y, const double* m,
                  const double* q, const double* px, const double* py, const double* pz, double* ro, double* jx,
                  double* jy, double* jz, cudaStream_t s, const double* packed = nullptr) {
-    DepositArgs a;
+    DepositArgs a{};
     a.x_offt = x; a.y_offt = y; a.m = m; a.q = q; a.px = px; a.py = py; a.pz = pz;
     a.packed = packed;   // the same values, packed by the move just before
     a.inf_prev = c->inf_prev; a.inf_next = c->inf_next; a.fine_grid = c->fine_grid;
@@ -144,7 +144,7 @@ int deposit_into(lc3d_ctx* c, const double* ro_initial, const double* x, const d
     a.Nc = c->Nc; a.Nf = c->Nf; a.N = c->N;
     a.h = c->p.grid_step_size; a.inv_h = 1.0 / c->p.grid_step_size; a.sf = c->sf;
     a.err = c->err;
-    DepositFinalizeArgs f;
+    DepositFinalizeArgs f{};
     f.acc = c->acc;
     f.plane = c->acc_plane;
     f.ro_initial = ro_initial;
@@ -227,7 +227,7 @@ int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& ou
     mv.px_prev = prev.px; mv.py_prev = prev.py; mv.pz_prev = prev.pz;
     mv.out_packed = c->packed;            // each deposition below follows a move
 
-    SolveInputs in;
+    SolveInputs in{};
     memset(&in, 0, sizeof(in));
     in.ro = c->dens[0]; in.jx = c->dens[1]; in.jy = c->dens[2]; in.jz = c->dens[3];
     in.ro_prev = A ? prev.ro : nullptr;
@@ -235,7 +235,7 @@ int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& ou
     in.jx_prev = prev.jx; in.jy_prev = prev.jy;
     in.beam = beam;
 
-    SolveOutputs so;
+    SolveOutputs so{};
     memset(&so, 0, sizeof(so));
     so.mode = 1;
     for (int f = 0; f < 6; ++f) {
@@ -268,7 +268,7 @@ int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& ou
         if (pass == 0 && predicted) {
             // the prediction stands in for the first-pass fields: only the
             // particle positions of this pass are used (as the estimate)
-            AvgArgs g;
+            AvgArgs g{};
             for (int f = 0; f < 6; ++f) {
                 g.a[f] = x->pred[f];
                 g.b[f] = prevF[f];
@@ -294,7 +294,7 @@ int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& ou
         LC3D_TRY(solve_fields(c, LC3D_F_ALL, in, so, s));
     }
     if (predicted && x->residual) {
-        ResidArgs ra;
+        ResidArgs ra{};
         const double* F2[5] = {out.Ex, out.Ey, out.Bx, out.By, out.Bz};
         const int pi[5] = {0, 1, 3, 4, 5};
         for (int f = 0; f < 5; ++f) {
@@ -575,7 +575,7 @@ int lc3d_init_plasma(lc3d_ctx* c, void* stream) {
     const cudaStream_t s = S(stream);
     const int N = c->N, co = c->p.plasma_coarseness, fi = c->p.plasma_fineness;
     const int steps = N - 2 * c->p.plasma_padding_steps;
-    PlasmaArgs a;
+    PlasmaArgs a{};
     a.m = c->m; a.q = c->q; a.x_init = c->x_init; a.y_init = c->y_init;
     a.inf_prev = c->inf_prev; a.inf_next = c->inf_next; a.fine = c->fine_grid;
     a.idx_prev = c->idx_prev; a.idx_next = c->idx_next;
@@ -694,7 +694,7 @@ int lc3d_step_arrays_predicted(lc3d_ctx* c, const lc3d_state_ptrs* prev, const l
 
 int lc3d_fields_rel_diff(lc3d_ctx* c, const double* const* a, const double* const* b, double* out, void* stream) {
     if (!c || !a || !b || !out) return LC3D_ERR_PARAM;
-    ResidArgs ra;
+    ResidArgs ra{};
     const int pi[5] = {0, 1, 3, 4, 5};   // Ex, Ey, Bx, By, Bz
     for (int f = 0; f < 5; ++f) {
         if (!a[pi[f]] || !b[pi[f]]) return LC3D_ERR_PARAM;
@@ -720,7 +720,7 @@ int lc3d_move_estimate_wo_fields(lc3d_ctx* c, const double* m, const double* x_i
         !out_y_offt)
         return LC3D_ERR_PARAM;
     DeviceGuard g(c->device);
-    EstimateArgs a;
+    EstimateArgs a{};
     a.m = m; a.x_init = x_init; a.y_init = y_init; a.x_prev = prev_x_offt; a.y_prev = prev_y_offt;
     a.px = px; a.py = py; a.pz = pz; a.out_x = out_x_offt; a.out_y = out_y_offt;
     a.n = c->Nc * c->Nc;
@@ -776,12 +776,12 @@ int lc3d_calculate_Ex_Ey_Bx_By(lc3d_ctx* c, const double* Ex_avg, const double* 
     for (const void* r : req)
         if (!r) return LC3D_ERR_PARAM;
     DeviceGuard g(c->device);
-    SolveInputs in;
+    SolveInputs in{};
     memset(&in, 0, sizeof(in));
     in.ro = ro; in.jz = jz; in.jx = jx; in.jy = jy; in.jx_prev = jx_prev; in.jy_prev = jy_prev;
     in.beam = beam_ro ? beam_ro : c->zeros;
     in.Ex_sub = Ex_avg; in.Ey_sub = Ey_avg; in.Bx_sub = Bx_avg; in.By_sub = By_avg;
-    SolveOutputs o;
+    SolveOutputs o{};
     memset(&o, 0, sizeof(o));
     o.out[0] = Ex; o.out[1] = Ey; o.out[3] = Bx; o.out[4] = By;
     return solve_fields(c, LC3D_F_EXEYBXBY, in, o, S(stream));
@@ -790,10 +790,10 @@ int lc3d_calculate_Ex_Ey_Bx_By(lc3d_ctx* c, const double* Ex_avg, const double* 
 int lc3d_calculate_Ez(lc3d_ctx* c, const double* jx, const double* jy, double* Ez, void* stream) {
     if (!c || !jx || !jy || !Ez) return LC3D_ERR_PARAM;
     DeviceGuard g(c->device);
-    SolveInputs in;
+    SolveInputs in{};
     memset(&in, 0, sizeof(in));
     in.jx = jx; in.jy = jy;
-    SolveOutputs o;
+    SolveOutputs o{};
     memset(&o, 0, sizeof(o));
     o.out[2] = Ez;
     return solve_fields(c, LC3D_F_EZ, in, o, S(stream));
@@ -802,10 +802,10 @@ int lc3d_calculate_Ez(lc3d_ctx* c, const double* jx, const double* jy, double* E
 int lc3d_calculate_Bz(lc3d_ctx* c, const double* jx, const double* jy, double* Bz, void* stream) {
     if (!c || !jx || !jy || !Bz) return LC3D_ERR_PARAM;
     DeviceGuard g(c->device);
-    SolveInputs in;
+    SolveInputs in{};
     memset(&in, 0, sizeof(in));
     in.jx = jx; in.jy = jy;
-    SolveOutputs o;
+    SolveOutputs o{};
     memset(&o, 0, sizeof(o));
     o.out[5] = Bz;
     return solve_fields(c, LC3D_F_BZ, in, o, S(stream));

@@ -666,7 +666,7 @@ extern "C" int lc3d_deposit_noalloc(const lc3d_params* p, const double* ro_initi
     LC3D_CUDA_TRY(cudaMemsetAsync(scratch, 0, DEP_WORDS_PER_CELL * plane * sizeof(unsigned long long), s));
     LC3D_CUDA_TRY(cudaMemsetAsync(err_word, 0, sizeof(unsigned long long), s));
     const int c = p->plasma_coarseness, f = p->plasma_fineness;
-    DepositArgs a;
+    DepositArgs a{};
     a.x_offt = x_offt; a.y_offt = y_offt; a.m = m; a.q = q; a.px = px; a.py = py; a.pz = pz;
     a.inf_prev = influence_prev; a.inf_next = influence_next; a.fine_grid = fine_grid;
     a.idx_prev = indices_prev; a.idx_next = indices_next;
@@ -677,7 +677,7 @@ extern "C" int lc3d_deposit_noalloc(const lc3d_params* p, const double* ro_initi
     a.inv_h = 1.0 / p->grid_step_size;
     a.sf = 1.0 / ((double)(c * f) * (c * f));
     a.err = reinterpret_cast<unsigned*>(err_word);
-    DepositFinalizeArgs fa;
+    DepositFinalizeArgs fa{};
     fa.acc = scratch;
     fa.plane = plane;
     fa.ro_initial = ro_initial;

@@ -917,7 +917,7 @@ int lc3d_predictor_set_scales(lc3d_predictor* P, const double* in_mult, const do
 
 int lc3d_predictor_pack(lc3d_predictor* P, const double* const* f1, const double* const* f2, void* stream) {
     if (!P || !f1 || !f2) return LC3D_ERR_PARAM;
-    PackArgs a;
+    PackArgs a{};
     for (int c = 0; c < 9; ++c) {
         if (!f1[c] || !f2[c]) return LC3D_ERR_PARAM;
         a.f1[c] = f1[c];
@@ -959,7 +959,7 @@ static int out_args(lc3d_predictor* P, OutArgs* a, const double* const* f1, cons
 int lc3d_predictor_predict(lc3d_predictor* P, const double* const* f1, const double* const* f2,
                            double* const* pred, void* stream) {
     if (!P || !f1 || !f2 || !pred) return LC3D_ERR_PARAM;
-    OutArgs a;
+    OutArgs a{};
     LC3D_TRY(out_args(P, &a, f1, f2, true));
     for (int f = 0; f < 6; ++f) {
         if (!pred[f]) return LC3D_ERR_PARAM;
@@ -974,7 +974,7 @@ int lc3d_predictor_predict(lc3d_predictor* P, const double* const* f1, const dou
 int lc3d_predictor_set_target(lc3d_predictor* P, const double* const* first, const double* const* f1,
                               const double* const* f2, void* stream) {
     if (!P || !first || !f1 || !f2) return LC3D_ERR_PARAM;
-    OutArgs a;
+    OutArgs a{};
     LC3D_TRY(out_args(P, &a, f1, f2, false));
     for (int k = 0; k < 5; ++k) {
         if (!first[net_field(k)]) return LC3D_ERR_PARAM;
