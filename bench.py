@@ -293,7 +293,7 @@ def run_ours(args, rank, world, dist):
     # ---- e2e through the public API, host beam in pinned memory ----
     st_e = st
     pinned = [torch.from_numpy(beam_np(cfg, x0 + i, xs, ys)).pin_memory() for i in range(W + K)]
-    L.lcode.check_errors = False
+    L.lcode.check_errors = True   # the drop-in default: the device error flag is read after every call
     for i in range(W):
         st_e = L.step(cfg, const, virt, st_e, pinned[i])
         float(st_e.Ez[N // 2, N // 2])
@@ -402,7 +402,8 @@ def run_ours(args, rank, world, dist):
                    'l2': 'flushed between timed steps (256 MiB write, outside the step events)',
                    'parallelism': f'replicas x{world}' if world > 1 else 'single GPU'},
         'e2e': {'value': world * K / (e2e_ms * 1e-3), 'unit': 'xi-steps/s',
-                'h2d_bytes_per_step': N * N * 8, 'd2h_bytes_per_step': 8,
+                'h2d_bytes_per_step': N * N * 8, 'd2h_bytes_per_step': 8 + 4,
+                'error_check': 'device error flag read after every step (lcode.check_errors = True, the default)',
                 'wall_ms': wall_ms, 'api': 'lcode3d_b200.step (drop-in for lcode.step)'},
         'gpu_launches': int(sum(launches)),
         'launches_per_step': sum(launches) / K,
@@ -442,19 +443,86 @@ def accuracy_vs_fp64(args, ez_pre, ez_field_pre):
             'within_1e-6': bool(max(e_h, e_f) <= 1e-6)}
 
 
+ACCURACY_FIELDS = ('Ex', 'Ey', 'Ez', 'Bx', 'By', 'Bz', 'ro', 'jx', 'jy', 'jz')
+
+
+def run_accuracy_table(args):
+    """Error of every reduced-precision form against the float64 path on the
+    641^2 production run (A = 0.5, dxi = 0.005) from its initial state: the
+    max |difference| / max |float64| of each field at the given steps, and of
+    the on-axis Ez(N/2, N/2) history up to each of them. Host beams through
+    the drop-in step(), as the reference's loop evaluates them."""
+    import torch
+    import lcode3d_b200 as L
+    torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+    N = args.grid
+    marks = sorted(int(x) for x in args.accuracy_steps.split(','))
+    steps = marks[-1]
+    forms = [('fp64', {})] + [(f, {}) for f in ('fft32', 'tf32') if f in args.forms.split(',')]
+    forms += [(f'mixed_s{S}', {'lc3d_mixed_slices': S}) for S in (3, 4, 5)
+              if f'mixed_s{S}' in args.forms.split(',')]
+    beams = None
+    results, ref = {}, None
+    for name, extra in forms:
+        prec = name.split('_')[0]
+        cfg = make_config(N, prec)
+        for k, v in extra.items():
+            setattr(cfg, k, v)
+        xs, ys, const, virt, st = L.init(cfg)
+        if beams is None:
+            beams = [torch.from_numpy(beam_np(cfg, i, xs, ys)) for i in range(steps)]
+        ez, snaps = [], {}
+        t0 = time.perf_counter()
+        for i in range(steps):
+            st = L.step(cfg, const, virt, st, beams[i])
+            ez.append(st.Ez[N // 2, N // 2].clone())
+            if i + 1 in marks:
+                snaps[i + 1] = {f: getattr(st, f).clone() for f in ACCURACY_FIELDS}
+        torch.cuda.synchronize()
+        secs = time.perf_counter() - t0
+        hist = torch.stack(ez)
+        if ref is None:
+            ref = (hist, snaps)
+            results[name] = {'seconds': secs}
+            continue
+        rows = {}
+        for m in marks:
+            r = {f: float((snaps[m][f] - ref[1][m][f]).abs().max() / ref[1][m][f].abs().max().clamp_min(1e-300))
+                 for f in ACCURACY_FIELDS}
+            h = (hist[:m] - ref[0][:m]).abs().max() / ref[0][:m].abs().max().clamp_min(1e-300)
+            r['Ez_axis_history'] = float(h)
+            rows[str(m)] = r
+        e_h = rows[str(steps)]['Ez_axis_history']
+        results[name] = {'seconds': secs, 'errors_vs_fp64': rows,
+                         'ez_gate_1e-6': bool(e_h <= 1e-6 and rows[str(steps)]['Ez'] <= 1e-6)}
+        del snaps
+    return {'accuracy_table': results, 'grid_steps': N, 'steps': steps, 'marks': marks,
+            'workload': f'{N}^2 production run, h={GRIDS[N][0]}, xi_step={GRIDS[N][1]}, A={GRIDS[N][2]}, '
+                        'from the initial state, host beams through lcode3d_b200.step',
+            'metric': 'max |form - fp64| / max |fp64| per field at each step; Ez(N/2, N/2) history up to it'}
+
+
 # ---------------------------------------------------------------------------
 # CPU: the oracle (reference algorithm) on the host cores
 # ---------------------------------------------------------------------------
 
-def time_oracle(grid, steps, threads, start):
+def time_oracle(grid, steps, threads, start, warmup=0):
+    """xi-steps/s of the oracle over `steps` steps that begin at xi step
+    `start` (the state is first advanced there, untimed), after `warmup`
+    untimed steps. The beam arrays are evaluated before the timed loop, as
+    the GPU arms have theirs ready before their timed regions."""
     from oracle import lcode_oracle as O
     O.use_c_kernels(threads)
     O.FFT_WORKERS = threads
     cfg = make_config(grid, 'fp64')
     xs, ys, const, virt, st = O.init(cfg)
+    for i in range(start + warmup):
+        st = O.step(cfg, const, virt, st, beam_np(cfg, i, xs, ys))
+    x0 = start + warmup
+    beams = [beam_np(cfg, x0 + i, xs, ys) for i in range(steps)]
     t0 = time.perf_counter()
     for i in range(steps):
-        st = O.step(cfg, const, virt, st, beam_np(cfg, start + i, xs, ys))
+        st = O.step(cfg, const, virt, st, beams[i])
     return steps / (time.perf_counter() - t0)
 
 
@@ -608,10 +676,7 @@ def run_reference(args):
     threads = cpu_threads()
     K = max(1, min(args.steps, args.ref_max_steps))
     W = min(args.warmup, 1)
-    from oracle import lcode_oracle as O
-    if W:
-        time_oracle(args.grid, W, threads, 0)
-    v = time_oracle(args.grid, K, threads, 0)
+    v = time_oracle(args.grid, K, threads, args.pre, W)
     cfg = make_config(args.grid, 'fp64')
     N = cfg.grid_steps
     return {
@@ -621,10 +686,12 @@ def run_reference(args):
         'data': 'synthetic (generated cold uniform plasma + axisymmetric beam; no dataset)',
         'config': {'workload': f'LCODE 3D xi step, {N}x{N} grid, h={cfg.grid_step_size}, '
                                f'xi_step={cfg.xi_step_size}, coarseness 3 / fineness 2, A={GRIDS[N][2]}, '
-                               'fp64 field solvers', 'grid_steps': N},
+                               'fp64 field solvers', 'grid_steps': N, 'start_xi_step': args.pre,
+                   'beam': 'evaluated before the timed loop'},
         'cpu_baseline': {'value': v, 'unit': 'xi-steps/s', 'cores': threads, 'kind': 'port',
-                         'sample': f'{K} xi steps of the {N}^2 workload from its initial state '
-                                   '(reference algorithm: numpy + scipy.fft, particle kernels in C/OpenMP)'},
+                         'sample': f'{K} xi steps of the {N}^2 workload from xi step {args.pre + W} '
+                                   f'(advanced there untimed; reference algorithm: numpy + scipy.fft, '
+                                   'particle kernels in C/OpenMP)'},
         'e2e': {'value': v, 'unit': 'xi-steps/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
 
@@ -649,7 +716,14 @@ def main():
                     help='learned first pass with these trained parameters (.npz; default: the packaged ones)')
     ap.add_argument('--tol', type=float, default=1e-6, help='learned: verification tolerance on max|pred - F1| / max|F1|')
     ap.add_argument('--verify-every', type=int, default=10, help='learned: steps between verifications')
+    ap.add_argument('--accuracy-table', action='store_true',
+                    help='error of the reduced-precision forms against float64 over a long run')
+    ap.add_argument('--accuracy-steps', default='500,1500,3000', help='accuracy table: steps to report')
+    ap.add_argument('--forms', default='fft32,mixed_s4,mixed_s5', help='accuracy table: forms to compare')
     args = ap.parse_args()
+    if args.accuracy_table:
+        print(json.dumps(run_accuracy_table(args)), flush=True)
+        return
     if args.warmup < 3 and args.impl == 'ours':
         args.warmup = 3
 
@@ -687,8 +761,9 @@ def main():
         v = time_oracle(args.grid, args.cpu_steps, threads, 0)
         out['cpu_baseline'] = {
             'value': v, 'unit': 'xi-steps/s', 'cores': threads, 'kind': 'port',
-            'sample': f'{args.cpu_steps} xi steps of the {args.grid}^2 workload from its initial state, '
-                      'oracle restatement of the reference (numpy + scipy.fft, particle kernels in C), 1 thread'}
+            'sample': f'{args.cpu_steps} xi steps of the {args.grid}^2 workload from its initial state '
+                      '(beams evaluated before the timed loop), oracle restatement of the reference '
+                      '(numpy + scipy.fft, particle kernels in C), 1 thread'}
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()

@@ -178,11 +178,22 @@ class Solver:
             self.ctx = None
 
     # -- constants ----------------------------------------------------------
+    @staticmethod
+    def _unchanged(arrays, seen):
+        """The same array objects as last time, none written since (torch
+        counts every in-place write of a tensor or of a view of it in
+        ``_version``): nothing to copy. The solver holds the arrays, so their
+        storage cannot have been freed and reused meanwhile."""
+        return seen is not None and all(a is b and getattr(a, '_version', None) == v
+                                        for a, (b, v) in zip(arrays, seen))
+
+    @staticmethod
+    def _seen(arrays):
+        return tuple((a, getattr(a, '_version', None)) for a in arrays)
+
     def set_virt(self, virt):
-        # the same array objects as last time: nothing to copy (the solver
-        # holds them, so their storage cannot have been freed and reused)
         arrays = tuple(getattr(virt, n) for n in _lib.VIRT_NAMES)
-        if self._virt_arrays is not None and all(a is b for a, b in zip(arrays, self._virt_arrays)):
+        if self._unchanged(arrays, self._virt_arrays):
             return
         ip = getattr(virt, 'indices_prev').to(torch.int32).contiguous()
         inn = getattr(virt, 'indices_next').to(torch.int32).contiguous()
@@ -191,15 +202,15 @@ class Solver:
         check(lib.lc3d_set_const(self.ctx, None, ctypes.byref(v), _stream()), 'lc3d_set_const')
         self._keep = (ip, inn)   # alive until the stream-ordered copy ran
         torch.cuda.current_stream().synchronize()
-        self._virt_arrays = arrays
+        self._virt_arrays = self._seen(arrays)
 
     def set_const(self, const):
         arrays = tuple(getattr(const, n) for n in _lib.CONST_NAMES)
-        if self._const_arrays is not None and all(a is b for a, b in zip(arrays, self._const_arrays)):
-            return   # the same array objects as last time
+        if self._unchanged(arrays, self._const_arrays):
+            return
         c = _lib.ConstPtrs(*[getattr(const, n).data_ptr() for n in _lib.CONST_NAMES])
         check(lib.lc3d_set_const(self.ctx, ctypes.byref(c), None, _stream()), 'lc3d_set_const')
-        self._const_arrays = arrays
+        self._const_arrays = self._seen(arrays)
 
     def check_device_flag(self, where):
         if check_errors:
@@ -272,16 +283,26 @@ def _state_arrays(state, shape_p, g, dev):
     return out
 
 
+_use_count = getattr(torch._C, '_storage_Use_Count', None)
+
+
 class _StatePool:
     """Output states of ``step`` kept for reuse (per Solver). An entry (a
     GPUArrays, its 15 arrays and their StatePtrs) is handed out again only
-    when nothing outside the pool refers to the object or to any of its
-    arrays: their CPython reference counts are back at the values taken
-    when the entry was made. That is the state before last in the
-    reference's loop (``state = step(..., state, ...)``), which the caller
-    has dropped. A reused state is the same Python object, with the new
-    step's values; states the caller keeps are never touched. Saves the
-    allocation and the 15 array objects of a step."""
+    when nothing outside the pool refers to it:
+
+    * the CPython reference counts of the object and of its 15 arrays are
+      back at the values taken when the entry was made, and
+    * the use count of the entry's one device allocation (every tensor that
+      shares the memory: slices and views such as ``state.Ez[i, j]``, a
+      DLPack export) is back at its value then.
+
+    That is the state before last in the reference's loop
+    (``state = step(..., state, ...)``), which the caller has dropped. A
+    reused state is the same Python object, with the new step's values;
+    states the caller keeps, or keeps any view of, are never touched. Saves
+    the allocation and the 15 array objects of a step. Without a storage use
+    count in this torch build nothing is reused."""
 
     SIZE = 3
 
@@ -290,7 +311,7 @@ class _StatePool:
 
     @staticmethod
     def _counts(e):
-        return [sys.getrefcount(e[0])] + [sys.getrefcount(t) for t in e[1]]
+        return [sys.getrefcount(e[0])] + [sys.getrefcount(t) for t in e[1]] + [_use_count(e[5])]
 
     def ptrs_of(self, state):
         """The StatePtrs of `state` if it is one of the pool's states with
@@ -311,9 +332,11 @@ class _StatePool:
         obj = GPUArrays.__new__(GPUArrays)
         for n, t in zip(_lib.STATE_NAMES, arrays):
             setattr(obj, n, t)
-        e = [obj, arrays, _lib.StatePtrs(*[t.data_ptr() for t in arrays]), None, (shape_p, g, dev)]
+        # the storage object only lends its handle: the pool's arrays keep the allocation alive
+        e = [obj, arrays, _lib.StatePtrs(*[t.data_ptr() for t in arrays]), None, (shape_p, g, dev),
+             arrays[0].untyped_storage()._cdata]
         del obj, arrays, n, t
-        if len(self.entries) < self.SIZE:
+        if len(self.entries) < self.SIZE and _use_count is not None:
             self.entries.append(e)
             e[3] = self._counts(e)
         return e

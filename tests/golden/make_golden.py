@@ -26,7 +26,18 @@ reference's own code.
 The reference only exists in the build container, so the vectors are
 committed as ``.npz`` fixtures next to this script and the tests read those.
 
-Usage:  python tests/golden/make_golden.py [--ref /root/reference] [--which all|stages|cfg1|cfg2]
+Usage:  python tests/golden/make_golden.py --ref <reference checkout> [--which all|stages|cfg1|cfg2]
+        (or set LCODE_REFERENCE to the checkout instead of passing --ref)
+
+        python tests/golden/make_golden.py --ref R --which cfg2full [--resume-dir D]
+        python tests/golden/make_golden.py --ref R --which cfg2full-reversed --out REV.npz [--resume-dir D2]
+        python tests/golden/make_golden.py --which cfg2floor --out REV.npz
+
+``cfg2full`` runs the 641^2 production configuration for its whole 3000
+steps (several CPU hours) twice: once in the serial deposition order and once
+with the deposition's thread ids visited in reverse. The second run stands in
+for another order of the reference's float64 atomics, and the difference of
+the two is the order-sensitivity floor stored beside the fixture.
 """
 import argparse
 import functools
@@ -80,8 +91,11 @@ def _fake_matplotlib():
     return mpl, plt
 
 
-def load_reference(ref_dir):
-    """Return the reference ``lcode`` module running on numpy + numba (CPU)."""
+def load_reference(ref_dir, reverse_deposit=False):
+    """Return the reference ``lcode`` module running on numpy + numba (CPU).
+
+    With ``reverse_deposit`` the deposition kernel's thread ids are visited
+    from the last to the first (another order of the same float64 adds)."""
     import numba
     src = open(os.path.join(ref_dir, 'lcode.py')).read()
 
@@ -106,11 +120,11 @@ def load_reference(ref_dir):
     sub('numba.cuda.synchronize()', 'None')
     src += '''
 
-def _make_launcher(body):
+def _make_launcher(body, reverse=False):
     @numba.njit
     def _loop(n, args):
         for t in range(n):
-            body(t, *args)
+            body(n - 1 - t if reverse else t, *args)
 
     class _Launcher:
         def __getitem__(self, cfg):
@@ -119,7 +133,7 @@ def _make_launcher(body):
     return _Launcher()
 
 
-deposit_kernel = _make_launcher(deposit_kernel_body)
+deposit_kernel = _make_launcher(deposit_kernel_body, _REVERSE_DEPOSIT)
 move_smart_kernel = _make_launcher(move_smart_kernel_body)
 '''
     saved = {k: sys.modules.get(k) for k in ('cupy', 'matplotlib', 'matplotlib.pyplot')}
@@ -130,6 +144,7 @@ move_smart_kernel = _make_launcher(move_smart_kernel_body)
     try:
         mod = types.ModuleType('lcode_reference')
         mod.__file__ = os.path.join(ref_dir, 'lcode.py')
+        mod._REVERSE_DEPOSIT = bool(reverse_deposit)
         exec(compile(src, mod.__file__, 'exec'), mod.__dict__)
     finally:
         for k, v in saved.items():
@@ -375,12 +390,102 @@ def gen_cfg2(lc, out, steps):
     print(f'cfg2: {steps} steps in {dt:.1f} s', flush=True)
 
 
+FULL_SNAPSHOTS = (500, 1000, 1500, 3000)
+
+
+def _rows_summary(prefix, st, g):
+    """Middle row and main diagonal of every state array (grids N x N and
+    coarse particle arrays Nc x Nc), plus its sum, sum of moduli and maximum
+    modulus."""
+    for k, v in state_dict(st).items():
+        n = v.shape[0]
+        g[prefix + 'axis_' + k] = v[n // 2, :].copy()
+        g[prefix + 'diag_' + k] = np.diagonal(v).copy()
+        g[prefix + 'sum_' + k] = v.sum()
+        g[prefix + 'abssum_' + k] = np.abs(v).sum()
+        g[prefix + 'maxabs_' + k] = np.abs(v).max()
+
+
+def gen_cfg2_full(lc, out, resume_dir=None):
+    """The whole 641^2 production run (h=0.025, dxi=0.005, A=0.5, 3000 steps):
+    the Ez(0,0) history and row summaries at FULL_SNAPSHOTS. With
+    ``resume_dir`` the state is saved there every 250 steps and a saved state
+    is picked up again, so an interrupted run continues where it stopped."""
+    cfg = make_config(641, 0.025, 0.005, 3000, amplitude=0.5)
+    N = cfg.grid_steps
+    steps = 3000
+    xs, ys, const, virt, state = lc.init(cfg)
+    ez = np.zeros(steps)
+    g = {}
+    start = 0
+    ck = os.path.join(resume_dir, 'cfg2full_ck.npz') if resume_dir else None
+    if ck and os.path.exists(ck):
+        z = np.load(ck)
+        start = int(z['next_step'])
+        ez[:start] = z['ez'][:start]
+        g = {k[5:]: z[k] for k in z.files if k.startswith('snap_')}
+        state = lc.GPUArrays(**{k: z['st_' + k] for k in state_dict(state)})
+        print(f'cfg2full: resumed at step {start}', flush=True)
+    t0 = time.time()
+    for xi_i in range(start, steps):
+        b = beam_array(cfg, xi_i, xs, ys)
+        state = lc.step(cfg, const, virt, state, b)
+        ez[xi_i] = float(state.Ez[N // 2, N // 2])
+        if xi_i + 1 in FULL_SNAPSHOTS:
+            _rows_summary(f's{xi_i + 1}_', state, g)
+        if ck and (xi_i + 1) % 250 == 0 and xi_i + 1 < steps:
+            d = {'st_' + k: v for k, v in state_dict(state).items()}
+            d.update({'snap_' + k: v for k, v in g.items()})
+            np.savez(ck + '.tmp.npz', next_step=xi_i + 1, ez=ez, **d)
+            os.replace(ck + '.tmp.npz', ck)
+            print(f'cfg2full: step {xi_i + 1}, {time.time() - t0:.0f} s', flush=True)
+    g['Ez00'] = ez
+    g['steps'] = steps
+    g['snapshots'] = np.array(FULL_SNAPSHOTS)
+    np.savez_compressed(out, **g)
+    print(f'cfg2full: {steps} steps, {time.time() - t0:.1f} s in this process', flush=True)
+
+
+def gen_cfg2_floor(serial, reversed_, out):
+    """Order-sensitivity floor of the full run: for every recorded quantity,
+    the largest difference between the serial and the reversed deposition
+    order relative to the quantity's scale (max modulus of the serial
+    values). Written into the serial fixture as ``floor_<key>``."""
+    a = dict(np.load(serial))
+    b = np.load(reversed_)
+    for k in list(a):
+        if k in ('steps', 'snapshots') or k.startswith('floor_'):
+            continue
+        x, y = np.asarray(a[k], dtype=np.float64), np.asarray(b[k], dtype=np.float64)
+        scale = max(np.abs(x).max(), 1e-300)
+        a['floor_' + k] = np.abs(x - y).max() / scale
+    np.savez_compressed(out, **a)
+    worst = sorted(((float(v), k) for k, v in a.items() if k.startswith('floor_')), reverse=True)
+    for v, k in worst[:12]:
+        print(f'{k}: {v:.2e}')
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--ref', default='/root/reference')
+    ap.add_argument('--ref', default=os.environ.get('LCODE_REFERENCE'),
+                    help='reference checkout holding lcode.py (or LCODE_REFERENCE)')
     ap.add_argument('--which', default='all')
     ap.add_argument('--cfg2-steps', type=int, default=30)
+    ap.add_argument('--resume-dir', default=None,
+                    help='cfg2full: where to keep the resumable state of the run')
+    ap.add_argument('--out', default=None, help='cfg2full: output file')
     a = ap.parse_args()
+    full = os.path.join(HERE, 'run_n641_full.npz')
+    if a.which == 'cfg2floor':
+        # combine a serial and a reversed run (both written by cfg2full)
+        gen_cfg2_floor(full, a.out, full)
+        return
+    if not a.ref:
+        ap.error('--ref (or LCODE_REFERENCE) is required')
+    if a.which == 'cfg2full-reversed':
+        lc = load_reference(a.ref, reverse_deposit=True)
+        gen_cfg2_full(lc, a.out, a.resume_dir)
+        return
     lc = load_reference(a.ref)
     if a.which in ('all', 'stages'):
         gen_stages(lc, os.path.join(HERE, 'stages_n41.npz'))
@@ -389,6 +494,8 @@ def main():
         gen_cfg1(lc, os.path.join(HERE, 'run_n161.npz'))
     if a.which in ('all', 'cfg2'):
         gen_cfg2(lc, os.path.join(HERE, 'run_n641_head.npz'), a.cfg2_steps)
+    if a.which == 'cfg2full':
+        gen_cfg2_full(lc, a.out or full, a.resume_dir)
 
 
 if __name__ == '__main__':

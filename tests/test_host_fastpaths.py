@@ -48,3 +48,19 @@ def test_equal_configs_share_a_solver(fake):
     a = make_config(41, 0.1, 0.05, 10, amplitude=0.3)
     b = make_config(41, 0.1, 0.05, 10, amplitude=0.3)
     assert lcode.solver_for(a) is lcode.solver_for(b) and len(fake) == 1
+
+
+def test_const_copy_skipped_only_for_unwritten_same_arrays():
+    # Solver.set_const / set_virt copy again after an in-place write (a
+    # GPUArraysView assignment, t.copy_, t[...] = ...), not only after the
+    # arrays are replaced
+    a, b = torch.zeros(4, dtype=torch.float64), torch.ones(4, dtype=torch.float64)
+    seen = lcode.Solver._seen((a, b))
+    assert lcode.Solver._unchanged((a, b), seen)
+    assert not lcode.Solver._unchanged((a, b.clone()), seen)
+    b[1] = 5.0
+    assert not lcode.Solver._unchanged((a, b), seen)
+    seen = lcode.Solver._seen((a, b))
+    a.view(2, 2)[0].copy_(torch.ones(2, dtype=torch.float64))   # a write through a view
+    assert not lcode.Solver._unchanged((a, b), seen)
+    assert not lcode.Solver._unchanged((a, b), None)

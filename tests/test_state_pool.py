@@ -56,3 +56,32 @@ def test_ptrs_of_knows_only_unmodified_pool_states():
     class Other:
         pass
     assert pool.ptrs_of(Other()) is None
+
+
+def test_a_held_view_keeps_its_state():
+    # a 0-d view such as an Ez(0,0) history entry shares the state's memory
+    # without touching the reference counts of the state or its arrays
+    pool = lcode._StatePool()
+    s0 = take(pool)
+    s0.Ez.fill_(7.0)
+    v = s0.Ez[2, 2]
+    first = pool.entries[0]
+    del s0
+    for _ in range(2 * lcode._StatePool.SIZE):
+        s = take(pool)
+        assert s is not first[0]
+        s.Ez.fill_(-1.0)         # what the next step would write
+    assert float(v) == 7.0
+    del v
+    assert take(pool) is first[0]   # free again once the view is gone
+
+
+def test_a_slice_of_another_array_keeps_its_state():
+    pool = lcode._StatePool()
+    s0 = take(pool)
+    row = s0.x_offt[1]           # any array of the one allocation
+    first = pool.entries[0]
+    del s0
+    assert take(pool) is not first[0]
+    del row
+    assert take(pool) is first[0]
