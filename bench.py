@@ -176,6 +176,30 @@ def fp64_peak_tflops(torch):
     return 2 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def tf32_peak_tflops(torch):
+    """TF32 denominator measured in this run: cuBLAS float32 GEMM 8192^3 with
+    TF32 tensor cores allowed (best of 5); the measured-peaks file holds
+    no TF32 figure."""
+    n = 8192
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    a = torch.randn(n, n, dtype=torch.float32, device='cuda')
+    b = torch.randn(n, n, dtype=torch.float32, device='cuda')
+    torch.matmul(a, b)
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
 def transform_flops_per_launch(N):
     """Algorithmic flops of one batched transform-GEMM launch: the 4 launches
     of a solve apply L and R to each of the 6 fields (r x c with r, c in
@@ -219,6 +243,11 @@ def run_ours(args, rank, world, dist):
     cfg.lc3d_mixed_slices = args.slices
     N = cfg.grid_steps
     xs, ys, const, virt, st = L.init(cfg)
+    # the e2e loop's beams in pinned host memory, allocated first: pinning
+    # memory has side effects on the host that slow the steps that follow it
+    # for a while, which must not fall into a timed region
+    K, W = args.steps, args.warmup
+    pinned = [torch.from_numpy(beam_np(cfg, args.pre + i, xs, ys)).pin_memory() for i in range(W + K)]
     s = L.solver_for(cfg)
     s.set_virt(virt)
     s.set_const(const)
@@ -241,7 +270,6 @@ def run_ours(args, rank, world, dist):
     names = _lib.STATE_NAMES
     ptrs = _lib.StatePtrs(*[getattr(st, n).data_ptr() for n in names])
     _lib.check(lib.lc3d_set_state(s.ctx, ctypes.byref(ptrs), sp), 'set_state')
-    K, W = args.steps, args.warmup
     beams = [torch.from_numpy(beam_np(cfg, x0 + i, xs, ys)).cuda() for i in range(W + 2 * K)]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
     for i in range(W):
@@ -292,7 +320,6 @@ def run_ours(args, rank, world, dist):
 
     # ---- e2e through the public API, host beam in pinned memory ----
     st_e = st
-    pinned = [torch.from_numpy(beam_np(cfg, x0 + i, xs, ys)).pin_memory() for i in range(W + K)]
     L.lcode.check_errors = True   # the drop-in default: the device error flag is read after every call
     for i in range(W):
         st_e = L.step(cfg, const, virt, st_e, pinned[i])
@@ -303,9 +330,12 @@ def run_ours(args, rank, world, dist):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
     e0.record(stream)
+    wall = []
     for i in range(K):
+        ta = time.perf_counter()
         st_e = L.step(cfg, const, virt, st_e, pinned[W + i])
         float(st_e.Ez[N // 2, N // 2])   # D2H of the step's result
+        wall.append((time.perf_counter() - ta) * 1e3)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
@@ -345,13 +375,17 @@ def run_ours(args, rank, world, dist):
     hbm, hbm_src = peaks()
     roof = None
     use_fft = args.fp64_transform != 'dense'
-    if dom == 'transform' and stage[dom]['timed'] and args.precision == 'mixed':
+    if dom == 'transform' and stage[dom]['timed'] and args.precision in ('mixed', 'tf32'):
         avg_ms = stage[dom]['ms'] / stage[dom]['timed']
-        S = args.slices
+        S = args.slices or (4 if args.precision == 'mixed' else 3)
         fl = transform_flops_per_launch(N) * S * (S + 1) / 2
         ach = fl / (avg_ms * 1e-3) / 1e12
-        pk, src = tensor_peak()
-        roof = {'kernel': f'oz_gemm_kernel (tcgen05 split-BF16 transforms, {S} slices, {S * (S + 1) // 2} products)',
+        if args.precision == 'tf32':
+            pk, src = tf32_peak_tflops(torch), 'measured in this run: cuBLAS TF32 GEMM 8192^3 (no TF32 figure on file)'
+        else:
+            pk, src = tensor_peak()
+        kname = 'BF16' if args.precision == 'mixed' else 'TF32'
+        roof = {'kernel': f'oz_gemm_kernel (tcgen05 split-{kname} transforms, {S} slices, {S * (S + 1) // 2} products)',
                 'bound': 'tensor', 'achieved': ach, 'peak': pk, 'unit': 'TFLOP/s', 'frac': ach / pk,
                 'peak_source': src, 'algorithmic_per_launch': fl, 'avg_launch_ms': avg_ms, 'traffic': None}
     elif dom == 'transform' and stage[dom]['timed'] and (use_fft or args.precision == 'fft32'):
@@ -390,21 +424,23 @@ def run_ours(args, rank, world, dist):
         'metric': METRIC, 'value': value, 'unit': 'xi-steps/s', 'n_gpus': world,
         'steps': K, 'warmup': W, 'ms_per_step': total_ms / K, 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None,
-        'dtype': {'fp64': 'f64', 'mixed': 'f64+bf16', 'fft32': 'f64+f32'}[args.precision],
+        'dtype': {'fp64': 'f64', 'mixed': 'f64+bf16', 'fft32': 'f64+f32', 'tf32': 'f64+tf32'}[args.precision],
         'data': 'synthetic (generated cold uniform plasma + axisymmetric beam; no dataset)',
         'config': {'workload': f'LCODE 3D xi step, {N}x{N} grid, h={cfg.grid_step_size}, '
                                f'xi_step={cfg.xi_step_size}, coarseness 3 / fineness 2, A={GRIDS[N][2]}, '
                                f'{args.precision} field solvers',
                    'grid_steps': N, 'coarse_particles': s.Nc ** 2, 'fine_particles': s.Nf ** 2,
                    'precision': args.precision, 'fp64_transform': args.fp64_transform,
-                   'mixed_slices': args.slices if args.precision == 'mixed' else None,
+                   'mixed_slices': (args.slices or (4 if args.precision == 'mixed' else 3))
+                   if args.precision in ('mixed', 'tf32') else None,
                    'start_xi_step': x0,
                    'l2': 'flushed between timed steps (256 MiB write, outside the step events)',
                    'parallelism': f'replicas x{world}' if world > 1 else 'single GPU'},
         'e2e': {'value': world * K / (e2e_ms * 1e-3), 'unit': 'xi-steps/s',
                 'h2d_bytes_per_step': N * N * 8, 'd2h_bytes_per_step': 8 + 4,
                 'error_check': 'device error flag read after every step (lcode.check_errors = True, the default)',
-                'wall_ms': wall_ms, 'api': 'lcode3d_b200.step (drop-in for lcode.step)'},
+                'wall_ms': wall_ms, 'api': 'lcode3d_b200.step (drop-in for lcode.step)',
+                'step_wall_ms': {'min': min(wall), 'median': statistics.median(wall), 'max': max(wall)}},
         'gpu_launches': int(sum(launches)),
         'launches_per_step': sum(launches) / K,
         'stages_ms_per_step': {n: stage[n]['ms'] / K for n in stage},
@@ -458,9 +494,11 @@ def run_accuracy_table(args):
     N = args.grid
     marks = sorted(int(x) for x in args.accuracy_steps.split(','))
     steps = marks[-1]
-    forms = [('fp64', {})] + [(f, {}) for f in ('fft32', 'tf32') if f in args.forms.split(',')]
+    forms = [('fp64', {})] + [(f, {}) for f in ('fft32',) if f in args.forms.split(',')]
     forms += [(f'mixed_s{S}', {'lc3d_mixed_slices': S}) for S in (3, 4, 5)
               if f'mixed_s{S}' in args.forms.split(',')]
+    forms += [(f'tf32_s{S}', {'lc3d_mixed_slices': S}) for S in (2, 3)
+              if f'tf32_s{S}' in args.forms.split(',')]
     beams = None
     results, ref = {}, None
     for name, extra in forms:
@@ -547,10 +585,11 @@ def run_scan(args, rank, world, dist):
     specs = B.scan_specs(args.scan, args.seed)
     mine = B.partition(specs, world)[rank]
     grids = sorted({specs[i]['grid_steps'] for i in mine})
-    choice, timings = B.autotune_transform(grids, steps=4)
+    choice, timings = B.autotune(grids, steps=4)
     torch.cuda.synchronize()
     t_setup = time.perf_counter()
-    bt = B.Batch([specs[i] for i in mine], transform=choice)
+    bt = B.Batch([specs[i] for i in mine], transform={N: c['transform'] for N, c in choice.items()},
+                 tiles={N: (c['deposit_rows'], c['fft_ctas_per_sm']) for N, c in choice.items()})
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t_setup
     K, W = args.steps, args.warmup
@@ -702,9 +741,10 @@ def main():
     ap.add_argument('--steps', type=int, default=100)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--precision', default='fp64', choices=['fp64', 'mixed', 'fft32'])
+    ap.add_argument('--precision', default='fp64', choices=['fp64', 'mixed', 'fft32', 'tf32'])
     ap.add_argument('--fp64-transform', default='auto', choices=['auto', 'fft', 'dense'])
-    ap.add_argument('--slices', type=int, default=4, help='bf16 slices per operand (mixed precision)')
+    ap.add_argument('--slices', type=int, default=0,
+                    help='slices per operand of the tensor-core transforms (0: 4 for mixed, 3 for tf32)')
     ap.add_argument('--grid', type=int, default=641, choices=sorted(GRIDS))
     ap.add_argument('--pre', type=int, default=400, help='untimed steps into the beam')
     ap.add_argument('--cpu-steps', type=int, default=16, help='oracle steps for cpu_baseline')

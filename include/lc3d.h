@@ -50,6 +50,9 @@ extern "C" {
 #define LC3D_PREC_FP64 0        /* float64 solvers (transform form: fp64_transform) */
 #define LC3D_PREC_MIXED 1       /* split-BF16 tcgen05 transforms, fp32 accumulate,
                                    float64 combination; grid_steps <= 1000 */
+#define LC3D_PREC_TF32 3        /* split-TF32 tcgen05 transforms (kind::tf32, 10-bit
+                                   digits, fp32 accumulate, float64 combination);
+                                   mixed_slices digits per operand (default 3) */
 #define LC3D_PREC_FFT32 2       /* float32 FFT transforms (float32 intermediates and
                                    eigenvalues); right-hand sides, field outputs,
                                    averaging and particles stay float64; needs
@@ -275,6 +278,28 @@ int lc3d_profile_read(lc3d_ctx* ctx, long long* launches, double* ms, long long*
  * LC3D_OK, LC3D_ERR_WINDOW, LC3D_ERR_NONFINITE or LC3D_ERR_TIMEOUT. */
 int lc3d_check_error(lc3d_ctx* ctx, void* stream);
 
+/* Tile shapes of this context (no reference counterpart; the autotuner of
+ * lcode3d_b200.batch picks them per grid size). deposit_rows: fine-lattice
+ * rows per CTA of the deposition, 4, 8 or 16 (0: the default, 8); the CTA
+ * covers that many rows x 32 columns, and 8, 4 or 2 CTAs share an SM.
+ * fft_ctas_per_sm: resident CTAs per SM of the persistent FFT row passes
+ * (0: as many as fit). Results agree to rounding (the deposition's window
+ * sums are grouped by tile). Graphs of lc3d_run are re-captured with the
+ * new shapes; batches keep the shapes their contexts had when the batch
+ * was made. Returns LC3D_ERR_PARAM for other values. */
+int lc3d_set_tiles(lc3d_ctx* ctx, int deposit_rows, int fft_ctas_per_sm);
+
+/* Test hook of the failure detection; no reference counterpart (the
+ * reference has no bounded waits). Every wait in the tensor-core pipeline of
+ * the mixed-precision transforms is bounded: once `cycles` SM clock cycles
+ * have passed (cycles <= 0: the default, 2e9, one to two seconds) the kernel
+ * stops waiting, frees its tensor memory, raises the timeout flag
+ * (LC3D_ERR_TIMEOUT from lc3d_check_error) and returns, and the context
+ * stays usable. With skip_loads != 0 the pipeline's producer issues no
+ * loads, so the consumer's first wait runs out with no copy in flight; the
+ * fields such a call writes are undefined. Only tests of that path set it. */
+int lc3d_test_wait_limit(lc3d_ctx* ctx, long long cycles, int skip_loads);
+
 /* ---- deposition that allocates nothing ----
  *
  * No counterpart in the reference. For callers that cannot allocate device
@@ -294,8 +319,9 @@ int lc3d_check_error(lc3d_ctx* ctx, void* stream);
  * the kernel's shared-memory limit; make that first call before any stream
  * capture. Each call clears the scratch it uses first; calls that overlap
  * on the GPU (no ordering between their streams) race on the shared array.
- * Particles whose stencil leaves the grid are skipped as in lc3d_deposit,
- * but this entry point does not report them. */
+ * Particles whose stencil leaves the grid, and particles with non-finite or
+ * out-of-range deposit values, are skipped as in lc3d_deposit, but this
+ * entry point does not report them. */
 #define LC3D_NOALLOC_MAX_GRID 321
 int lc3d_deposit_noalloc(const lc3d_params* p, const double* ro_initial,
         const double* x_offt, const double* y_offt,

@@ -12,7 +12,7 @@ LIB_PATH = os.path.join(HERE, 'liblc3d.so')
 c_int, c_double, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
 OK, ERR_PARAM, ERR_CUDA, ERR_WINDOW, ERR_NONFINITE, ERR_STATE, ERR_SIZE, ERR_TIMEOUT = range(8)
-PREC_FP64, PREC_MIXED, PREC_FFT32 = 0, 1, 2
+PREC_FP64, PREC_MIXED, PREC_FFT32, PREC_TF32 = 0, 1, 2, 3
 FP64_AUTO, FP64_FFT, FP64_DENSE = 0, 1, 2
 
 
@@ -75,6 +75,8 @@ SIGNATURES = [
     ('lc3d_calculate_Ez', c_int, [P] * 5),
     ('lc3d_calculate_Bz', c_int, [P] * 5),
     ('lc3d_check_error', c_int, [P, P]),
+    ('lc3d_test_wait_limit', c_int, [P, ctypes.c_longlong, c_int]),
+    ('lc3d_set_tiles', c_int, [P, c_int, c_int]),
     ('lc3d_profile', c_int, [P, c_int]),
     ('lc3d_profile_read', c_int, [P, P, P, P]),
     ('lc3d_deposit_noalloc', c_int, [ctypes.POINTER(Params)] + [P] * 18),

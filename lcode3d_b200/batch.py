@@ -82,11 +82,13 @@ class Sim:
     cache of ``lcode``) with its plasma, ion background and initial state
     built on the device (lc3d_init_plasma)."""
 
-    def __init__(self, spec, precision='fp64', transform='auto', slices=0):
+    def __init__(self, spec, precision='fp64', transform='auto', slices=0, tiles=None):
         self.spec = spec
         self.config = make_config(spec, precision, transform, slices)
         L.init_config_checks(self.config)
         self.solver = L.Solver(L.params_of(self.config), L._device().index)
+        if tiles:
+            check(lib.lc3d_set_tiles(self.solver.ctx, int(tiles[0]), int(tiles[1])), 'lc3d_set_tiles')
         check(lib.lc3d_init_plasma(self.solver.ctx, L._stream()), 'lc3d_init_plasma')
         bp = _lib.BeamParams(spec['amplitude'], spec['sigma_r'], spec['length_factor'])
         check(lib.lc3d_set_beam(self.solver.ctx, ctypes.byref(bp)), 'lc3d_set_beam')
@@ -109,10 +111,14 @@ class Sim:
 class Batch:
     """Simulations advanced together by ``lc3d_batch_run``."""
 
-    def __init__(self, specs, precision='fp64', transform=None, slices=0):
+    def __init__(self, specs, precision='fp64', transform=None, slices=0, tiles=None):
+        """``transform``: one form or {N: form}; ``tiles``: {N: (deposit
+        rows, FFT CTAs per SM)} as lc3d_set_tiles takes them (both as
+        ``autotune`` returns them)."""
         transform = transform or {}
+        tiles = tiles or {}
         self.sims = [Sim(s, precision, transform.get(s['grid_steps'], 'auto') if isinstance(transform, dict)
-                         else transform, slices) for s in specs]
+                         else transform, slices, tiles.get(s['grid_steps'])) for s in specs]
         self._ctxs = (ctypes.c_void_p * len(self.sims))(*[s.solver.ctx.value for s in self.sims])
         self.handle = ctypes.c_void_p()
         check(lib.lc3d_batch_create(self._ctxs, len(self.sims), ctypes.byref(self.handle)), 'lc3d_batch_create')
@@ -140,30 +146,64 @@ class Batch:
             check(lib.lc3d_check_error(s.solver.ctx, L._stream()), 'batch simulation')
 
 
+def _time_sim(spec, precision, form, tiles, steps):
+    """ms per graph-replayed step of one simulation, or None if the form is
+    not available for this grid."""
+    try:
+        sim = Sim(spec, precision, form, tiles=tiles)
+    except _lib.LC3DError:
+        return None
+    ez = L._empty((steps,))
+    check(lib.lc3d_run(sim.solver.ctx, 0, 2, ctypes.c_void_p(ez.data_ptr()), L._stream()), 'warm')
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    check(lib.lc3d_run(sim.solver.ctx, 2, steps, ctypes.c_void_p(ez.data_ptr()), L._stream()), 'tune')
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+TILE_CHOICES = {'deposit_rows': (4, 8, 16), 'fft_ctas_per_sm': (0, 2)}
+
+
+def autotune(grids, steps=6, precision='fp64'):
+    """Pick, per grid size, the float64 transform form (FFT or dense) and
+    the tile shapes (deposition fine rows per CTA; resident FFT CTAs per SM,
+    0 = as many as fit) by timing a few graph-replayed steps of every
+    combination on this GPU. Returns ({N: {'transform', 'deposit_rows',
+    'fft_ctas_per_sm'}}, {N: {label: ms per step}})."""
+    choice, timings = {}, {}
+    for N in sorted(set(grids)):
+        spec = dict(grid_steps=N, grid_step_size=16.0 / (N - 1), xi_step_size=0.01, amplitude=0.5,
+                    sigma_r=1.0, length_factor=1.0)
+        timings[N] = {}
+        best = None
+        for form in ('fft', 'dense'):
+            for rows in TILE_CHOICES['deposit_rows']:
+                for per_sm in (TILE_CHOICES['fft_ctas_per_sm'] if form == 'fft' else (0,)):
+                    ms = _time_sim(spec, precision, form, (rows, per_sm), steps)
+                    if ms is None:
+                        continue
+                    timings[N][f'{form} rows={rows} fft_per_sm={per_sm}'] = ms
+                    if best is None or ms < best[0]:
+                        best = (ms, {'transform': form, 'deposit_rows': rows, 'fft_ctas_per_sm': per_sm})
+        choice[N] = best[1]
+    return choice, timings
+
+
 def autotune_transform(grids, steps=6, precision='fp64'):
-    """Pick the float64 transform form (FFT or dense) per grid size by timing
-    a few graph-replayed steps of each on this GPU. Returns
-    ({N: 'fft' | 'dense'}, {N: {form: ms per step}})."""
+    """The transform form part of ``autotune``: ({N: 'fft' | 'dense'},
+    {N: {form: ms per step}}) at the default tile shapes."""
     choice, timings = {}, {}
     for N in sorted(set(grids)):
         spec = dict(grid_steps=N, grid_step_size=16.0 / (N - 1), xi_step_size=0.01, amplitude=0.5,
                     sigma_r=1.0, length_factor=1.0)
         timings[N] = {}
         for form in ('fft', 'dense'):
-            try:
-                sim = Sim(spec, precision, form)
-            except _lib.LC3DError:
-                continue
-            ez = L._empty((steps,))
-            check(lib.lc3d_run(sim.solver.ctx, 0, 2, ctypes.c_void_p(ez.data_ptr()), L._stream()), 'warm')
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            check(lib.lc3d_run(sim.solver.ctx, 2, steps, ctypes.c_void_p(ez.data_ptr()), L._stream()), 'tune')
-            e1.record()
-            e1.synchronize()
-            timings[N][form] = e0.elapsed_time(e1) / steps
-            del sim
+            ms = _time_sim(spec, precision, form, None, steps)
+            if ms is not None:
+                timings[N][form] = ms
         choice[N] = min(timings[N], key=timings[N].get)
     return choice, timings
 

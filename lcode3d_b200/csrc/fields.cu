@@ -466,7 +466,7 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
         }
     }
     int bz_partials = 0;   // > 0: the FFT pass left this many Bz partial sums in c->red
-    if (c->p.precision == LC3D_PREC_MIXED) {
+    if (c->p.precision == LC3D_PREC_MIXED || c->p.precision == LC3D_PREC_TF32) {
         // four split-BF16 tensor-core GEMM stages (fields_mixed.cu)
         for (int stage = 0; stage < 4; ++stage) {
             MixedStageDesc d[6]{};

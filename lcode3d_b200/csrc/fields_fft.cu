@@ -489,6 +489,11 @@ int fft_init(lc3d_ctx* c) {
     c->fft_ok = fft_plan(P, rad) > 0 && fft_cta_smem_bytes(P, N, FFT_F64) <= 200 * 1024;
     if (!c->fft_ok) return LC3D_OK;
     LC3D_TRY(fft_prepare(P));
+    {
+        int dev = 0;
+        LC3D_CUDA_TRY(cudaGetDevice(&dev));
+        LC3D_CUDA_TRY(cudaDeviceGetAttribute(&c->fft_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
     LC3D_TRY((fft_grid_size<double, double, double>(P, N, &c->fft_grid[FFT_F64])));
     LC3D_TRY((fft_grid_size<float, double, float>(P, N, &c->fft_grid[FFT_F64_F32])));
     LC3D_TRY((fft_grid_size<float, float, float>(P, N, &c->fft_grid[FFT_F32])));
@@ -570,12 +575,15 @@ int fft_rows(lc3d_ctx* c, const FftRowsDesc* desc, int count, int types, cudaStr
     }
     if (!ctas) return LC3D_OK;
     b.ngroups = ctas;
+    if (types < 0 || types > 3) return LC3D_ERR_PARAM;
+    // resident CTAs per SM: as many as fit, or the tile setting's cap
+    int G = c->fft_grid[types];
+    if (c->fft_per_sm > 0) G = std::min(G, std::max(1, c->fft_per_sm * c->fft_sms));
     ProfScope ps(c, LC3D_STAGE_TRANSFORM, s);
     switch (types) {
-        case FFT_F64: return fft_launch<double, double, double>(b, c->fft_grid[FFT_F64], s);
-        case FFT_F64_F32: return fft_launch<float, double, float>(b, c->fft_grid[FFT_F64_F32], s);
-        case FFT_F32: return fft_launch<float, float, float>(b, c->fft_grid[FFT_F32], s);
-        case FFT_F32_F64: return fft_launch<float, float, double>(b, c->fft_grid[FFT_F32_F64], s);
-        default: return LC3D_ERR_PARAM;
+        case FFT_F64: return fft_launch<double, double, double>(b, G, s);
+        case FFT_F64_F32: return fft_launch<float, double, float>(b, G, s);
+        case FFT_F32: return fft_launch<float, float, float>(b, G, s);
+        default: return fft_launch<float, float, double>(b, G, s);
     }
 }

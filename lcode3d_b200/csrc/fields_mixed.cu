@@ -33,6 +33,15 @@
 //   3. U^T = (Z R)^T      A = Z       B^T = R^T     output transposed
 //   4. F = L U            A = L       B^T = U^T
 // The data operands are sliced by a row kernel before each stage.
+//
+// TF32 form (LC3D_PREC_TF32). The same pipeline with tcgen05.mma kind::tf32:
+// the digits are 10 bits wide, |d_0| <= 1024, |d_s| <= 512, each slice
+// d_s 2^-10(s+1) exact in tf32 (11-bit significand), stored as float32 (16
+// values per 64-byte row, K blocks of 16, two MMAs of K = 8 per row). A
+// level's products reach 2^20 units per k, so over K of several hundred
+// the FP32 accumulation is no longer exact: each stage carries the FP32
+// rounding of its sums (about 2^-24 sqrt(K) of the level's size) on top of
+// the truncation after S slices, ~2^-10S.
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -47,8 +56,12 @@
 
 namespace {
 
-constexpr int TM = 128, TN = 128, BK = 32;                     // tile and K block
-constexpr int TILE_BYTES = TM * BK * 2;                          // 8 KiB (A and B tiles alike)
+constexpr int TM = 128, TN = 128, BK = 32;                     // tile and K block (bf16 elements)
+constexpr int TILE_BYTES = TM * 64;                              // 8 KiB: 128 rows of 64 bytes (A and B alike)
+constexpr int KIND_BF16 = 0, KIND_TF32 = 1;
+
+// Elements of one 64-byte operand row: 32 bf16 or 16 tf32 (float32).
+__host__ __device__ constexpr int k_block(int kind) { return kind == KIND_TF32 ? 16 : 32; }
 constexpr int MAX_SLICES = 6;
 constexpr int GEMM_THREADS = 192;
 constexpr int NACC = 4;                                          // f32 accumulators, one per digit level
@@ -70,13 +83,27 @@ struct OzProb {
 
 struct OzBatch {
     OzProb p[6];
-    int count, S, stages;
+    int count, S, stages, kind;
     unsigned* err;
+    long long wait_limit;          // bound of every pipeline wait (SM clock cycles)
+    int skip_loads;                // timeout test only: the producer issues no loads
 };
 
 using namespace tc;
 
 constexpr uint32_t IDESC = idesc_bf16(TM, TN);
+// kind::tf32: A and B tf32 (format 2), f32 accumulator, both K-major.
+constexpr uint32_t IDESC_TF32 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                                ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
 
 __device__ __forceinline__ double pow2(int e) {
     return __longlong_as_double((long long)(e + 1023) << 52);   // exact for -1022 <= e <= 1023
@@ -85,7 +112,9 @@ __device__ __forceinline__ double pow2(int e) {
 // ---------------------------------------------------------------------------
 // The GEMM kernel
 // ---------------------------------------------------------------------------
+template <int KIND>
 __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_constant__ OzBatch b) {
+    constexpr int KB = k_block(KIND);   // K elements per 64-byte row
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int S = b.S, NS = b.stages;
@@ -105,7 +134,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
     const int t = (int)blockIdx.x - P.tile_start;
     const int m0 = (t / P.tiles_n) * TM, n0 = (t % P.tiles_n) * TN;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nkb = (P.K + BK - 1) / BK;
+    const int nkb = (P.K + KB - 1) / KB;
 
     if (threadIdx.x == 0) {
         s_fail = 0;
@@ -127,18 +156,20 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0) {
-        if (lane == 0) {   // ---- TMA producer ----
+        if (lane == 0 && !b.skip_loads) {   // ---- TMA producer ----
+            // (skip_loads: nothing is loaded, so no copy is in flight when
+            // the MMA issuer's wait for the first stage runs out)
             for (int kb = 0; kb < nkb; ++kb) {
                 const int st = kb % NS, round = kb / NS;
-                if (round > 0 && !mbar_wait(&empty[st], (round - 1) & 1)) {
+                if (round > 0 && !mbar_wait(&empty[st], (round - 1) & 1, b.wait_limit)) {
                     s_fail = 1;
                     break;
                 }
                 mbar_expect_tx(&full[st], 2u * S * TILE_BYTES);
                 for (int s = 0; s < S; ++s) {
-                    tma_load_2d(sA + ((size_t)st * S + s) * TILE_BYTES, &P.ta, &full[st], kb * BK,
+                    tma_load_2d(sA + ((size_t)st * S + s) * TILE_BYTES, &P.ta, &full[st], kb * KB,
                                 s * P.a_rows_pad + m0);
-                    tma_load_2d(sB + ((size_t)st * S + s) * TILE_BYTES, &P.tb, &full[st], kb * BK,
+                    tma_load_2d(sB + ((size_t)st * S + s) * TILE_BYTES, &P.tb, &full[st], kb * KB,
                                 s * P.b_rows_pad + n0);
                 }
             }
@@ -149,7 +180,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
             bool ok = true;
             for (int kb = 0; kb < nkb && ok; ++kb) {
                 const int st = kb % NS, round = kb / NS;
-                if (!mbar_wait(&full[st], round & 1)) {
+                if (!mbar_wait(&full[st], round & 1, b.wait_limit)) {
                     ok = false;
                     s_fail = 1;
                     break;
@@ -163,10 +194,13 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
                         const int lvl = min(s + u, NACC - 1);
                         const uint32_t acc = tmem + lvl * TN;
 #pragma unroll
-                        for (int kk = 0; kk < BK / 16; ++kk) {
+                        for (int kk = 0; kk < 2; ++kk) {   // two MMAs per 64-byte row: K = 16 bf16 or 8 tf32
                             const uint64_t ad = umma_desc_sw64(a_base + s * TILE_BYTES + kk * 32);
                             const uint64_t bd = umma_desc_sw64(b_base + u * TILE_BYTES + kk * 32);
-                            umma_bf16(acc, ad, bd, IDESC, ((fresh >> lvl) & 1u) ? 0u : 1u);
+                            if constexpr (KIND == KIND_TF32)
+                                umma_tf32(acc, ad, bd, IDESC_TF32, ((fresh >> lvl) & 1u) ? 0u : 1u);
+                            else
+                                umma_bf16(acc, ad, bd, IDESC, ((fresh >> lvl) & 1u) ? 0u : 1u);
                             fresh &= ~(1u << lvl);
                         }
                     }
@@ -178,7 +212,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
         const int quarter = warp & 3;
         const int row = quarter * 32 + lane;
         const int m = m0 + row;
-        const bool ok = mbar_wait(done, 0);
+        const bool ok = mbar_wait(done, 0, b.wait_limit);
         if (!ok) s_fail = 1;
         fence_after();
         if (ok) {
@@ -255,10 +289,10 @@ __device__ __forceinline__ int exponent_bound(double amax) {
 struct SliceArgs {
     const double* in[6];
     int ld[6], rows[6], K[6];
-    __nv_bfloat16* out[6];
+    void* out[6];                  // bf16 or float32 (tf32) slices
     int* e[6];
     int row_start[7];              // prefix over problems, in rows
-    int count, S, rows_pad, k_pad;
+    int count, S, rows_pad, k_pad, kind;
 };
 
 __global__ void __launch_bounds__(256) slice_rows_kernel(const __grid_constant__ SliceArgs a) {
@@ -277,7 +311,19 @@ __global__ void __launch_bounds__(256) slice_rows_kernel(const __grid_constant__
     if (lane == 0) a.e[q][r] = e;
     const double scale = pow2(-e);
     const size_t plane = (size_t)a.rows_pad * a.k_pad;
-    __nv_bfloat16* o = a.out[q] + (size_t)r * a.k_pad;
+    if (a.kind == KIND_TF32) {   // 10-bit digits, float32 storage (exact in tf32)
+        float* o = static_cast<float*>(a.out[q]) + (size_t)r * a.k_pad;
+        for (int k = lane; k < a.k_pad; k += 32) {
+            double v = k < K ? x[k] * scale : 0.0;   // |v| < 1
+            for (int s = 0; s < a.S; ++s) {
+                const double d = rint(v * 1024.0);       // digit, exact
+                v = v * 1024.0 - d;                      // exact remainder, |v| <= 1/2
+                o[s * plane + k] = (float)(d * pow2(-10 * (s + 1)));
+            }
+        }
+        return;
+    }
+    __nv_bfloat16* o = static_cast<__nv_bfloat16*>(a.out[q]) + (size_t)r * a.k_pad;
     for (int k = lane; k < a.k_pad; k += 32) {
         double v = k < K ? x[k] * scale : 0.0;   // |v| < 1
         for (int s = 0; s < a.S; ++s) {
@@ -297,24 +343,26 @@ __global__ void __launch_bounds__(256) slice_rows_kernel(const __grid_constant__
 namespace {
 
 struct MixedState {
-    int S, stages;
+    int S, stages, kind;
     int rows_pad, k_pad;           // common padded shape of every operand buffer
-    __nv_bfloat16* fixed[2];       // sliced S2 (M x M) and C (N x N)
+    void* fixed[2];                // sliced S2 (M x M) and C (N x N): bf16 or float32 (tf32)
     int* efixed[2];
-    __nv_bfloat16* data[6];        // per-field data slices
+    void* data[6];                 // per-field data slices
     int* edata[6];
     CUtensorMap map_fixed[2];
     CUtensorMap map_data[6];
 };
 
-int make_map(CUtensorMap* m, void* base, int S, int rows_pad, int k_pad) {
+int make_map(CUtensorMap* m, void* base, int S, int rows_pad, int k_pad, int kind) {
     auto enc = tc_get_encode();
     if (!enc) return LC3D_ERR_CUDA;
+    const int esize = kind == KIND_TF32 ? 4 : 2;
     cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)S * rows_pad};
-    cuuint64_t strides[1] = {(cuuint64_t)k_pad * 2};
-    cuuint32_t box[2] = {BK, TM};
+    cuuint64_t strides[1] = {(cuuint64_t)k_pad * esize};
+    cuuint32_t box[2] = {(cuuint32_t)k_block(kind), TM};   // 64-byte rows
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+    CUresult r = enc(m, kind == KIND_TF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                     base, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? LC3D_OK : LC3D_ERR_CUDA;
@@ -326,10 +374,14 @@ uint16_t bf16_bits(float f) {   // exact values only (digits times powers of two
     return (uint16_t)(u >> 16);
 }
 
-// Slice a float64 matrix on the host exactly like slice_rows_kernel.
-void slice_host(const std::vector<double>& A, int rows, int K, int S, int rows_pad, int k_pad,
-                std::vector<uint16_t>& out, std::vector<int>& e) {
-    out.assign((size_t)S * rows_pad * k_pad, 0);
+// Slice a float64 matrix on the host exactly like slice_rows_kernel (bf16
+// bits into out16, or float32 tf32 values into out32).
+void slice_host(const std::vector<double>& A, int rows, int K, int S, int rows_pad, int k_pad, int kind,
+                std::vector<uint16_t>& out16, std::vector<float>& out32, std::vector<int>& e) {
+    if (kind == KIND_TF32)
+        out32.assign((size_t)S * rows_pad * k_pad, 0.0f);
+    else
+        out16.assign((size_t)S * rows_pad * k_pad, 0);
     e.assign(rows_pad, 0);
     for (int r = 0; r < rows; ++r) {
         double amax = 0;
@@ -341,12 +393,18 @@ void slice_host(const std::vector<double>& A, int rows, int K, int S, int rows_p
             er = ex;
         }
         e[r] = er;
+        const int bits = kind == KIND_TF32 ? 10 : 7;
+        const double base = std::ldexp(1.0, bits);
         for (int k = 0; k < K; ++k) {
             double v = std::ldexp(A[(size_t)r * K + k], -er);
             for (int s = 0; s < S; ++s) {
-                const double d = std::nearbyint(v * 128.0);
-                v = v * 128.0 - d;
-                out[((size_t)s * rows_pad + r) * k_pad + k] = bf16_bits((float)std::ldexp(d, -7 * (s + 1)));
+                const double d = std::nearbyint(v * base);
+                v = v * base - d;
+                const size_t o = ((size_t)s * rows_pad + r) * k_pad + k;
+                if (kind == KIND_TF32)
+                    out32[o] = (float)std::ldexp(d, -bits * (s + 1));
+                else
+                    out16[o] = bf16_bits((float)std::ldexp(d, -bits * (s + 1)));
             }
         }
     }
@@ -354,14 +412,16 @@ void slice_host(const std::vector<double>& A, int rows, int K, int S, int rows_p
 
 }  // namespace
 
-int mixed_init(lc3d_ctx* c, int slices) {
+int mixed_init(lc3d_ctx* c, int slices, int tf32) {
     if (slices < 1 || slices > MAX_SLICES) return LC3D_ERR_PARAM;
     const int N = c->N, M = c->M;
-    if (N > 1000) return LC3D_ERR_SIZE;   // exactness of the leading product needs K * 128^2 < 2^24
+    if (!tf32 && N > 1000) return LC3D_ERR_SIZE;   // exactness of the leading bf16 product needs K 128^2 < 2^24
     MixedState* ms = new MixedState;
     memset(ms, 0, sizeof(*ms));
     c->mixed = ms;
     ms->S = slices;
+    ms->kind = tf32 ? KIND_TF32 : KIND_BF16;
+    const int esize = tf32 ? 4 : 2;
     ms->rows_pad = (N + ROWS_PAD_ALIGN - 1) / ROWS_PAD_ALIGN * ROWS_PAD_ALIGN;
     ms->k_pad = (N + 7) / 8 * 8;
     ms->stages = 200 * 1024 / (2 * slices * TILE_BYTES);
@@ -389,26 +449,30 @@ int mixed_init(lc3d_ctx* c, int slices) {
     const std::vector<double>* fx[2] = {&S2, &C};
     const int fdim[2] = {M, N};
     for (int q = 0; q < 2; ++q) {
-        std::vector<uint16_t> sl;
+        std::vector<uint16_t> sl16;
+        std::vector<float> sl32;
         std::vector<int> e;
-        slice_host(*fx[q], fdim[q], fdim[q], slices, ms->rows_pad, ms->k_pad, sl, e);
-        LC3D_CUDA_TRY(cudaMalloc(&ms->fixed[q], plane_elems * 2));
-        LC3D_CUDA_TRY(cudaMemcpy(ms->fixed[q], sl.data(), plane_elems * 2, cudaMemcpyHostToDevice));
+        slice_host(*fx[q], fdim[q], fdim[q], slices, ms->rows_pad, ms->k_pad, ms->kind, sl16, sl32, e);
+        const void* src = tf32 ? static_cast<const void*>(sl32.data()) : static_cast<const void*>(sl16.data());
+        LC3D_CUDA_TRY(cudaMalloc(&ms->fixed[q], plane_elems * esize));
+        LC3D_CUDA_TRY(cudaMemcpy(ms->fixed[q], src, plane_elems * esize, cudaMemcpyHostToDevice));
         LC3D_CUDA_TRY(cudaMalloc(&ms->efixed[q], ms->rows_pad * sizeof(int)));
         LC3D_CUDA_TRY(cudaMemcpy(ms->efixed[q], e.data(), ms->rows_pad * sizeof(int), cudaMemcpyHostToDevice));
-        LC3D_TRY(make_map(&ms->map_fixed[q], ms->fixed[q], slices, ms->rows_pad, ms->k_pad));
+        LC3D_TRY(make_map(&ms->map_fixed[q], ms->fixed[q], slices, ms->rows_pad, ms->k_pad, ms->kind));
     }
     for (int f = 0; f < 6; ++f) {
-        LC3D_CUDA_TRY(cudaMalloc(&ms->data[f], plane_elems * 2));
-        LC3D_CUDA_TRY(cudaMemset(ms->data[f], 0, plane_elems * 2));
+        LC3D_CUDA_TRY(cudaMalloc(&ms->data[f], plane_elems * esize));
+        LC3D_CUDA_TRY(cudaMemset(ms->data[f], 0, plane_elems * esize));
         LC3D_CUDA_TRY(cudaMalloc(&ms->edata[f], ms->rows_pad * sizeof(int)));
         LC3D_CUDA_TRY(cudaMemset(ms->edata[f], 0, ms->rows_pad * sizeof(int)));
-        LC3D_TRY(make_map(&ms->map_data[f], ms->data[f], slices, ms->rows_pad, ms->k_pad));
+        LC3D_TRY(make_map(&ms->map_data[f], ms->data[f], slices, ms->rows_pad, ms->k_pad, ms->kind));
     }
     // per-kernel limit: the largest pipeline any slice count uses (stages x
     // 2S tiles <= 200 KiB) plus alignment slack and barriers, so contexts
     // with different slice counts can coexist
-    LC3D_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<KIND_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       200 * 1024 + 1024 + 256));
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<KIND_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        200 * 1024 + 1024 + 256));
     return LC3D_OK;
 }
@@ -438,6 +502,7 @@ int mixed_stage(lc3d_ctx* c, const MixedStageDesc* d, int count, cudaStream_t s)
     SliceArgs sa{};
     memset(&sa, 0, sizeof(sa));
     sa.count = count;
+    sa.kind = ms->kind;
     sa.S = ms->S;
     sa.rows_pad = ms->rows_pad;
     sa.k_pad = ms->k_pad;
@@ -463,8 +528,11 @@ int mixed_stage(lc3d_ctx* c, const MixedStageDesc* d, int count, cudaStream_t s)
     memset(&b, 0, sizeof(b));
     b.count = count;
     b.S = ms->S;
+    b.kind = ms->kind;
     b.stages = ms->stages;
     b.err = c->err;
+    b.wait_limit = c->wait_limit > 0 ? c->wait_limit : WAIT_LIMIT;
+    b.skip_loads = c->skip_loads;
     int tiles = 0;
     for (int q = 0; q < count; ++q) {
         OzProb& p = b.p[q];
@@ -495,7 +563,10 @@ int mixed_stage(lc3d_ctx* c, const MixedStageDesc* d, int count, cudaStream_t s)
     }
     const size_t smem = (size_t)ms->stages * 2 * ms->S * TILE_BYTES + 1024 + 256;
     ProfScope ps(c, LC3D_STAGE_TRANSFORM, s);
-    oz_gemm_kernel<<<tiles, GEMM_THREADS, smem, s>>>(b);
+    if (ms->kind == KIND_TF32)
+        oz_gemm_kernel<KIND_TF32><<<tiles, GEMM_THREADS, smem, s>>>(b);
+    else
+        oz_gemm_kernel<KIND_BF16><<<tiles, GEMM_THREADS, smem, s>>>(b);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }

@@ -57,7 +57,8 @@ int check_params(const lc3d_params* p, int* Nc, int* Nf, double* rb) {
     if (!(p->grid_step_size > 0) || !(p->xi_step_size > 0)) return LC3D_ERR_PARAM;
     if (c < 1 || f < 1) return LC3D_ERR_PARAM;
     if (!(p->reflect_padding_steps > c + 1)) return LC3D_ERR_PARAM;       // lcode.py:944
-    if (p->precision != LC3D_PREC_FP64 && p->precision != LC3D_PREC_MIXED && p->precision != LC3D_PREC_FFT32)
+    if (p->precision != LC3D_PREC_FP64 && p->precision != LC3D_PREC_MIXED && p->precision != LC3D_PREC_FFT32 &&
+        p->precision != LC3D_PREC_TF32)
         return LC3D_ERR_PARAM;
     if (p->fp64_transform < LC3D_FP64_AUTO || p->fp64_transform > LC3D_FP64_DENSE) return LC3D_ERR_PARAM;
     if (p->mixed_slices < 0 || p->mixed_slices > 6) return LC3D_ERR_PARAM;
@@ -142,6 +143,8 @@ int deposit_into(lc3d_ctx* c, const double* ro_initial, const double* x, const d
     a.acc = c->acc;
     a.plane = c->acc_plane;
     a.Nc = c->Nc; a.Nf = c->Nf; a.N = c->N;
+    a.fine_off = deposit_fine_offset(c->p.plasma_fineness);
+    a.tile_rows = c->dep_rows;
     a.h = c->p.grid_step_size; a.inv_h = 1.0 / c->p.grid_step_size; a.sf = c->sf;
     a.err = c->err;
     DepositFinalizeArgs f{};
@@ -519,7 +522,9 @@ int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out) {
         c->use_fft = c->fft_ok && p->fp64_transform != LC3D_FP64_DENSE;
     }
     if (rc == LC3D_OK && p->precision == LC3D_PREC_MIXED)
-        rc = mixed_init(c, p->mixed_slices ? p->mixed_slices : 4);
+        rc = mixed_init(c, p->mixed_slices ? p->mixed_slices : 4, 0);
+    if (rc == LC3D_OK && p->precision == LC3D_PREC_TF32)
+        rc = mixed_init(c, p->mixed_slices ? p->mixed_slices : 3, 1);
 #undef LC3D_STEP
     if (rc == LC3D_OK && cudaDeviceSynchronize() != cudaSuccess) rc = LC3D_ERR_CUDA;
     if (rc != LC3D_OK) {
@@ -852,6 +857,28 @@ int lc3d_profile_read(lc3d_ctx* c, long long* launches, double* ms, long long* t
     }
     c->prof_used = 0;
     return c->prof_overflow ? LC3D_ERR_SIZE : LC3D_OK;
+}
+
+int lc3d_test_wait_limit(lc3d_ctx* c, long long cycles, int skip_loads) {
+    if (!c) return LC3D_ERR_PARAM;
+    DeviceGuard g(c->device);
+    LC3D_CUDA_TRY(cudaDeviceSynchronize());   // no replay of a graph holding the old bound is in flight
+    c->wait_limit = cycles > 0 ? cycles : 0;
+    c->skip_loads = skip_loads ? 1 : 0;
+    run_drop_graphs(c);                       // the bound is a kernel parameter inside them
+    return LC3D_OK;
+}
+
+int lc3d_set_tiles(lc3d_ctx* c, int deposit_rows, int fft_ctas_per_sm) {
+    if (!c) return LC3D_ERR_PARAM;
+    if (!(deposit_rows == 0 || deposit_rows == 4 || deposit_rows == 8 || deposit_rows == 16)) return LC3D_ERR_PARAM;
+    if (fft_ctas_per_sm < 0 || fft_ctas_per_sm > 64) return LC3D_ERR_PARAM;
+    DeviceGuard g(c->device);
+    LC3D_CUDA_TRY(cudaDeviceSynchronize());   // no replay of the old graphs is in flight
+    c->dep_rows = deposit_rows;
+    c->fft_per_sm = fft_ctas_per_sm;
+    run_drop_graphs(c);                       // the shapes are launch parameters inside them
+    return LC3D_OK;
 }
 
 int lc3d_check_error(lc3d_ctx* c, void* stream) {

@@ -94,6 +94,8 @@ struct DepositArgs {
     unsigned long long* acc;                                  // 8 planes of fixed-point words
     size_t plane;                                             // plane stride (>= N*N, 256-byte multiple)
     int Nc, Nf, N;
+    int fine_off;                                             // tile origin: fine_off particles before 0
+    int tile_rows;                                            // fine rows per CTA (4, 8, 16; 0: default)
     double h, inv_h, sf;
     unsigned* err;
 };
@@ -110,6 +112,7 @@ struct DepositFinalizeArgs {
 int launch_move_estimate(const EstimateArgs& a, cudaStream_t s);
 int launch_move_smart(const MoveArgs& a, cudaStream_t s);
 int launch_deposit_main(const DepositArgs& a, cudaStream_t s);
+int deposit_fine_offset(int fineness);
 int launch_deposit_finalize(const DepositFinalizeArgs& f, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
@@ -196,7 +199,7 @@ struct MixedStageDesc {
     const double* lam;                    // optional Lambda[m][n]
     int ldl;
 };
-int mixed_init(lc3d_ctx* ctx, int slices);
+int mixed_init(lc3d_ctx* ctx, int slices, int tf32);   // split-bf16 or split-tf32 transforms
 void mixed_free(lc3d_ctx* ctx);
 int mixed_stage(lc3d_ctx* ctx, const MixedStageDesc* d, int count, cudaStream_t s);
 // one-time per-device kernel attributes (shared-memory opt-ins)
@@ -253,6 +256,7 @@ struct lc3d_ctx {
     int fft_ok, use_fft;                  // FFT transforms available / selected
     double* fft_tw;                       // FFT twiddles, P complex
     int fft_grid[4];                      // persistent FFT grid per FftTypes instantiation
+    int fft_sms;                          // SMs of the device (the grid cap of lc3d_set_tiles)
     void* mixed;                          // mixed-precision solver state (fields_mixed.cu)
     // launch accounting / profiling
     long long launches[LC3D_NSTAGES];
@@ -268,10 +272,19 @@ struct lc3d_ctx {
     double beam_A, beam_sr, beam_lf;      // amplitude, sigma_r, length factor
     cudaGraphExec_t graph[2];             // one xi step from state parity 0 / 1
     long long graph_launches[2][LC3D_NSTAGES];
+    // bounded tensor-core pipeline waits (lc3d_test_wait_limit): limit in SM
+    // clock cycles (0: the default) and the timeout test's load skipping
+    long long wait_limit;
+    int skip_loads;
+    // tile shapes (lc3d_set_tiles): deposition fine rows per CTA (0: default)
+    // and resident FFT CTAs per SM (0: as many as fit)
+    int dep_rows;
+    int fft_per_sm;
 };
 
 // The xi-step schedule (lc3d_api.cu), and the run machinery (run.cu).
 int step_schedule(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& out, const double* beam,
                   cudaStream_t s);
 int run_init(lc3d_ctx* c);
+void run_drop_graphs(lc3d_ctx* c);       // graphs of lc3d_run (re-captured on the next run)
 void run_free(lc3d_ctx* c);

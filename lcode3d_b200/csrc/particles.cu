@@ -481,6 +481,336 @@ __global__ void __launch_bounds__(DEP_THREADS, 1024 / DEP_THREADS) deposit_kerne
     }
 }
 
+// ---------------------------------------------------------------------------
+// Deposition, second form (the default): the same exact fixed-point
+// accumulation and the same register patches of 2 x 2 fine particles as
+// deposit_kernel above, with three changes.
+//  * Coarse->fine mix in two separable passes (the equivalent formula noted
+//    beside the reference's make_plasma, lcode.py:554-556). Each warp holds
+//    one fine row fi of the tile; it first mixes the two coarse rows of fi,
+//        R[c] = inf_prev[fi] Q[prev_i][c] + inf_next[fi] Q[next_i][c],
+//    for every coarse column c its 32 fine columns use (7 quantities, a
+//    warp-private shared-memory table), and each lane then mixes two
+//    entries, Q = inf_prev[fj] R[prev_j] + inf_next[fj] R[next_j]: 14
+//    float64 operations and 8 shared loads instead of 32 operations and 16
+//    scattered global loads, with no CTA barrier. A tile whose columns span
+//    more than DEP2_CMAX coarse columns (other coarseness / fineness
+//    settings, or arbitrary virt_params) mixes per particle from global
+//    memory as deposit_kernel does.
+//  * Tiles start `a.fine_off` fine particles before the lattice origin. With
+//    an even fineness the lattice has two fine particles per cell and axis
+//    and the pairs (odd, even) of fine indices share a cell; an offset of 1
+//    makes every 2 x 2 block of an undisturbed lattice lie in one cell, so
+//    its patch is the 3 x 3 stencil (9 window entries and 36 products per
+//    field instead of 16 and 64).
+//  * Blocks whose particles lie in one cell take a 3 x 3 patch; the others
+//    the 4 x 4 patch of deposit_kernel.
+// The window fill keeps deposit_kernel's claims and barrier-separated steps
+// (9 or 16), so results do not depend on timing: every float64 sum has a
+// fixed order and the sums that cross CTAs are integer sums.
+// ---------------------------------------------------------------------------
+#ifndef LC3D_DEP2_CLOCKS
+#define LC3D_DEP2_CLOCKS 0
+#endif
+#ifndef LC3D_DEP2_ROWS
+#define LC3D_DEP2_ROWS 8                    // default fine rows per CTA (4, 8 or 16)
+#endif
+constexpr int DEP2_CMAX = 16;               // coarse columns one row table holds
+constexpr int DEP2_WC = 32;                 // window columns (cells); rows: 2 per fine row of the tile
+
+// Dynamic shared memory of a tile of `ti` fine rows x 32 columns.
+constexpr size_t dep2_smem(int ti) {
+    return (size_t)ti * DEP2_CMAX * 8 * sizeof(double)              // row tables
+           + (size_t)ti * 32 * (6 * sizeof(double) + sizeof(int))   // staging
+           + (size_t)4 * (2 * ti * DEP2_WC) * sizeof(double)        // window, 4 fields
+           + (size_t)(2 * ti * DEP2_WC) * sizeof(int);               // anchor claims
+}
+
+#if LC3D_DEP2_CLOCKS
+constexpr int DEP2_NCLK = 6;
+__device__ long long g_dep2_clocks[16384][DEP2_NCLK];
+#define DEP2_CLK(k)                                                                      \
+    do {                                                                                 \
+        if (threadIdx.x == 0) {                                                          \
+            const int cta = blockIdx.y * gridDim.x + blockIdx.x;                         \
+            if (cta < 16384) g_dep2_clocks[cta][k] = clock64() - clk0;                   \
+        }                                                                                \
+    } while (0)
+#else
+#define DEP2_CLK(k) do { } while (0)
+#endif
+
+// Two of the seven coarse quantities of coarse particle k as a pair: h = 0
+// (x_offt, y_offt), 1 (m, q), 2 (px, py), 3 (pz, 0).
+__device__ __forceinline__ double2 coarse_pair(const DepositArgs& a, int k, int h) {
+    if (a.packed) return __ldg(reinterpret_cast<const double2*>(a.packed) + 4 * (size_t)k + h);
+    switch (h) {
+        case 0: return make_double2(__ldg(a.x_offt + k), __ldg(a.y_offt + k));
+        case 1: return make_double2(__ldg(a.m + k), __ldg(a.q + k));
+        case 2: return make_double2(__ldg(a.px + k), __ldg(a.py + k));
+        default: return make_double2(__ldg(a.pz + k), 0.0);
+    }
+}
+
+// TI fine rows x 32 fine columns per CTA, one warp per row (TI = 4, 8, 16:
+// 8, 4 or 2 resident CTAs per SM at 64 registers).
+template <int TI>
+__global__ void __launch_bounds__(TI * 32, 1024 / (TI * 32)) deposit_kernel2(DepositArgs a) {
+    constexpr int DEP2_TI = TI;
+    constexpr int DEP2_THREADS = DEP2_TI * 32;
+    constexpr int DEP2_BLOCKS = DEP2_THREADS / 4;
+    constexpr int DEP2_WR = 2 * DEP2_TI;   // window rows (cells)
+    constexpr int DEP2_WIN = DEP2_WR * DEP2_WC;
+    static_assert(DEP2_TI % 2 == 0 && DEP2_TI <= 32, "2 x 2 blocks, at most 32 warps");
+#if LC3D_DEP2_CLOCKS
+    const long long clk0 = clock64();
+#endif
+    extern __shared__ double smem_f64[];
+    double2* s_R = reinterpret_cast<double2*>(smem_f64);                 // [DEP2_TI][DEP2_CMAX][4]
+    double* s_xl = smem_f64 + DEP2_TI * DEP2_CMAX * 8;                   // [DEP2_THREADS]
+    double* s_yl = s_xl + DEP2_THREADS;
+    double* s_v = s_yl + DEP2_THREADS;                                   // [4][DEP2_THREADS]
+    double* s_win = s_v + 4 * DEP2_THREADS;                              // [4][DEP2_WIN]
+    int* s_claim = reinterpret_cast<int*>(s_win + 4 * DEP2_WIN);         // [DEP2_WIN]
+    int* s_cell = s_claim + DEP2_WIN;                                    // [DEP2_THREADS]: i << 16 | j, or -1
+    __shared__ int s_bb[4];                                              // imin imax jmin jmax
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (t == 0) {
+        s_bb[0] = s_bb[2] = 1 << 30;
+        s_bb[1] = s_bb[3] = -(1 << 30);
+    }
+    for (int w = t; w < 4 * DEP2_WIN; w += DEP2_THREADS) s_win[w] = 0.0;
+    for (int w = t; w < DEP2_WIN; w += DEP2_THREADS) s_claim[w] = -1;
+    const int N = a.N;
+    const size_t NN = a.plane;
+    pdl_wait();   // global memory from here on
+    DEP2_CLK(0);
+
+    // ---- phase 1: one fine particle per thread; warp = fine row ----
+    {
+        const int fi = (int)blockIdx.y * DEP2_TI + warp - a.fine_off;
+        const int fj = (int)blockIdx.x * 32 + lane - a.fine_off;
+        const bool row_ok = fi >= 0 && fi < a.Nf, col_ok = fj >= 0 && fj < a.Nf;
+        // every input of the particle first (independent loads), then the
+        // coarse rows of the row table
+        int pi = 0, ni = 0, pj = 0, nj = 0;
+        double ipi = 0, ini = 0, fgi = 0, ipj = 0, inj = 0, fgj = 0;
+        if (row_ok) {
+            pi = a.idx_prev[fi];
+            ni = a.idx_next[fi];
+            ipi = a.inf_prev[fi];
+            ini = a.inf_next[fi];
+            fgi = a.fine_grid[fi];
+        }
+        if (col_ok) {
+            pj = a.idx_prev[fj];
+            nj = a.idx_next[fj];
+            ipj = a.inf_prev[fj];
+            inj = a.inf_next[fj];
+            fgj = a.fine_grid[fj];
+        }
+        const bool row_idx = pi >= 0 && pi < a.Nc && ni >= 0 && ni < a.Nc;
+        const bool col_idx = pj >= 0 && pj < a.Nc && nj >= 0 && nj < a.Nc;
+        // the coarse columns of the tile (the same in every warp)
+        const int c0 = __reduce_min_sync(0xffffffffu, col_ok ? (col_idx ? min(pj, nj) : -(1 << 30)) : 1 << 30);
+        const int c1 = __reduce_max_sync(0xffffffffu, col_ok ? (col_idx ? max(pj, nj) : 1 << 30) : -(1 << 30));
+        const int nc = c1 - c0 + 1;
+        const bool staged = c0 >= 0 && nc >= 1 && nc <= DEP2_CMAX;
+        double2* R = s_R + warp * DEP2_CMAX * 4;
+        if (staged && row_ok && row_idx) {
+            for (int it = lane; it < nc * 4; it += 32) {
+                const int jc = it >> 2, h = it & 3;
+                const double2 qp = coarse_pair(a, pi * a.Nc + c0 + jc, h);
+                const double2 qn = coarse_pair(a, ni * a.Nc + c0 + jc, h);
+                R[it] = make_double2(ipi * qp.x + ini * qn.x, ipi * qp.y + ini * qn.y);
+            }
+        }
+        __syncwarp();
+        int cell = -1, i = 1 << 30, j = 1 << 30;
+        if (row_ok && col_ok) {
+            if (!(row_idx && col_idx)) {
+                atomicOr(a.err, LC3D_FLAG_WINDOW);
+            } else {
+                FineParticle f;
+                if (staged) {
+                    const double2* Rp = R + (pj - c0) * 4;
+                    const double2* Rn = R + (nj - c0) * 4;
+                    double2 q[4];
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) {
+                        const double2 rp = Rp[h], rn = Rn[h];
+                        q[h] = make_double2(ipj * rp.x + inj * rn.x, ipj * rp.y + inj * rn.y);
+                    }
+                    f.x = fgi + q[0].x;
+                    f.y = fgj + q[0].y;
+                    particle_values(f, a.sf * q[1].x, a.sf * q[1].y, a.sf * q[2].x, a.sf * q[2].y,
+                                    a.sf * q[3].x);
+                } else {
+                    f = fine_particle(a, fi, fj);
+                }
+                double xl, yl;
+                tsc_cell(f.x, f.y, N, a.h, a.inv_h, i, j, xl, yl);
+                const double vmax = fmax(fmax(fabs(f.dro), fabs(f.djx)), fmax(fabs(f.djy), fabs(f.djz)));
+                if (!(i >= 1 && i <= N - 2 && j >= 1 && j <= N - 2)) {
+                    atomicOr(a.err, LC3D_FLAG_WINDOW);
+                } else if (!(vmax < FX_MAX)) {   // also catches NaN
+                    atomicOr(a.err, LC3D_FLAG_NONFINITE);
+                } else {
+                    cell = (i << 16) | j;
+                }
+                s_xl[t] = xl;
+                s_yl[t] = yl;
+                s_v[t] = f.dro;
+                s_v[DEP2_THREADS + t] = f.djx;
+                s_v[2 * DEP2_THREADS + t] = f.djy;
+                s_v[3 * DEP2_THREADS + t] = f.djz;
+            }
+        }
+        s_cell[t] = cell;
+        // warp bounding box of the cells (one redux instruction each)
+        const int imin = __reduce_min_sync(0xffffffffu, cell >= 0 ? i : 1 << 30);
+        const int imax = __reduce_max_sync(0xffffffffu, cell >= 0 ? i : -(1 << 30));
+        const int jmin = __reduce_min_sync(0xffffffffu, cell >= 0 ? j : 1 << 30);
+        const int jmax = __reduce_max_sync(0xffffffffu, cell >= 0 ? j : -(1 << 30));
+        __syncthreads();   // s_bb initialised, window and claims cleared
+        if (lane == 0 && imin <= imax) {
+            atomicMin(&s_bb[0], imin);
+            atomicMax(&s_bb[1], imax);
+            atomicMin(&s_bb[2], jmin);
+            atomicMax(&s_bb[3], jmax);
+        }
+    }
+    __syncthreads();
+    DEP2_CLK(1);
+
+    // ---- phase 2: one (2 x 2 block, field) per thread ----
+    const int f = t / DEP2_BLOCKS, blk = t % DEP2_BLOCKS;
+    const int p0 = (blk >> 4) * 64 + (blk & 15) * 2;   // top-left particle of the block
+    const int pidx[4] = {p0, p0 + 1, p0 + 32, p0 + 33};
+    int ci[4], cj[4];
+    bool ok[4];
+    int i0 = 1 << 30, i1 = -(1 << 30), j0 = 1 << 30, j1 = -(1 << 30);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int c = s_cell[pidx[p]];
+        ok[p] = c >= 0;
+        ci[p] = c >> 16;
+        cj[p] = c & 0xffff;
+        if (ok[p]) {
+            i0 = min(i0, ci[p]);
+            i1 = max(i1, ci[p]);
+            j0 = min(j0, cj[p]);
+            j1 = max(j1, cj[p]);
+        }
+    }
+    const int oi = s_bb[0] - 1, oj = s_bb[2] - 1;   // window origin (cells)
+    const bool patch = i0 <= i1 && i1 - i0 <= 1 && j1 - j0 <= 1 && i0 + 2 - oi < DEP2_WR && j0 + 2 - oj < DEP2_WC;
+    const bool one = patch && i1 == i0 && j1 == j0;   // all four in one cell: a 3 x 3 patch
+    const int ar = i0 - 1, ac = j0 - 1;             // the patch's corner cell
+    const int r0 = ar - oi, c0w = ac - oj;          // ... in window coordinates
+    if (patch && f == 0) atomicMax(&s_claim[r0 * DEP2_WC + c0w], blk);
+    __syncthreads();
+    const bool winner = patch && s_claim[r0 * DEP2_WC + c0w] == blk;
+    unsigned long long* ghi = a.acc + (2 * f) * NN;
+    unsigned long long* glo = ghi + NN;
+    const double* vf = s_v + f * DEP2_THREADS;
+    double acc[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) acc[k] = 0.0;
+    if (one) {
+        // the four stencils on the same 3 x 3 cells: entry (r, c) of the
+        // patch is acc[r * 4 + c], r, c < 3
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (!ok[p]) continue;
+            double wx[3], wy[3];
+            tsc_axis(s_xl[pidx[p]], wx[0], wx[1], wx[2]);
+            tsc_axis(s_yl[pidx[p]], wy[0], wy[1], wy[2]);
+            const double v = vf[pidx[p]];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const double vx = v * wx[r];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) acc[r * 4 + c] = fma(vx, wy[c], acc[r * 4 + c]);
+            }
+        }
+    } else if (patch) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (!ok[p]) continue;
+            double wxM, wx0, wxP, wyM, wy0, wyP;
+            tsc_axis(s_xl[pidx[p]], wxM, wx0, wxP);
+            tsc_axis(s_yl[pidx[p]], wyM, wy0, wyP);
+            const bool si = ci[p] != i0, sj = cj[p] != j0;
+            const double wx4[4] = {si ? 0.0 : wxM, si ? wxM : wx0, si ? wx0 : wxP, si ? wxP : 0.0};
+            const double wy4[4] = {sj ? 0.0 : wyM, sj ? wyM : wy0, sj ? wy0 : wyP, sj ? wyP : 0.0};
+            const double v = vf[pidx[p]];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const double vx = v * wx4[r];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r * 4 + c] = fma(vx, wy4[c], acc[r * 4 + c]);
+            }
+        }
+    } else {
+#pragma unroll 1
+        for (int p = 0; p < 4; ++p) {
+            const int c = s_cell[pidx[p]];
+            if (c < 0) continue;
+            const int pi = c >> 16, pj = c & 0xffff;
+            double wx[3], wy[3];
+            tsc_axis(s_xl[pidx[p]], wx[0], wx[1], wx[2]);
+            tsc_axis(s_yl[pidx[p]], wy[0], wy[1], wy[2]);
+            const double v = vf[pidx[p]];
+#pragma unroll
+            for (int di = 0; di < 3; ++di)
+#pragma unroll
+                for (int dj = 0; dj < 3; ++dj)
+                    fx_add(ghi, glo, (size_t)(pi + di - 1) * N + (pj + dj - 1), v * (wx[di] * wy[dj]));
+        }
+    }
+    if (patch && !winner) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (acc[r * 4 + c] != 0.0) fx_add(ghi, glo, (size_t)(ar + r) * N + (ac + c), acc[r * 4 + c]);
+    }
+    DEP2_CLK(2);
+    // winners add their patches, one entry per barrier-separated step; a
+    // CTA whose blocks all lie in single cells needs only the 9 entries of
+    // a 3 x 3 patch
+    double* fw = s_win + f * DEP2_WIN + (winner ? r0 * DEP2_WC + c0w : 0);
+    if (__syncthreads_or(patch && !one)) {   // uniform over the CTA
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            if (winner && acc[k] != 0.0) fw[(k >> 2) * DEP2_WC + (k & 3)] += acc[k];
+            __syncthreads();
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+            const int k = (e / 3) * 4 + e % 3;
+            if (winner && acc[k] != 0.0) fw[(k >> 2) * DEP2_WC + (k & 3)] += acc[k];
+            __syncthreads();
+        }
+    }
+    DEP2_CLK(3);
+
+    // ---- phase 3: split each touched window cell once, add to global ----
+    if (s_bb[0] <= s_bb[1]) {
+        const int ni = min(s_bb[1] + 2 - oi, DEP2_WR), nj = min(s_bb[3] + 2 - oj, DEP2_WC);
+        const int cells = ni * nj;
+        for (int w = t; w < 4 * cells; w += DEP2_THREADS) {
+            const int q = w / cells, rc = w - q * cells, r = rc / nj, c = rc - r * nj;
+            const double v = s_win[q * DEP2_WIN + r * DEP2_WC + c];
+            if (v != 0.0)
+                fx_add(a.acc + (2 * q) * NN, a.acc + (2 * q + 1) * NN, (size_t)(oi + r) * N + (oj + c), v);
+        }
+    }
+    DEP2_CLK(4);
+}
+
 // Accumulators -> float64 (+ ion background), two cells per thread; the
 // accumulators are cleared for the next deposition. All eight 16-byte
 // accumulator loads of a thread are issued before any store (the clears
@@ -561,18 +891,58 @@ int launch_move_smart(const MoveArgs& a, cudaStream_t s) {
     return LC3D_OK;
 }
 
+#ifndef LC3D_DEP_V2
+#define LC3D_DEP_V2 1
+#endif
+
 int particles_prepare() {
     LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DEP_SMEM));
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel2<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(4)));
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel2<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(8)));
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel2<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(16)));
     return LC3D_OK;
+}
+
+// Tile origin of the deposition: with an even fineness the fine lattice
+// (lcode.py:468-487) puts two particles per cell and axis, and the pairs of
+// fine indices (odd, even) share a cell, so tiles start one particle early.
+int deposit_fine_offset(int fineness) {
+#ifdef LC3D_DEP2_FORCE_OFF
+    (void)fineness;
+    return LC3D_DEP2_FORCE_OFF;
+#else
+    return fineness % 2 == 0 ? 1 : 0;
+#endif
 }
 
 int launch_deposit_main(const DepositArgs& a, cudaStream_t s) {
     if (a.Nf <= 0) return LC3D_OK;
     dim3 grid((a.Nf + DEP_TJ - 1) / DEP_TJ, (a.Nf + DEP_TI - 1) / DEP_TI);
+#if LC3D_DEP_V2
+    const int ti = a.tile_rows ? a.tile_rows : LC3D_DEP2_ROWS;
+    const dim3 grid2((a.Nf + a.fine_off + 31) / 32, (a.Nf + a.fine_off + ti - 1) / ti);
+    switch (ti) {
+        case 4: LC3D_CUDA_TRY(launch_pdl(deposit_kernel2<4>, grid2, dim3(4 * 32), dep2_smem(4), s, a)); break;
+        case 8: LC3D_CUDA_TRY(launch_pdl(deposit_kernel2<8>, grid2, dim3(8 * 32), dep2_smem(8), s, a)); break;
+        case 16: LC3D_CUDA_TRY(launch_pdl(deposit_kernel2<16>, grid2, dim3(16 * 32), dep2_smem(16), s, a)); break;
+        default: return LC3D_ERR_PARAM;
+    }
+#else
     LC3D_CUDA_TRY(launch_pdl(deposit_kernel, grid, dim3(DEP_THREADS), DEP_SMEM, s, a));
+#endif
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
+
+#if LC3D_DEP2_CLOCKS
+// Instrumented builds only: phase clocks of the last deposit_kernel2 launch,
+// [16384][DEP2_NCLK] cycles since each CTA's start.
+extern "C" int lc3d_debug_dep_clocks(long long* host) {
+    LC3D_CUDA_TRY(cudaDeviceSynchronize());
+    LC3D_CUDA_TRY(cudaMemcpyFromSymbol(host, g_dep2_clocks, sizeof(g_dep2_clocks)));
+    return LC3D_OK;
+}
+#endif
 
 int launch_deposit_finalize(const DepositFinalizeArgs& f_in, cudaStream_t s) {
     DepositFinalizeArgs f = f_in;
@@ -673,6 +1043,7 @@ extern "C" int lc3d_deposit_noalloc(const lc3d_params* p, const double* ro_initi
     a.acc = scratch;
     a.plane = plane;
     a.Nc = Nc; a.Nf = Nf; a.N = N;
+    a.fine_off = deposit_fine_offset(p->plasma_fineness);
     a.h = p->grid_step_size;
     a.inv_h = 1.0 / p->grid_step_size;
     a.sf = 1.0 / ((double)(c * f) * (c * f));

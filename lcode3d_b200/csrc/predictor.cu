@@ -46,6 +46,7 @@
 
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -71,6 +72,7 @@ struct ConvArgs {
     CUtensorMap twt;               // [9 Cout][Cin] bf16, box (32, Cout)
     const float* bias;             // [Cout]
     void* out;                     // [H Wp][Cout], bf16 or f32
+    const __nv_bfloat16* mask;     // [H Wp][Cout] or NULL: zero the outputs where mask <= 0
     int out_f32, relu;
     int H, W, Wp, NP, Cin, Cout;
     uint32_t idesc;
@@ -165,6 +167,14 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) conv3x3_tc_kernel(const __gri
                     v[j] = pad ? 0.0f : t;
                 }
                 if (!live) continue;
+                if (a.mask) {   // adjoint of a ReLU: the gradient passes where the activation is positive
+                    const uint4* mp = reinterpret_cast<const uint4*>(a.mask + (size_t)p * a.Cout + c0);
+                    const uint4 mw[2] = {__ldg(mp), __ldg(mp + 1)};
+                    const __nv_bfloat16* mb = reinterpret_cast<const __nv_bfloat16*>(mw);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (!(__bfloat162float(mb[j]) > 0.0f)) v[j] = 0.0f;
+                }
                 if (a.out_f32) {
                     float4* o = reinterpret_cast<float4*>(static_cast<float*>(a.out) + (size_t)p * a.Cout + c0);
 #pragma unroll
@@ -446,6 +456,36 @@ __global__ void loss_kernel(const float* __restrict__ y, const float* __restrict
 }
 
 // ---------------------------------------------------------------------------
+// Backward data pass on the tensor cores. dL/dx of a 3x3 convolution is the
+// 3x3 convolution of the output gradient g with the flipped, transposed
+// weights, W'[tap][ci][co] = W[8 - tap][co][ci] (tap 8 - t is the opposite
+// shift of tap t), so conv3x3_tc_kernel computes it: g is rounded to bf16
+// (its channels padded with zeros to a multiple of 32, zero in the pad
+// column), the accumulation is f32 in TMEM, and the epilogue applies the
+// ReLU adjoint of the layer's input.
+// ---------------------------------------------------------------------------
+
+// out[p][c] = bf16(g[p][c]) for c < CG and real pixels; 0 for c >= CG and
+// in the pad column.
+__global__ void grad_to_bf16_kernel(const float* __restrict__ g, int CG, __nv_bfloat16* __restrict__ out, int CGp,
+                                    Level L) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)L.NP * CGp) return;
+    const int p = (int)(t / CGp), c = (int)(t - (long long)p * CGp);
+    const bool pad = (p % L.Wp) >= L.W;
+    out[t] = __float2bfloat16_rn(!pad && c < CG ? g[(size_t)p * CG + c] : 0.0f);
+}
+
+// wt[tap][ci][co] = w[8 - tap][co][ci] (co < CG), 0 for CG <= co < CGp.
+__global__ void flip_weights_kernel(const __nv_bfloat16* __restrict__ w, int CG, int CIN, int CGp,
+                                    __nv_bfloat16* __restrict__ wt) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 9 * CIN * CGp) return;
+    const int tap = t / (CIN * CGp), rem = t - tap * CIN * CGp, ci = rem / CGp, co = rem - ci * CGp;
+    wt[t] = co < CG ? w[((size_t)(8 - tap) * CG + co) * CIN + ci] : __float2bfloat16_rn(0.0f);
+}
+
+// ---------------------------------------------------------------------------
 // Training kernels (float32)
 // ---------------------------------------------------------------------------
 constexpr int BWD_THREADS = 256;
@@ -684,6 +724,14 @@ struct lc3d_predictor {
     // gradients (float32 NHWC)
     float *g_out = nullptr, *g_d1 = nullptr, *g_u2 = nullptr, *g_d2 = nullptr, *g_u3 = nullptr, *g_e3 = nullptr,
           *g_p2 = nullptr, *g_p1 = nullptr;
+    // tensor-core backward data pass: the bf16 output gradient of the layer
+    // in hand, the flipped transposed bf16 weights of every layer, zeros for
+    // the bias, and the convolution arguments of each layer's pass
+    __nv_bfloat16* g_bf = nullptr;
+    __nv_bfloat16* wt = nullptr;
+    long long wt_off[NLAYERS];
+    float* zero_bias = nullptr;
+    ConvArgs bconv[NLAYERS];
     unsigned* err = nullptr;
     double* scale = nullptr;       // [23] per-sample channel scales (device)
     double* partial = nullptr;     // [STAT_BLOCKS][18]
@@ -729,6 +777,42 @@ int run_conv(lc3d_predictor* P, int l, cudaStream_t s) {
     return LC3D_OK;
 }
 
+// Output-gradient channels of layer l as the tensor-core pass reads them.
+int grad_channels(int l) { return LAYERS[l].cout < KB ? KB : LAYERS[l].cout; }
+
+int setup_bconv(lc3d_predictor* P, int l) {
+    const LayerDef& d = LAYERS[l];
+    const Level& L = P->lv[d.level];
+    const int CGp = grad_channels(l);
+    ConvArgs& a = P->bconv[l];
+    memset(&a, 0, sizeof(a));
+    LC3D_TRY(make_map_2d(&a.tin, P->g_bf, L.NP, CGp, TILE_PIX));
+    LC3D_TRY(make_map_2d(&a.twt, P->wt + P->wt_off[l], 9LL * d.cin, CGp, d.cin));
+    a.bias = P->zero_bias;
+    a.out_f32 = 1;
+    a.relu = 0;
+    a.H = L.H; a.W = L.W; a.Wp = L.Wp; a.NP = L.NP;
+    a.Cin = CGp; a.Cout = d.cin;
+    a.idesc = idesc_bf16(TILE_PIX, d.cin);
+    a.err = P->err;
+    return LC3D_OK;
+}
+
+// dx = dL/d(input of layer l) from g = dL/d(output), zeroed where mask <= 0.
+int bwd_data_tc(lc3d_predictor* P, int l, const float* g, const __nv_bfloat16* mask, float* dx, cudaStream_t s) {
+    const LayerDef& d = LAYERS[l];
+    const Level& L = P->lv[d.level];
+    const int CGp = grad_channels(l);
+    grad_to_bf16_kernel<<<blocks_for((long long)L.NP * CGp, 256), 256, 0, s>>>(g, d.cout, P->g_bf, CGp, L);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    ConvArgs a = P->bconv[l];
+    a.out = dx;
+    a.mask = mask;
+    conv3x3_tc_kernel<<<blocks_for(a.NP, TILE_PIX), CONV_THREADS, conv_smem_bytes(), s>>>(a);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
 template <int CIN>
 int bwd_data(const float* g, int CG, const __nv_bfloat16* w, const __nv_bfloat16* mask, float* dx, const Level& L,
              cudaStream_t s) {
@@ -768,29 +852,47 @@ int forward(lc3d_predictor* P, cudaStream_t s) {
     return LC3D_OK;
 }
 
+#ifndef LC3D_PRED_BWD_TC
+#define LC3D_PRED_BWD_TC 1                  // backward data pass on the tensor cores (else float32 SIMT)
+#endif
+
 int backward(lc3d_predictor* P, float* loss, cudaStream_t s) {
     const Level &l0 = P->lv[0], &l1 = P->lv[1], &l2 = P->lv[2];
     const __nv_bfloat16* w = P->wbf;
+    (void)w;
     LC3D_CUDA_TRY(cudaMemsetAsync(P->grad, 0, (size_t)P->np * sizeof(float), s));
+#if LC3D_PRED_BWD_TC
+    // the flipped, transposed bf16 weights of the layers whose input gradient is needed
+    for (int l = 1; l < NLAYERS; ++l) {
+        const int n = 9 * LAYERS[l].cin * grad_channels(l);
+        flip_weights_kernel<<<blocks_for(n, 256), 256, 0, s>>>(P->wbf + P->w_off[l], LAYERS[l].cout, LAYERS[l].cin,
+                                                                grad_channels(l), P->wt + P->wt_off[l]);
+    }
+    LC3D_CUDA_TRY(cudaGetLastError());
+#define LC3D_BWD_DATA(l, CIN, g, CG, mask, dx, lev) LC3D_TRY(bwd_data_tc(P, l, g, mask, dx, s))
+#else
+#define LC3D_BWD_DATA(l, CIN, g, CG, mask, dx, lev) LC3D_TRY(bwd_data<CIN>(g, CG, w + P->w_off[l], mask, dx, lev, s))
+#endif
     loss_kernel<<<blocks_for(l0.NP, 256), 256, 0, s>>>(P->y, P->target, P->g_out, l0, loss);
     // conv6: d1 -> y
     LC3D_TRY((bwd_weights<16, 32>(P, 5, P->g_out, P->d1, s)));
-    LC3D_TRY(bwd_data<32>(P->g_out, 16, w + P->w_off[5], P->d1, P->g_d1, l0, s));
+    LC3D_BWD_DATA(5, 32, P->g_out, 16, P->d1, P->g_d1, l0);
     downsum_kernel<<<blocks_for((long long)l1.NP * 32, 256), 256, 0, s>>>(P->g_d1, l0, P->g_u2, l1, 32);
     // conv5: d2 -> u2
     LC3D_TRY((bwd_weights<32, 64>(P, 4, P->g_u2, P->d2, s)));
-    LC3D_TRY(bwd_data<64>(P->g_u2, 32, w + P->w_off[4], P->d2, P->g_d2, l1, s));
+    LC3D_BWD_DATA(4, 64, P->g_u2, 32, P->d2, P->g_d2, l1);
     downsum_kernel<<<blocks_for((long long)l2.NP * 64, 256), 256, 0, s>>>(P->g_d2, l1, P->g_u3, l2, 64);
     // conv4: e3 -> u3
     LC3D_TRY((bwd_weights<64, 128>(P, 3, P->g_u3, P->e3, s)));
-    LC3D_TRY(bwd_data<128>(P->g_u3, 64, w + P->w_off[3], P->e3, P->g_e3, l2, s));
+    LC3D_BWD_DATA(3, 128, P->g_u3, 64, P->e3, P->g_e3, l2);
     // conv3: p2 -> e3
     LC3D_TRY((bwd_weights<128, 64>(P, 2, P->g_e3, P->p2, s)));
-    LC3D_TRY(bwd_data<64>(P->g_e3, 128, w + P->w_off[2], nullptr, P->g_p2, l2, s));
+    LC3D_BWD_DATA(2, 64, P->g_e3, 128, nullptr, P->g_p2, l2);
     pool_bwd_mask_kernel<<<blocks_for((long long)l1.NP * 64, 256), 256, 0, s>>>(P->g_d2, P->e2, l1, P->g_p2, l2, 64);
     // conv2: p1 -> e2 (g_d2 now holds dL/d pre-activation of e2)
     LC3D_TRY((bwd_weights<64, 32>(P, 1, P->g_d2, P->p1, s)));
-    LC3D_TRY(bwd_data<32>(P->g_d2, 64, w + P->w_off[1], nullptr, P->g_p1, l1, s));
+    LC3D_BWD_DATA(1, 32, P->g_d2, 64, nullptr, P->g_p1, l1);
+#undef LC3D_BWD_DATA
     pool_bwd_mask_kernel<<<blocks_for((long long)l0.NP * 32, 256), 256, 0, s>>>(P->g_d1, P->e1, l0, P->g_p1, l1, 32);
     // conv1: x0 -> e1
     LC3D_TRY((bwd_weights<32, 32>(P, 0, P->g_d1, P->x0, s)));
@@ -840,6 +942,17 @@ int lc3d_predictor_create(int grid_steps, int device, lc3d_predictor** out) {
     PA(P->g_out, n0 * 16); PA(P->g_d1, n0 * 32); PA(P->g_u2, n1 * 32); PA(P->g_d2, n1 * 64);
     PA(P->g_u3, n2 * 64); PA(P->g_e3, n2 * 128); PA(P->g_p2, n2 * 64); PA(P->g_p1, n1 * 32);
     PA(P->err, 1); PA(P->scale, 23); PA(P->partial, (size_t)STAT_BLOCKS * 18);
+    {   // tensor-core backward data pass (layers 2..6; the input gradient of layer 1 is not needed)
+        size_t gmax = 0;
+        long long wtot = 0;
+        for (int l = 0; l < NLAYERS; ++l) {
+            P->wt_off[l] = wtot;
+            if (l == 0) continue;
+            gmax = std::max(gmax, (size_t)P->lv[LAYERS[l].level].NP * grad_channels(l));
+            wtot += 9LL * LAYERS[l].cin * grad_channels(l);
+        }
+        PA(P->g_bf, gmax); PA(P->wt, (size_t)wtot); PA(P->zero_bias, 128);
+    }
 #undef PA
     if (rc == LC3D_OK) rc = setup_conv(P, 0, P->x0, P->e1);
     if (rc == LC3D_OK) rc = setup_conv(P, 1, P->p1, P->e2);
@@ -847,6 +960,7 @@ int lc3d_predictor_create(int grid_steps, int device, lc3d_predictor** out) {
     if (rc == LC3D_OK) rc = setup_conv(P, 3, P->e3, P->u3);
     if (rc == LC3D_OK) rc = setup_conv(P, 4, P->d2, P->u2);
     if (rc == LC3D_OK) rc = setup_conv(P, 5, P->d1, P->y);
+    for (int l = 1; l < NLAYERS && rc == LC3D_OK; ++l) rc = setup_bconv(P, l);
     if (rc == LC3D_OK) {
         static bool attrs_set[64] = {};
         bool& attrs = attrs_set[device & 63];

@@ -130,6 +130,8 @@ int capture(lc3d_ctx* c, int par) {
 
 }  // namespace
 
+void run_drop_graphs(lc3d_ctx* c) { drop_graphs(c); }
+
 int run_init(lc3d_ctx* c) {
     LC3D_CUDA_TRY(cudaMalloc(&c->beam_buf, (size_t)c->N * c->N * sizeof(double)));
     LC3D_CUDA_TRY(cudaMemset(c->beam_buf, 0, (size_t)c->N * c->N * sizeof(double)));

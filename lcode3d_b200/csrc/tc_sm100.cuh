@@ -30,9 +30,9 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Bounded wait for the phase with the given parity: false once WAIT_LIMIT
-// SM clock cycles have passed.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for the phase with the given parity: false once `limit` SM
+// clock cycles (WAIT_LIMIT unless a caller passes its own) have passed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = WAIT_LIMIT) {
     const uint32_t a = smem_u32(bar);
     const long long t0 = clock64();
     for (;;) {
@@ -45,7 +45,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
             : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
-        if (clock64() - t0 > WAIT_LIMIT) return false;
+        if (clock64() - t0 > limit) return false;
     }
 }
 

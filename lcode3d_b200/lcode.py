@@ -16,12 +16,13 @@ attribute access like the reference's. All device work runs in liblc3d.so
 
 Extra, optional config attributes (absent in the reference's config):
 ``lc3d_precision`` = 'fp64' (default), 'mixed' (split-bf16 tensor-core
-transforms) or 'fft32' (float32 FFT transforms; right-hand sides, fields,
-averaging and particles in float64);
+transforms), 'tf32' (split-tf32 tensor-core transforms) or 'fft32' (float32
+FFT transforms; right-hand sides, fields, averaging and particles in
+float64);
 ``lc3d_fp64_transform`` = 'auto' (default: FFT where 2(N-1) factors into
 2, 3, 5), 'fft' or 'dense' (DGEMM-form transform matrices);
-``lc3d_mixed_slices`` = bf16 slices per operand of the mixed-precision
-transforms (1..6, default 4).
+``lc3d_mixed_slices`` = slices per operand of the tensor-core transforms
+(1..6; default 4 for 'mixed', 3 for 'tf32').
 """
 import ctypes
 import sys
@@ -112,7 +113,9 @@ def _precision(config):
         return _lib.PREC_MIXED
     if p in ('fft32', _lib.PREC_FFT32):
         return _lib.PREC_FFT32
-    raise ValueError(f'lc3d_precision must be "fp64", "mixed" or "fft32", not {p!r}')
+    if p in ('tf32', _lib.PREC_TF32):
+        return _lib.PREC_TF32
+    raise ValueError(f'lc3d_precision must be "fp64", "mixed", "fft32" or "tf32", not {p!r}')
 
 
 def _fp64_transform(config):

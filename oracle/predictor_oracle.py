@@ -67,14 +67,18 @@ def conv(x, w, b):
     return y + b
 
 
-def conv_bwd(x, w, g):
-    """(dL/dx, dL/dW, dL/db) of y = conv(x, w, b) given g = dL/dy."""
+def conv_bwd(x, w, g, g_data=None):
+    """(dL/dx, dL/dW, dL/db) of y = conv(x, w, b) given g = dL/dy. dL/dx is
+    computed from ``g_data`` when it is given: the GPU's backward data pass
+    runs on the tensor cores and reads g rounded to bf16 (the weight and
+    bias gradients use g as it is)."""
+    gd = g if g_data is None else g_data
     dw = np.zeros_like(w)
     dx = np.zeros(x.shape)
     for tap in range(9):
         dy_, dx_ = tap // 3 - 1, tap % 3 - 1
         dw[tap] = np.einsum('hwo,hwi->oi', g, _shift(x, dy_, dx_))
-        dx += _shift(g, -dy_, -dx_) @ w[tap]
+        dx += _shift(gd, -dy_, -dx_) @ w[tap]
     return dx, dw, g.sum(axis=(0, 1))
 
 
@@ -147,23 +151,25 @@ def loss_and_grad(params, x0, target, use_bf16=True):
     loss = float((d ** 2).sum() / (N_OUT * H * W))
     g = 2.0 * d / (N_OUT * H * W)
     L = c['L']
+    # the output gradients the backward data passes read: bf16 on the GPU
+    RG = (lambda a: bf16(a).astype(np.float64)) if use_bf16 else (lambda a: a)
     grads = [None] * 6
     # conv6
-    gd1, *grads[5] = conv_bwd(c['d1'], L[5][0], g)
+    gd1, *grads[5] = conv_bwd(c['d1'], L[5][0], g, RG(g))
     gd1 = gd1 * (c['d1'] > 0)
     gu2 = up_bwd(gd1, c['u2'].shape)
     # conv5
-    gd2, *grads[4] = conv_bwd(c['d2'], L[4][0], gu2)
+    gd2, *grads[4] = conv_bwd(c['d2'], L[4][0], gu2, RG(gu2))
     gd2 = gd2 * (c['d2'] > 0)
     gu3 = up_bwd(gd2, c['u3'].shape)
     # conv4
-    ge3, *grads[3] = conv_bwd(c['e3'], L[3][0], gu3)
+    ge3, *grads[3] = conv_bwd(c['e3'], L[3][0], gu3, RG(gu3))
     ge3 = ge3 * (c['e3'] > 0)
     # conv3
-    gp2, *grads[2] = conv_bwd(c['p2'], L[2][0], ge3)
+    gp2, *grads[2] = conv_bwd(c['p2'], L[2][0], ge3, RG(ge3))
     ge2 = (gd2 + pool_bwd(gp2, c['n2'], c['e2'].shape)) * (c['e2'] > 0)
     # conv2
-    gp1, *grads[1] = conv_bwd(c['p1'], L[1][0], ge2)
+    gp1, *grads[1] = conv_bwd(c['p1'], L[1][0], ge2, RG(ge2))
     ge1 = (gd1 + pool_bwd(gp1, c['n1'], c['e1'].shape)) * (c['e1'] > 0)
     # conv1
     _, *grads[0] = conv_bwd(c['x0'], L[0][0], ge1)

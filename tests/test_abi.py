@@ -94,9 +94,9 @@ def test_sizes_reject_bad_config(lib, bad):
     assert lib.lc3d_sizes(ctypes.byref(p), None, None, None) == 1
 
 
-@pytest.mark.parametrize('prec,ok', [(0, True), (1, True), (2, True), (3, False), (-1, False)])
+@pytest.mark.parametrize('prec,ok', [(0, True), (1, True), (2, True), (3, True), (4, False), (-1, False)])
 def test_sizes_check_precision(lib, prec, ok):
-    """lc3d_params.precision: LC3D_PREC_FP64, _MIXED and _FFT32 are
+    """lc3d_params.precision: LC3D_PREC_FP64, _MIXED, _FFT32 and _TF32 are
     accepted, anything else is LC3D_ERR_PARAM (host-only check)."""
     from lcode3d_b200 import _lib
     p = _params()
@@ -104,7 +104,7 @@ def test_sizes_check_precision(lib, prec, ok):
     lib.lc3d_sizes.argtypes = [ctypes.POINTER(_lib.Params), ctypes.c_void_p, ctypes.c_void_p,
                                ctypes.c_void_p]
     assert lib.lc3d_sizes(ctypes.byref(p), None, None, None) == (0 if ok else 1)
-    assert (_lib.PREC_FP64, _lib.PREC_MIXED, _lib.PREC_FFT32) == (0, 1, 2)
+    assert (_lib.PREC_FP64, _lib.PREC_MIXED, _lib.PREC_FFT32, _lib.PREC_TF32) == (0, 1, 2, 3)
 
 
 def test_strerror(lib):

@@ -95,3 +95,27 @@ def test_mixed_run_n161(L, S):
     assert e < 1e-6
     for k, v in errs.items():
         assert v < 1e-4, (k, v)
+
+
+@pytest.mark.parametrize('S', [2, 3])
+@pytest.mark.parametrize('N', [41, 161, 641])
+def test_tf32_solvers_vs_fp64(L, N, S):
+    """The split-TF32 transforms (tcgen05 kind::tf32, 10-bit digits): the
+    FP32 accumulation is not exact for these digits, so besides the
+    truncation (2^-10S of the row maxima) every stage carries FP32 rounding
+    of its sums; the bound here is that level with the stages'
+    amplification and headroom."""
+    rng = np.random.default_rng(300 * N + S)
+    h = 16 / (N - 1)
+    ins = [torch.from_numpy(rng.normal(size=(N, N))).cuda() for _ in range(11)]
+    cfg64 = make_config(N, h, 0.01, 10, amplitude=0.1)
+    cfgt = make_config(N, h, 0.01, 10, amplitude=0.1)
+    cfgt.lc3d_precision = 'tf32'
+    cfgt.lc3d_mixed_slices = S
+    ref = solve_all(L, cfg64, ins)
+    got = solve_all(L, cfgt, ins)
+    errs = {k: rel(a, b) for k, a, b in zip(('Ex', 'Ey', 'Bx', 'By', 'Ez', 'Bz'), got, ref)}
+    print(f'N={N} tf32 S={S} relative errors vs float64: ' +
+          ' '.join(f'{k}={v:.2e}' for k, v in errs.items()))
+    for k, v in errs.items():
+        assert v < 1e-3, (k, v)

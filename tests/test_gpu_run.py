@@ -99,6 +99,41 @@ def test_autotuner_picks_a_form(L):
     assert set(timings[161]) == {'fft', 'dense'} and all(v > 0 for v in timings[161].values())
 
 
+def test_autotuner_picks_tile_shapes(L):
+    from lcode3d_b200 import batch as B
+    choice, timings = B.autotune([161], steps=2)
+    c = choice[161]
+    assert c['transform'] in ('fft', 'dense')
+    assert c['deposit_rows'] in B.TILE_CHOICES['deposit_rows']
+    assert c['fft_ctas_per_sm'] in B.TILE_CHOICES['fft_ctas_per_sm']
+    assert len(timings[161]) >= 6 and all(v > 0 for v in timings[161].values())
+
+
+@pytest.mark.parametrize('tiles', [(4, 0), (8, 2), (16, 1)])
+def test_tile_shapes_agree_with_the_oracle(L, tiles):
+    """Every deposition tile height and FFT grid cap gives the reference's
+    result: 20 steps of the 161^2 run against the oracle (1e-10)."""
+    from lcode3d_b200 import _lib
+    cfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+    cfg.lc3d_fp64_transform = 'fft'   # a context of its own (the default config says 'auto')
+    s = L.solver_for(cfg)
+    _lib.check(_lib.lib.lc3d_set_tiles(s.ctx, *tiles), 'lc3d_set_tiles')
+    try:
+        xs, ys, const, virt, st = L.init(cfg)
+        ocfg = make_config(161, 0.05, 0.05, 300, amplitude=0.05)
+        oxs, oys, oconst, ovirt, ost = O.init(ocfg)
+        for i in range(20):
+            b = beam_array(cfg, 40 + i, xs, ys)
+            st = L.step(cfg, const, virt, st, b)
+            ost = O.step(ocfg, oconst, ovirt, ost, b)
+        for k in STATE:
+            assert rel(getattr(st, k), getattr(ost, k)) < 1e-10, k
+    finally:
+        _lib.check(_lib.lib.lc3d_set_tiles(s.ctx, 0, 0), 'lc3d_set_tiles')
+    for bad in ((3, 0), (32, 0), (8, -1)):
+        assert _lib.lib.lc3d_set_tiles(s.ctx, *bad) == _lib.ERR_PARAM
+
+
 def test_diag_zn_matches_scipy(L):
     """lc3d_diag_zn against the reference's own zn expression (scipy.ndimage
     gaussian_filter, oracle restatement) on a state from a real run and on
