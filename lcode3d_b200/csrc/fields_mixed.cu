@@ -56,7 +56,7 @@
 
 namespace {
 
-constexpr int TM = 128, TN = 128, BK = 32;                     // tile and K block (bf16 elements)
+constexpr int TM = 128, TN = 128;                              // output tile
 constexpr int TILE_BYTES = TM * 64;                              // 8 KiB: 128 rows of 64 bytes (A and B alike)
 constexpr int KIND_BF16 = 0, KIND_TF32 = 1;
 

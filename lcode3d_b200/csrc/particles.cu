@@ -11,13 +11,14 @@
 //     c = hi * 2^-24 + lo * 2^-76 + (rounding below 2^-77),
 // which are summed with 64-bit integer adds; integer addition is associative,
 // so the sums do not depend on the order in which threads add them, and the
-// final conversion rounds once. Each CTA owns a 16x32 patch of the fine
-// lattice and accumulates into a 32x32-cell shared-memory window placed on
-// the bounding box of its particles' cells; particles whose stencil falls outside the
-// window (strongly displaced plasma) add straight to the global accumulators.
-// The window is then flushed with 64-bit integer reductions into global
-// memory, and a finalize pass converts to float64, adds the ion background
-// and clears the accumulators for the next call.
+// final conversion rounds once. Each CTA owns a tile of 8 (or 4, 16) fine
+// lattice rows x 32 columns and accumulates into a shared-memory window
+// placed on the bounding box of its particles' cells (float64 sums in a
+// fixed order); particles whose stencil falls outside the window (strongly
+// displaced plasma) add straight to the global accumulators. The window is
+// then flushed with 64-bit integer reductions into global memory, and a
+// finalize pass converts to float64, adds the ion background and clears the
+// accumulators for the next call.
 
 #include <mutex>
 
@@ -224,24 +225,6 @@ __device__ __forceinline__ double fx_value(long long hi, long long lo) {
            (double)lo * 0x1p-76;
 }
 
-#ifndef LC3D_DEP_ROWS
-#define LC3D_DEP_ROWS 16
-#endif
-constexpr int DEP_TJ = 32;                // fine particles per CTA along j (one warp)
-constexpr int DEP_TI = LC3D_DEP_ROWS;     // ... along i (16: two CTAs share an SM)
-constexpr int DEP_THREADS = DEP_TI * DEP_TJ; // phase 1: one fine particle per thread
-constexpr int DEP_BLOCKS = DEP_THREADS / 4;  // phase 2: 2 x 2 blocks of the patch
-static_assert(DEP_TI % 2 == 0 && DEP_THREADS % 4 == 0, "the patch is tiled by 2 x 2 blocks");
-#ifndef LC3D_DEP_W
-#define LC3D_DEP_W 32
-#endif
-constexpr int DEP_W = LC3D_DEP_W;         // shared window side (cells)
-constexpr int DEP_WIN = DEP_W * DEP_W;
-// shared memory: float64 window (4 fields), anchor claims, per-particle
-// staging (cell, xl, yl, 4 values)
-constexpr size_t DEP_SMEM = (size_t)4 * DEP_WIN * sizeof(double) + (size_t)DEP_WIN * sizeof(int) +
-                            (size_t)DEP_THREADS * (6 * sizeof(double) + sizeof(int));
-
 // One fine particle: coarse->fine mix (lcode.py:591-621) and the deposit
 // quantities (lcode.py:651-655).
 struct FineParticle {
@@ -304,210 +287,41 @@ __device__ __forceinline__ void fx_add(unsigned long long* hi_plane, unsigned lo
     atomicAdd(lo_plane + cell, (unsigned long long)lo);
 }
 
-// Deposition of a DEP_TI x 32 patch of the fine lattice by one CTA, one
-// thread per fine particle (16 x 32 by default: with 64 registers two CTAs
-// share an SM, so one CTA's phases overlap the other's barriers and load
-// latencies). Deterministic: every float64 sum below has a fixed order, and
-// the sums that cross CTAs are exact integer (fixed-point) sums.
-//  1. One thread per fine particle: coarse->fine interpolation, deposit
-//     values and TSC cell, staged in shared memory; the CTA's bounding box
-//     of cells places a 32 x 32-cell float64 window.
+// ---------------------------------------------------------------------------
+// Deposition kernel. A CTA of TI warps deposits TI fine-lattice rows x 32
+// columns; one thread per fine particle, then one per (2 x 2 block, field).
+//  1. Coarse->fine mix in two separable passes (the equivalent formula noted
+//     beside the reference's make_plasma, lcode.py:554-556). Each warp holds
+//     one fine row fi of the tile; it first mixes the two coarse rows of fi,
+//         R[c] = inf_prev[fi] Q[prev_i][c] + inf_next[fi] Q[next_i][c],
+//     for every coarse column c its 32 fine columns use (7 quantities, a
+//     warp-private shared-memory table), and each lane then mixes two
+//     entries, Q = inf_prev[fj] R[prev_j] + inf_next[fj] R[next_j]: 14
+//     float64 operations and 8 shared loads per particle, no CTA barrier. A
+//     tile whose columns span more than DEP2_CMAX coarse columns (other
+//     coarseness / fineness settings, or arbitrary virt_params) mixes per
+//     particle from global memory (fine_particle). Then the deposit values
+//     (lcode.py:651-655) and the TSC cell, staged in shared memory; the CTA's
+//     bounding box of cells places the window.
 //  2. One thread per (2 x 2 block of fine particles, field). If the block's
 //     centre cells span at most 2 x 2 cells -- neighbouring fine particles
 //     are interpolated from the same coarse particles and move together --
-//     its four TSC stencils are summed in a fixed order into a 4 x 4 float64
-//     register patch. Blocks claim their patch anchor cell (atomicMax of
-//     the block index: the winner does not depend on timing); winners add
-//     their patches to the window in 16 barrier-separated steps, one patch
-//     entry per step, so in each step every window cell has at most one
-//     writer and its summation order is fixed. Losing blocks (two blocks on
-//     one anchor, < 1% of blocks in the 641^2 blowout run) and blocks that
-//     span more cells or leave the window add their contributions straight
-//     to the global accumulators through the exact fixed-point split.
+//     its four TSC stencils are summed in a fixed order into a register
+//     patch: 3 x 3 when all four lie in one cell, else 4 x 4. Tiles start
+//     `a.fine_off` fine particles before the lattice origin: with an even
+//     fineness the lattice has two particles per cell and axis and the fine
+//     index pairs (odd, even) share a cell, so with an offset of 1 every
+//     block of an undisturbed lattice lies in one cell (9 window entries and
+//     36 products per field instead of 16 and 64). Blocks claim their patch's
+//     corner cell (atomicMax of the block index: the winner does not depend
+//     on timing); winners add their patches to the window in 9 or 16
+//     barrier-separated steps, one patch entry per step, so in each step
+//     every window cell has at most one writer and its summation order is
+//     fixed. Losing blocks (two on one corner) and blocks that span more
+//     cells or leave the window add their contributions straight to the
+//     global accumulators through the exact split.
 //  3. Each touched window cell is split once into fixed point and added to
 //     the global accumulators.
-__global__ void __launch_bounds__(DEP_THREADS, 1024 / DEP_THREADS) deposit_kernel(DepositArgs a) {
-    extern __shared__ double smem_f64[];
-    double* fwin = smem_f64;                                   // [4][DEP_WIN]
-    double* s_xl = fwin + 4 * DEP_WIN;                         // [DEP_THREADS]
-    double* s_yl = s_xl + DEP_THREADS;
-    double* s_v = s_yl + DEP_THREADS;                          // [4][DEP_THREADS]
-    int* s_cell = reinterpret_cast<int*>(s_v + 4 * DEP_THREADS);   // i << 16 | j, or -1
-    int* s_claim = s_cell + DEP_THREADS;                       // [DEP_WIN]
-    __shared__ int s_bb[4];                                    // imin imax jmin jmax
-    const int t = threadIdx.x;
-    const int N = a.N;
-    const size_t NN = a.plane;
-    if (t == 0) {
-        s_bb[0] = s_bb[2] = 1 << 30;
-        s_bb[1] = s_bb[3] = -(1 << 30);
-    }
-    for (int w = t; w < 4 * DEP_WIN; w += DEP_THREADS) fwin[w] = 0.0;
-    for (int w = t; w < DEP_WIN; w += DEP_THREADS) s_claim[w] = -1;
-    pdl_wait();   // global memory from here on
-
-    // ---- phase 1: one fine particle per thread ----
-    {
-        const int fi = blockIdx.y * DEP_TI + (t >> 5), fj = blockIdx.x * DEP_TJ + (t & 31);
-        int cell = -1, i = 1 << 30, j = 1 << 30;
-        if (fi < a.Nf && fj < a.Nf) {
-            const FineParticle f = fine_particle(a, fi, fj);
-            double xl, yl;
-            tsc_cell(f.x, f.y, N, a.h, a.inv_h, i, j, xl, yl);
-            const double vmax = fmax(fmax(fabs(f.dro), fabs(f.djx)), fmax(fabs(f.djy), fabs(f.djz)));
-            if (!(i >= 1 && i <= N - 2 && j >= 1 && j <= N - 2)) {
-                atomicOr(a.err, LC3D_FLAG_WINDOW);
-            } else if (!(vmax < FX_MAX)) {   // also catches NaN
-                atomicOr(a.err, LC3D_FLAG_NONFINITE);
-            } else {
-                cell = (i << 16) | j;
-            }
-            s_xl[t] = xl;
-            s_yl[t] = yl;
-            s_v[t] = f.dro;
-            s_v[DEP_THREADS + t] = f.djx;
-            s_v[2 * DEP_THREADS + t] = f.djy;
-            s_v[3 * DEP_THREADS + t] = f.djz;
-        }
-        s_cell[t] = cell;
-        // warp bounding box of the cells (one redux instruction each)
-        const int imin = __reduce_min_sync(0xffffffffu, cell >= 0 ? i : 1 << 30);
-        const int imax = __reduce_max_sync(0xffffffffu, cell >= 0 ? i : -(1 << 30));
-        const int jmin = __reduce_min_sync(0xffffffffu, cell >= 0 ? j : 1 << 30);
-        const int jmax = __reduce_max_sync(0xffffffffu, cell >= 0 ? j : -(1 << 30));
-        __syncthreads();   // s_bb initialised, window and claims cleared
-        if ((t & 31) == 0 && imin <= imax) {
-            atomicMin(&s_bb[0], imin);
-            atomicMax(&s_bb[1], imax);
-            atomicMin(&s_bb[2], jmin);
-            atomicMax(&s_bb[3], jmax);
-        }
-    }
-    __syncthreads();
-    const int oi = s_bb[0] - 1, oj = s_bb[2] - 1;   // window origin (cells)
-
-    // ---- phase 2: one (2 x 2 block, field) per thread ----
-    const int f = t / DEP_BLOCKS, blk = t % DEP_BLOCKS;
-    const int p0 = (blk >> 4) * 2 * DEP_TJ + (blk & 15) * 2;   // top-left particle of the block
-    const int pidx[4] = {p0, p0 + 1, p0 + DEP_TJ, p0 + DEP_TJ + 1};
-    int ci[4], cj[4];
-    bool ok[4];
-    int i0 = 1 << 30, i1 = -(1 << 30), j0 = 1 << 30, j1 = -(1 << 30);
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-        const int c = s_cell[pidx[p]];
-        ok[p] = c >= 0;
-        ci[p] = c >> 16;
-        cj[p] = c & 0xffff;
-        if (ok[p]) {
-            i0 = min(i0, ci[p]);
-            i1 = max(i1, ci[p]);
-            j0 = min(j0, cj[p]);
-            j1 = max(j1, cj[p]);
-        }
-    }
-    const bool patch = i0 <= i1 && i1 - i0 <= 1 && j1 - j0 <= 1 && i0 + 2 - oi < DEP_W && j0 + 2 - oj < DEP_W;
-    const int r0 = i0 - 1 - oi, c0 = j0 - 1 - oj;   // window coordinates of the patch corner
-    if (patch && f == 0) atomicMax(&s_claim[r0 * DEP_W + c0], blk);
-    __syncthreads();
-    const bool winner = patch && s_claim[r0 * DEP_W + c0] == blk;
-    unsigned long long* ghi = a.acc + (2 * f) * NN;
-    unsigned long long* glo = ghi + NN;
-    const double* vf = s_v + f * DEP_THREADS;
-    double acc[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) acc[k] = 0.0;
-    if (patch) {
-#pragma unroll
-        for (int p = 0; p < 4; ++p) {
-            if (!ok[p]) continue;
-            double wxM, wx0, wxP, wyM, wy0, wyP;
-            tsc_axis(s_xl[pidx[p]], wxM, wx0, wxP);
-            tsc_axis(s_yl[pidx[p]], wyM, wy0, wyP);
-            const bool si = ci[p] != i0, sj = cj[p] != j0;
-            const double wx4[4] = {si ? 0.0 : wxM, si ? wxM : wx0, si ? wx0 : wxP, si ? wxP : 0.0};
-            const double wy4[4] = {sj ? 0.0 : wyM, sj ? wyM : wy0, sj ? wy0 : wyP, sj ? wyP : 0.0};
-            const double v = vf[pidx[p]];
-            // v wx wy as (v wx) wy: 20 instead of 32 float64 operations
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const double vx = v * wx4[r];
-#pragma unroll
-                for (int c = 0; c < 4; ++c) acc[r * 4 + c] = fma(vx, wy4[c], acc[r * 4 + c]);
-            }
-        }
-        if (!winner) {
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int c = 0; c < 4; ++c)
-                    if (acc[r * 4 + c] != 0.0) fx_add(ghi, glo, (size_t)(i0 - 1 + r) * N + (j0 - 1 + c), acc[r * 4 + c]);
-        }
-    } else {
-#pragma unroll 1
-        for (int p = 0; p < 4; ++p) {
-            const int c = s_cell[pidx[p]];
-            if (c < 0) continue;
-            const int pi = c >> 16, pj = c & 0xffff;
-            double wx[3], wy[3];
-            tsc_axis(s_xl[pidx[p]], wx[0], wx[1], wx[2]);
-            tsc_axis(s_yl[pidx[p]], wy[0], wy[1], wy[2]);
-            const double v = vf[pidx[p]];
-#pragma unroll
-            for (int di = 0; di < 3; ++di)
-#pragma unroll
-                for (int dj = 0; dj < 3; ++dj)
-                    fx_add(ghi, glo, (size_t)(pi + di - 1) * N + (pj + dj - 1), v * (wx[di] * wy[dj]));
-        }
-    }
-    // winners add their patches, one entry per barrier-separated step
-    double* fw = fwin + f * DEP_WIN + (winner ? r0 * DEP_W + c0 : 0);
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        if (winner && acc[k] != 0.0) fw[(k >> 2) * DEP_W + (k & 3)] += acc[k];
-        __syncthreads();
-    }
-
-    // ---- phase 3: split each touched window cell once, add to global ----
-    if (s_bb[0] <= s_bb[1]) {
-        const int ni = min(s_bb[1] + 2 - oi, DEP_W), nj = min(s_bb[3] + 2 - oj, DEP_W);
-        for (int w = t; w < 4 * DEP_WIN; w += DEP_THREADS) {
-            const int q = w / DEP_WIN, r = (w / DEP_W) % DEP_W, c = w % DEP_W;
-            if (r >= ni || c >= nj) continue;
-            const double v = fwin[w];
-            if (v != 0.0)
-                fx_add(a.acc + (2 * q) * NN, a.acc + (2 * q + 1) * NN, (size_t)(oi + r) * N + (oj + c), v);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Deposition, second form (the default): the same exact fixed-point
-// accumulation and the same register patches of 2 x 2 fine particles as
-// deposit_kernel above, with three changes.
-//  * Coarse->fine mix in two separable passes (the equivalent formula noted
-//    beside the reference's make_plasma, lcode.py:554-556). Each warp holds
-//    one fine row fi of the tile; it first mixes the two coarse rows of fi,
-//        R[c] = inf_prev[fi] Q[prev_i][c] + inf_next[fi] Q[next_i][c],
-//    for every coarse column c its 32 fine columns use (7 quantities, a
-//    warp-private shared-memory table), and each lane then mixes two
-//    entries, Q = inf_prev[fj] R[prev_j] + inf_next[fj] R[next_j]: 14
-//    float64 operations and 8 shared loads instead of 32 operations and 16
-//    scattered global loads, with no CTA barrier. A tile whose columns span
-//    more than DEP2_CMAX coarse columns (other coarseness / fineness
-//    settings, or arbitrary virt_params) mixes per particle from global
-//    memory as deposit_kernel does.
-//  * Tiles start `a.fine_off` fine particles before the lattice origin. With
-//    an even fineness the lattice has two fine particles per cell and axis
-//    and the pairs (odd, even) of fine indices share a cell; an offset of 1
-//    makes every 2 x 2 block of an undisturbed lattice lie in one cell, so
-//    its patch is the 3 x 3 stencil (9 window entries and 36 products per
-//    field instead of 16 and 64).
-//  * Blocks whose particles lie in one cell take a 3 x 3 patch; the others
-//    the 4 x 4 patch of deposit_kernel.
-// The window fill keeps deposit_kernel's claims and barrier-separated steps
-// (9 or 16), so results do not depend on timing: every float64 sum has a
-// fixed order and the sums that cross CTAs are integer sums.
 // ---------------------------------------------------------------------------
 #ifndef LC3D_DEP2_CLOCKS
 #define LC3D_DEP2_CLOCKS 0
@@ -555,7 +369,7 @@ __device__ __forceinline__ double2 coarse_pair(const DepositArgs& a, int k, int 
 // TI fine rows x 32 fine columns per CTA, one warp per row (TI = 4, 8, 16:
 // 8, 4 or 2 resident CTAs per SM at 64 registers).
 template <int TI>
-__global__ void __launch_bounds__(TI * 32, 1024 / (TI * 32)) deposit_kernel2(DepositArgs a) {
+__global__ void __launch_bounds__(TI * 32, 1024 / (TI * 32)) deposit_kernel(DepositArgs a) {
     constexpr int DEP2_TI = TI;
     constexpr int DEP2_THREADS = DEP2_TI * 32;
     constexpr int DEP2_BLOCKS = DEP2_THREADS / 4;
@@ -891,15 +705,10 @@ int launch_move_smart(const MoveArgs& a, cudaStream_t s) {
     return LC3D_OK;
 }
 
-#ifndef LC3D_DEP_V2
-#define LC3D_DEP_V2 1
-#endif
-
 int particles_prepare() {
-    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DEP_SMEM));
-    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel2<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(4)));
-    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel2<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(8)));
-    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel2<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(16)));
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(4)));
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(8)));
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(16)));
     return LC3D_OK;
 }
 
@@ -917,25 +726,20 @@ int deposit_fine_offset(int fineness) {
 
 int launch_deposit_main(const DepositArgs& a, cudaStream_t s) {
     if (a.Nf <= 0) return LC3D_OK;
-    dim3 grid((a.Nf + DEP_TJ - 1) / DEP_TJ, (a.Nf + DEP_TI - 1) / DEP_TI);
-#if LC3D_DEP_V2
     const int ti = a.tile_rows ? a.tile_rows : LC3D_DEP2_ROWS;
     const dim3 grid2((a.Nf + a.fine_off + 31) / 32, (a.Nf + a.fine_off + ti - 1) / ti);
     switch (ti) {
-        case 4: LC3D_CUDA_TRY(launch_pdl(deposit_kernel2<4>, grid2, dim3(4 * 32), dep2_smem(4), s, a)); break;
-        case 8: LC3D_CUDA_TRY(launch_pdl(deposit_kernel2<8>, grid2, dim3(8 * 32), dep2_smem(8), s, a)); break;
-        case 16: LC3D_CUDA_TRY(launch_pdl(deposit_kernel2<16>, grid2, dim3(16 * 32), dep2_smem(16), s, a)); break;
+        case 4: LC3D_CUDA_TRY(launch_pdl(deposit_kernel<4>, grid2, dim3(4 * 32), dep2_smem(4), s, a)); break;
+        case 8: LC3D_CUDA_TRY(launch_pdl(deposit_kernel<8>, grid2, dim3(8 * 32), dep2_smem(8), s, a)); break;
+        case 16: LC3D_CUDA_TRY(launch_pdl(deposit_kernel<16>, grid2, dim3(16 * 32), dep2_smem(16), s, a)); break;
         default: return LC3D_ERR_PARAM;
     }
-#else
-    LC3D_CUDA_TRY(launch_pdl(deposit_kernel, grid, dim3(DEP_THREADS), DEP_SMEM, s, a));
-#endif
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
 
 #if LC3D_DEP2_CLOCKS
-// Instrumented builds only: phase clocks of the last deposit_kernel2 launch,
+// Instrumented builds only: phase clocks of the last deposit_kernel launch,
 // [16384][DEP2_NCLK] cycles since each CTA's start.
 extern "C" int lc3d_debug_dep_clocks(long long* host) {
     LC3D_CUDA_TRY(cudaDeviceSynchronize());

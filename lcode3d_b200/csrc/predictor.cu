@@ -858,8 +858,6 @@ int forward(lc3d_predictor* P, cudaStream_t s) {
 
 int backward(lc3d_predictor* P, float* loss, cudaStream_t s) {
     const Level &l0 = P->lv[0], &l1 = P->lv[1], &l2 = P->lv[2];
-    const __nv_bfloat16* w = P->wbf;
-    (void)w;
     LC3D_CUDA_TRY(cudaMemsetAsync(P->grad, 0, (size_t)P->np * sizeof(float), s));
 #if LC3D_PRED_BWD_TC
     // the flipped, transposed bf16 weights of the layers whose input gradient is needed
@@ -871,6 +869,7 @@ int backward(lc3d_predictor* P, float* loss, cudaStream_t s) {
     LC3D_CUDA_TRY(cudaGetLastError());
 #define LC3D_BWD_DATA(l, CIN, g, CG, mask, dx, lev) LC3D_TRY(bwd_data_tc(P, l, g, mask, dx, s))
 #else
+    const __nv_bfloat16* w = P->wbf;
 #define LC3D_BWD_DATA(l, CIN, g, CG, mask, dx, lev) LC3D_TRY(bwd_data<CIN>(g, CG, w + P->w_off[l], mask, dx, lev, s))
 #endif
     loss_kernel<<<blocks_for(l0.NP, 256), 256, 0, s>>>(P->y, P->target, P->g_out, l0, loss);

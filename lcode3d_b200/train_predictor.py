@@ -43,9 +43,9 @@ def main(argv=None):
     ap.add_argument('--h', type=float, default=0.025)
     ap.add_argument('--xi-step', type=float, default=0.005)
     ap.add_argument('--steps', type=int, default=3000, help='xi steps per run')
-    ap.add_argument('--runs', type=int, default=40, help='training runs')
+    ap.add_argument('--runs', type=int, default=200, help='training runs')
     ap.add_argument('--held-out', type=int, default=20)
-    ap.add_argument('--eval-runs', type=int, default=4, help='held-out runs of the learned method')
+    ap.add_argument('--eval-runs', type=int, default=20, help='held-out runs of the learned method')
     ap.add_argument('--every', type=int, default=30)
     ap.add_argument('--buffer', type=int, default=600)
     ap.add_argument('--epochs-per-run', type=int, default=2)
@@ -74,20 +74,37 @@ def main(argv=None):
     base = float(np.mean([e[1] for e in ev]))
     print(f'held-out ({len(held)} runs): MSE network {net:.4e}, linear extrapolation {base:.4e}, '
           f'ratio {net / base:.4e}', flush=True)
-    learned = []
+    learned, table = [], {}
     for tol in [float(t) for t in a.tols.split(',')]:
+        rows = []
         for b in held[:a.eval_runs]:
             cfg = mk(b)
             ez_l, st, _ = P.run_learned(cfg, b, a.steps, pr, tol=tol)
-            ez_p, _, _ = P.run_learned(cfg, b, a.steps, pr, tol=-1.0)   # plain steps only
+            ez_p, stp, _ = P.run_learned(cfg, b, a.steps, pr, tol=-1.0)   # plain steps only
+            st['tol'] = tol
             st['beam'] = b
             st['ez_max_rel_err_vs_plain'] = float(np.abs(ez_l - ez_p).max() / np.abs(ez_p).max())
+            st['plain_xi_steps_per_s'] = stp['xi_steps_per_s']
             learned.append(st)
+            rows.append(st)
             print(json.dumps(st), flush=True)
+        # the config's report over the held-out seeds: first passes saved,
+        # fallback rate, Ez error against the float64 method, speed
+        table[f'{tol:g}'] = {
+            'runs': len(rows),
+            'first_passes_saved_mean': float(np.mean([r['learned_steps'] / a.steps for r in rows])),
+            'fallback_rate_mean': float(np.mean([1.0 if r['fallback_rate'] is None else r['fallback_rate']
+                                                 for r in rows])),
+            'ez_max_rel_err_vs_fp64_max': float(np.max([r['ez_max_rel_err_vs_plain'] for r in rows])),
+            'xi_steps_per_s_mean': float(np.mean([r['xi_steps_per_s'] for r in rows])),
+            'plain_xi_steps_per_s_mean': float(np.mean([r['plain_xi_steps_per_s'] for r in rows])),
+        }
+        print(json.dumps({'tol': tol, **table[f'{tol:g}']}), flush=True)
     summary = {'grid': a.grid, 'runs': a.runs, 'steps_per_run': a.steps, 'every': a.every,
                'epochs_per_run': a.epochs_per_run, 'train_seconds': t_train, 'loss_history': hist,
                'held_out_runs': len(held), 'held_out_mse_network': net, 'held_out_mse_linear_extrapolation': base,
-               'learned_runs': learned, 'weights': os.path.relpath(a.out, os.path.dirname(HERE))}
+               'learned_runs': learned, 'learned_table': table,
+               'weights': os.path.relpath(a.out, os.path.dirname(HERE))}
     if a.summary:
         with open(a.summary, 'w') as f:
             json.dump(summary, f, indent=1)
