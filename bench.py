@@ -588,8 +588,10 @@ def run_scan(args, rank, world, dist):
     choice, timings = B.autotune(grids, steps=4)
     torch.cuda.synchronize()
     t_setup = time.perf_counter()
+    multi = args.scan_deposit == 'multi'
     bt = B.Batch([specs[i] for i in mine], transform={N: c['transform'] for N, c in choice.items()},
-                 tiles={N: (c['deposit_rows'], c['fft_ctas_per_sm']) for N, c in choice.items()})
+                 tiles={N: (c['deposit_rows'], c['fft_ctas_per_sm']) for N, c in choice.items()},
+                 multi_deposit=multi)
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t_setup
     K, W = args.steps, args.warmup
@@ -630,7 +632,9 @@ def run_scan(args, rank, world, dist):
         'higher_is_better': True, 'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f64',
         'data': 'synthetic (seeded scan draws, generated plasma and beams)',
         'config': {'workload': f'{len(specs)} independent simulations, grids {counts}, window +-8, dxi 0.01',
-                   'seed': args.seed, 'l2': 'no flush (each batch step touches several GB, far more than L2)'},
+                   'seed': args.seed, 'l2': 'no flush (each batch step touches several GB, far more than L2)',
+                   'deposition': ('one launch over all simulations per deposition point (8-row tiles)' if multi
+                                  else 'per simulation, on its graph branch (autotuned tile rows)')},
         'autotune': {'choice': {str(k): v for k, v in choice.items()},
                      'ms_per_step': {str(k): v for k, v in timings.items()}},
         'gpu_launches': launches,
@@ -752,6 +756,8 @@ def main():
     ap.add_argument('--scan', type=int, default=0,
                     help='batched parameter scan of this many simulations instead of the single-grid workload')
     ap.add_argument('--seed', type=int, default=2025, help='seed of the scan draws')
+    ap.add_argument('--scan-deposit', default='branches', choices=['branches', 'multi'],
+                    help='scan: depositions per simulation on graph branches, or one launch over all')
     ap.add_argument('--learned', nargs='?', const='default', default=None,
                     help='learned first pass with these trained parameters (.npz; default: the packaged ones)')
     ap.add_argument('--tol', type=float, default=1e-6, help='learned: verification tolerance on max|pred - F1| / max|F1|')

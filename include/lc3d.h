@@ -193,6 +193,15 @@ int lc3d_batch_create(lc3d_ctx* const* ctxs, int count, lc3d_batch** out);
 int lc3d_batch_run(lc3d_batch* b, const int* xi0, int nsteps, double* const* ez_history, void* stream);
 int lc3d_batch_destroy(lc3d_batch* b);
 
+/* How a batch's graphs are built (no reference counterpart). 0 (default):
+ * every simulation's whole step on its own branch. 1: each simulation's
+ * step is cut at its three depositions, and every deposition point is ONE
+ * launch over all simulations (a work list of (simulation, tile) items,
+ * tiles of 8 fine rows) between the branches. Results are bit-identical to
+ * the simulations run alone with 8-row deposition tiles. The next
+ * lc3d_batch_run captures the graphs again. */
+int lc3d_batch_set_mode(lc3d_batch* b, int multi_deposit);
+
 /* ---- per-stage entry points (the functions step() calls) ---- */
 
 /* move_estimate_wo_fields, lcode.py:369-391. */

@@ -85,6 +85,7 @@ SIGNATURES = [
     ('lc3d_batch_create', c_int, [P, c_int, ctypes.POINTER(c_void_p)]),
     ('lc3d_batch_run', c_int, [P, P, c_int, P, P]),
     ('lc3d_batch_destroy', c_int, [P]),
+    ('lc3d_batch_set_mode', c_int, [P, c_int]),
     ('lc3d_beam_eval', c_int, [P, c_int, P, P]),
     ('lc3d_diag_zn', c_int, [P, P, P, P]),
     ('lc3d_init_plasma', c_int, [P, P]),

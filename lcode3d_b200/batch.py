@@ -111,10 +111,11 @@ class Sim:
 class Batch:
     """Simulations advanced together by ``lc3d_batch_run``."""
 
-    def __init__(self, specs, precision='fp64', transform=None, slices=0, tiles=None):
+    def __init__(self, specs, precision='fp64', transform=None, slices=0, tiles=None, multi_deposit=False):
         """``transform``: one form or {N: form}; ``tiles``: {N: (deposit
         rows, FFT CTAs per SM)} as lc3d_set_tiles takes them (both as
-        ``autotune`` returns them)."""
+        ``autotune`` returns them); ``multi_deposit``: every deposition point
+        of a step is one launch over all simulations (lc3d_batch_set_mode)."""
         transform = transform or {}
         tiles = tiles or {}
         self.sims = [Sim(s, precision, transform.get(s['grid_steps'], 'auto') if isinstance(transform, dict)
@@ -122,6 +123,8 @@ class Batch:
         self._ctxs = (ctypes.c_void_p * len(self.sims))(*[s.solver.ctx.value for s in self.sims])
         self.handle = ctypes.c_void_p()
         check(lib.lc3d_batch_create(self._ctxs, len(self.sims), ctypes.byref(self.handle)), 'lc3d_batch_create')
+        if multi_deposit:
+            check(lib.lc3d_batch_set_mode(self.handle, 1), 'lc3d_batch_set_mode')
 
     def __del__(self):
         h = getattr(self, 'handle', None)

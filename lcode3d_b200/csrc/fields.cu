@@ -242,23 +242,55 @@ struct FinalizeArgs {
     double* avg[6];
     const double* partial;
     int nblocks, n, variant_A, has_bz;
+    int vec;                          // set by the launcher: every array 16-byte aligned, two cells per thread
     double inv_n;
 };
+
+// Field f of one cell: the mean-free Bz, Variant A's 2 F - F_prev, and the
+// half-step average (lcode.py:876-881, 906-911).
+__device__ __forceinline__ double2 finalize_value(const FinalizeArgs& a, int f, double raw, double prev, double mean) {
+    double v = raw;
+    if (f == 5) v -= mean;
+    if (a.variant_A && f != 2 && f != 5) v = 2 * v - prev;
+    return make_double2(v, (v + prev) / 2);
+}
 
 __global__ void __launch_bounds__(RED_THREADS) finalize_step_kernel(const __grid_constant__ FinalizeArgs a) {
     pdl_wait();
     __shared__ double sh[RED_THREADS];
     const double mean = a.has_bz ? mean_from_partials(a.partial, a.nblocks, a.inv_n, sh) : 0.0;
-    const int k = blockIdx.x * RED_THREADS + threadIdx.x;
+    int k = blockIdx.x * RED_THREADS + threadIdx.x;
+    if (a.vec) {
+        // two cells per thread: all twelve 16-byte loads issued before the stores
+        k *= 2;
+        if (k >= a.n) return;
+        if (k + 1 < a.n) {
+            double2 r[6], p[6];
+#pragma unroll
+            for (int f = 0; f < 6; ++f)
+                if (a.raw[f]) {
+                    r[f] = __ldcg(reinterpret_cast<const double2*>(a.raw[f] + k));
+                    p[f] = __ldcg(reinterpret_cast<const double2*>(a.prev[f] + k));
+                }
+#pragma unroll
+            for (int f = 0; f < 6; ++f) {
+                if (!a.raw[f]) continue;
+                const double2 v0 = finalize_value(a, f, r[f].x, p[f].x, mean);
+                const double2 v1 = finalize_value(a, f, r[f].y, p[f].y, mean);
+                if (a.out[f]) *reinterpret_cast<double2*>(a.out[f] + k) = make_double2(v0.x, v1.x);
+                *reinterpret_cast<double2*>(a.avg[f] + k) = make_double2(v0.y, v1.y);
+            }
+            return;
+        }
+        // an odd cell count leaves the last cell to one thread, below
+    }
     if (k >= a.n) return;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         if (!a.raw[f]) continue;
-        double v = a.raw[f][k];
-        if (f == 5) v -= mean;
-        if (a.variant_A && f != 2 && f != 5) v = 2 * v - a.prev[f][k];
-        if (a.out[f]) a.out[f][k] = v;
-        a.avg[f][k] = (v + a.prev[f][k]) / 2;
+        const double2 v = finalize_value(a, f, a.raw[f][k], a.prev[f][k], mean);
+        if (a.out[f]) a.out[f][k] = v.x;
+        a.avg[f][k] = v.y;
     }
 }
 
@@ -610,9 +642,15 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
     fa.variant_A = c->p.field_solver_variant_A;
     fa.has_bz = on[5];
     fa.inv_n = inv_n;
+    uintptr_t al = 0;
+    for (int f = 0; f < 6; ++f)
+        al |= reinterpret_cast<uintptr_t>(fa.raw[f]) | reinterpret_cast<uintptr_t>(fa.prev[f]) |
+              reinterpret_cast<uintptr_t>(fa.out[f]) | reinterpret_cast<uintptr_t>(fa.avg[f]);
+    fa.vec = (al & 15) == 0;
+    const int threads = fa.vec ? (n + 1) / 2 : n;
     ProfScope ps(c, LC3D_STAGE_FIELD_FIN, s);
-    LC3D_CUDA_TRY(launch_pdl(finalize_step_kernel, dim3((n + RED_THREADS - 1) / RED_THREADS), dim3(RED_THREADS), 0,
-                             s, fa));
+    LC3D_CUDA_TRY(launch_pdl(finalize_step_kernel, dim3((threads + RED_THREADS - 1) / RED_THREADS),
+                             dim3(RED_THREADS), 0, s, fa));
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }

@@ -132,9 +132,8 @@ MoveArgs move_base(lc3d_ctx* c) {
     return a;
 }
 
-int deposit_into(lc3d_ctx* c, const double* ro_initial, const double* x, const double* y, const double* m,
-                 const double* q, const double* px, const double* py, const double* pz, double* ro, double* jx,
-                 double* jy, double* jz, cudaStream_t s, const double* packed = nullptr) {
+DepositArgs deposit_args(lc3d_ctx* c, const double* x, const double* y, const double* m, const double* q,
+                         const double* px, const double* py, const double* pz, const double* packed) {
     DepositArgs a{};
     a.x_offt = x; a.y_offt = y; a.m = m; a.q = q; a.px = px; a.py = py; a.pz = pz;
     a.packed = packed;   // the same values, packed by the move just before
@@ -147,12 +146,25 @@ int deposit_into(lc3d_ctx* c, const double* ro_initial, const double* x, const d
     a.tile_rows = c->dep_rows;
     a.h = c->p.grid_step_size; a.inv_h = 1.0 / c->p.grid_step_size; a.sf = c->sf;
     a.err = c->err;
+    return a;
+}
+
+DepositFinalizeArgs finalize_args(lc3d_ctx* c, const double* ro_initial, double* ro, double* jx, double* jy,
+                                  double* jz) {
     DepositFinalizeArgs f{};
     f.acc = c->acc;
     f.plane = c->acc_plane;
     f.ro_initial = ro_initial;
     f.ro = ro; f.jx = jx; f.jy = jy; f.jz = jz;
     f.n = c->N * c->N;
+    return f;
+}
+
+int deposit_into(lc3d_ctx* c, const double* ro_initial, const double* x, const double* y, const double* m,
+                 const double* q, const double* px, const double* py, const double* pz, double* ro, double* jx,
+                 double* jy, double* jz, cudaStream_t s, const double* packed = nullptr) {
+    const DepositArgs a = deposit_args(c, x, y, m, q, px, py, pz, packed);
+    const DepositFinalizeArgs f = finalize_args(c, ro_initial, ro, jx, jy, jz);
     {
         ProfScope ps(c, LC3D_STAGE_DEPOSIT, s);
         LC3D_TRY(launch_deposit_main(a, s));
@@ -437,6 +449,69 @@ __global__ void negate_kernel(const double* __restrict__ a, double* __restrict__
 int step_schedule(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& out, const double* beam,
                   cudaStream_t s) {
     return run_step(c, prev, out, beam, s);
+}
+
+// The plain xi step of run_step cut at its three depositions, for batches
+// whose depositions run as one launch over all simulations. Segment `seg`
+// enqueues the launches between deposition seg - 1 and deposition seg and
+// returns the kernel arguments of deposition seg in *dep (segments 0-2);
+// the finalize of deposition seg - 1 opens segment seg (1-3). The launches
+// and their order are those of run_step without extras.
+int step_schedule_segment(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& out,
+                          const double* beam, cudaStream_t s, int seg, DepositArgs* dep) {
+    const double* prevF[6] = {prev.Ex, prev.Ey, prev.Ez, prev.Bx, prev.By, prev.Bz};
+    const bool A = c->p.field_solver_variant_A != 0;
+    MoveArgs mv = move_base(c);
+    mv.m = c->m; mv.q = c->q; mv.x_init = c->x_init; mv.y_init = c->y_init;
+    mv.x_prev = prev.x_offt; mv.y_prev = prev.y_offt;
+    mv.px_prev = prev.px; mv.py_prev = prev.py; mv.pz_prev = prev.pz;
+    mv.out_packed = c->packed;
+    auto move = [&](int pass) -> int {   // pass 0, 1: predictor / corrector; 2: final
+        if (pass == 0) {
+            mv.est_x = mv.est_y = nullptr;
+        } else {
+            mv.est_x = c->pw[pass - 1][0];
+            mv.est_y = c->pw[pass - 1][1];
+        }
+        for (int f = 0; f < 6; ++f) mv.F[f] = pass ? c->avg[f] : prevF[f];
+        double* const* o = pass < 2 ? c->pw[pass] : nullptr;
+        mv.out_x = o ? o[0] : out.x_offt; mv.out_y = o ? o[1] : out.y_offt;
+        mv.out_px = o ? o[2] : out.px; mv.out_py = o ? o[3] : out.py; mv.out_pz = o ? o[4] : out.pz;
+        ProfScope ps(c, LC3D_STAGE_MOVE, s);
+        LC3D_TRY(launch_move_smart(mv, s));
+        *dep = deposit_args(c, mv.out_x, mv.out_y, c->m, c->q, mv.out_px, mv.out_py, mv.out_pz, c->packed);
+        return LC3D_OK;
+    };
+    auto finalize = [&](double* ro, double* jx, double* jy, double* jz) -> int {
+        ProfScope ps(c, LC3D_STAGE_DEPOSIT_FIN, s);
+        return launch_deposit_finalize(finalize_args(c, c->ro_initial, ro, jx, jy, jz), s);
+    };
+    if (seg == 0) return move(0);
+    if (seg == 3) return finalize(out.ro, out.jx, out.jy, out.jz);
+    if (seg != 1 && seg != 2) return LC3D_ERR_PARAM;
+    const int pass = seg - 1;
+    LC3D_TRY(finalize(c->dens[0], c->dens[1], c->dens[2], c->dens[3]));
+    SolveInputs in{};
+    in.ro = c->dens[0]; in.jx = c->dens[1]; in.jy = c->dens[2]; in.jz = c->dens[3];
+    in.ro_prev = A ? prev.ro : nullptr;
+    in.jz_prev = A ? prev.jz : nullptr;
+    in.jx_prev = prev.jx; in.jy_prev = prev.jy;
+    in.beam = beam;
+    SolveOutputs so{};
+    so.mode = 1;
+    for (int f = 0; f < 6; ++f) {
+        so.prev[f] = prevF[f];
+        so.avg[f] = c->avg[f];
+    }
+    if (pass == 0) {
+        in.Ex_sub = prev.Ex; in.Ey_sub = prev.Ey; in.Bx_sub = prev.Bx; in.By_sub = prev.By;
+    } else {
+        in.Ex_sub = c->avg[0]; in.Ey_sub = c->avg[1]; in.Bx_sub = c->avg[3]; in.By_sub = c->avg[4];
+        so.out[0] = out.Ex; so.out[1] = out.Ey; so.out[2] = out.Ez;
+        so.out[3] = out.Bx; so.out[4] = out.By; so.out[5] = out.Bz;
+    }
+    LC3D_TRY(solve_fields(c, LC3D_F_ALL, in, so, s));
+    return move(pass + 1);
 }
 
 extern "C" {

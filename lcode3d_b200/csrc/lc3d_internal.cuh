@@ -113,6 +113,12 @@ int launch_move_estimate(const EstimateArgs& a, cudaStream_t s);
 int launch_move_smart(const MoveArgs& a, cudaStream_t s);
 int launch_deposit_main(const DepositArgs& a, cudaStream_t s);
 int deposit_fine_offset(int fineness);
+// Depositions of several simulations in one launch (batches): tiles of
+// DEP_MULTI_ROWS fine rows, CTA b of the launch takes tile b - cta_start[s]
+// of simulation s.
+constexpr int DEP_MULTI_ROWS = 8;
+int deposit_multi_tiles(const DepositArgs& a);
+int launch_deposit_multi(const DepositArgs* args_dev, const int* cta_start_dev, int n, int ctas, cudaStream_t s);
 int launch_deposit_finalize(const DepositFinalizeArgs& f, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
@@ -285,6 +291,8 @@ struct lc3d_ctx {
 // The xi-step schedule (lc3d_api.cu), and the run machinery (run.cu).
 int step_schedule(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& out, const double* beam,
                   cudaStream_t s);
+int step_schedule_segment(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& out,
+                          const double* beam, cudaStream_t s, int seg, DepositArgs* dep);
 int run_init(lc3d_ctx* c);
 void run_drop_graphs(lc3d_ctx* c);       // graphs of lc3d_run (re-captured on the next run)
 void run_free(lc3d_ctx* c);

@@ -231,10 +231,23 @@ struct FineParticle {
     double x, y, dro, djx, djy, djz;
 };
 
+#ifndef LC3D_DEP_ONE_DIVISION
+#define LC3D_DEP_ONE_DIVISION 0
+#endif
+
 // Deposit quantities from the mixed coarse values (lcode.py:651-655).
 __device__ __forceinline__ void particle_values(FineParticle& p, double m, double q, double px, double py,
                                                 double pz) {
     const double gamma_m = sqrt(m * m + px * px + py * py + pz * pz);
+#if LC3D_DEP_ONE_DIVISION
+    // dro = q / (1 - pz / gamma_m) = q gamma_m / (gamma_m - pz) and
+    // dj = p dro / gamma_m = p q / (gamma_m - pz): one division
+    const double qd = q / (gamma_m - pz);
+    p.dro = qd * gamma_m;
+    p.djx = px * qd;
+    p.djy = py * qd;
+    p.djz = pz * qd;
+#else
     // the two quotients by gamma_m from one reciprocal, each corrected by
     // its exact residual (div_h): the reference's divisions, one division
     // sequence fewer per particle
@@ -244,6 +257,7 @@ __device__ __forceinline__ void particle_values(FineParticle& p, double m, doubl
     p.djx = px * dro_g;
     p.djy = py * dro_g;
     p.djz = pz * dro_g;
+#endif
 }
 
 __device__ __forceinline__ FineParticle fine_particle(const DepositArgs& a, int fi, int fj) {
@@ -369,7 +383,7 @@ __device__ __forceinline__ double2 coarse_pair(const DepositArgs& a, int k, int 
 // TI fine rows x 32 fine columns per CTA, one warp per row (TI = 4, 8, 16:
 // 8, 4 or 2 resident CTAs per SM at 64 registers).
 template <int TI>
-__global__ void __launch_bounds__(TI * 32, 1024 / (TI * 32)) deposit_kernel(DepositArgs a) {
+__device__ __forceinline__ void deposit_tile(const DepositArgs& a, int tile_x, int tile_y) {
     constexpr int DEP2_TI = TI;
     constexpr int DEP2_THREADS = DEP2_TI * 32;
     constexpr int DEP2_BLOCKS = DEP2_THREADS / 4;
@@ -402,8 +416,8 @@ __global__ void __launch_bounds__(TI * 32, 1024 / (TI * 32)) deposit_kernel(Depo
 
     // ---- phase 1: one fine particle per thread; warp = fine row ----
     {
-        const int fi = (int)blockIdx.y * DEP2_TI + warp - a.fine_off;
-        const int fj = (int)blockIdx.x * 32 + lane - a.fine_off;
+        const int fi = tile_y * DEP2_TI + warp - a.fine_off;
+        const int fj = tile_x * 32 + lane - a.fine_off;
         const bool row_ok = fi >= 0 && fi < a.Nf, col_ok = fj >= 0 && fj < a.Nf;
         // every input of the particle first (independent loads), then the
         // coarse rows of the row table
@@ -625,6 +639,41 @@ __global__ void __launch_bounds__(TI * 32, 1024 / (TI * 32)) deposit_kernel(Depo
     DEP2_CLK(4);
 }
 
+// One tile per CTA: blockIdx.x / .y = tile column / row.
+template <int TI>
+__global__ void __launch_bounds__(TI * 32, 1024 / (TI * 32)) deposit_kernel(DepositArgs a) {
+    deposit_tile<TI>(a, blockIdx.x, blockIdx.y);
+}
+
+// Depositions of several simulations in one launch: CTA b takes the tile
+// b - cta_start[s] of simulation s (cta_start: prefix sums of the tile
+// counts, n + 1 entries), whose arguments are args[s].
+template <int TI>
+__global__ void __launch_bounds__(TI * 32, 1024 / (TI * 32))
+    deposit_multi_kernel(const DepositArgs* __restrict__ args, const int* __restrict__ cta_start, int n) {
+    __shared__ DepositArgs sa;
+    __shared__ int s_sim;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = n - 1;   // the last s with cta_start[s] <= blockIdx.x
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (cta_start[mid] <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+        }
+        s_sim = lo;
+    }
+    __syncthreads();
+    {
+        static_assert(sizeof(DepositArgs) % 4 == 0, "copied as words");
+        const int* src = reinterpret_cast<const int*>(args + s_sim);
+        int* dst = reinterpret_cast<int*>(&sa);
+        for (int w = threadIdx.x; w < (int)(sizeof(DepositArgs) / 4); w += blockDim.x) dst[w] = src[w];
+    }
+    __syncthreads();
+    const int t = (int)blockIdx.x - cta_start[s_sim];
+    const int ntx = (sa.Nf + sa.fine_off + 31) / 32;
+    deposit_tile<TI>(sa, t % ntx, t / ntx);
+}
+
 // Accumulators -> float64 (+ ion background), two cells per thread; the
 // accumulators are cleared for the next deposition. All eight 16-byte
 // accumulator loads of a thread are issued before any store (the clears
@@ -709,6 +758,8 @@ int particles_prepare() {
     LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(4)));
     LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(8)));
     LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dep2_smem(16)));
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(deposit_multi_kernel<DEP_MULTI_ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)dep2_smem(DEP_MULTI_ROWS)));
     return LC3D_OK;
 }
 
@@ -747,6 +798,19 @@ extern "C" int lc3d_debug_dep_clocks(long long* host) {
     return LC3D_OK;
 }
 #endif
+
+// Tiles of one simulation's deposition at the multi-simulation tile height.
+int deposit_multi_tiles(const DepositArgs& a) {
+    return ((a.Nf + a.fine_off + 31) / 32) * ((a.Nf + a.fine_off + DEP_MULTI_ROWS - 1) / DEP_MULTI_ROWS);
+}
+
+int launch_deposit_multi(const DepositArgs* args_dev, const int* cta_start_dev, int n, int ctas, cudaStream_t s) {
+    if (n <= 0 || ctas <= 0) return LC3D_OK;
+    deposit_multi_kernel<DEP_MULTI_ROWS><<<ctas, DEP_MULTI_ROWS * 32, dep2_smem(DEP_MULTI_ROWS), s>>>(
+        args_dev, cta_start_dev, n);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
 
 int launch_deposit_finalize(const DepositFinalizeArgs& f_in, cudaStream_t s) {
     DepositFinalizeArgs f = f_in;

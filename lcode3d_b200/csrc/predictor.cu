@@ -208,6 +208,157 @@ constexpr size_t conv_smem_bytes() {
 }
 
 // ---------------------------------------------------------------------------
+// Weight gradient on the tensor cores: for one tap,
+//     dW[tap][co][ci] = sum_p g[p][co] x[p + off(tap)][ci]
+// is a GEMM D = A B^T over K = pixels with A[co][p] = g[p][co] and
+// B[ci][p] = x[p + off][ci]. Both operands arrive from the NHWC arrays as
+// TMA boxes of 32 channels x 32 pixels (64-byte rows of channels, 64-byte
+// swizzle): channel-contiguous, i.e. MN-major, so the instruction descriptor
+// sets both major bits and the shared-memory descriptors use the canonical
+// MN-major 64-byte-swizzle layout ((4, m), (8, k)) : ((1, LBO), (4, SBO)) in
+// 16-byte units: a 32-channel group is one 64-byte row of a box, the next
+// group (the next box) LBO = 2 KiB further, 8-pixel row groups SBO = 512 bytes
+// apart. M = 128 output channels (rows past Cout are TMA zero fill), N = Cin.
+// A CTA sums one chunk of pixels for one tap in TMEM (f32) and adds its
+// partial to dW with float32 atomics. The bias gradient stays a plain
+// reduction. Pixels past the level and shifted rows outside it are zero
+// fill; the pad column of g is zero.
+// ---------------------------------------------------------------------------
+constexpr int WG_PIX = 32;                                  // K block: pixels per stage
+constexpr int WG_BOX = 32 * WG_PIX * 2;                     // one 32-channel x 32-pixel box: 2 KiB
+constexpr int WG_A_BYTES = 4 * WG_BOX;                      // 128 channels of g
+constexpr int WG_B_MAX = 4 * WG_BOX;                        // up to 128 channels of x
+constexpr int WG_STAGES = 4;
+
+struct WgradArgs {
+    CUtensorMap tg;                // g: [NP][CGp] bf16, box (32 channels, 32 pixels)
+    CUtensorMap tx;                // x: [NP][Cin] bf16, box (32, 32)
+    float* dw;                     // [9][Cout][Cin] float32, accumulated into
+    int Cout, Cin, Wp, NP, chunk;  // chunk: pixels per CTA (a multiple of 32)
+    uint32_t idesc;
+    long long wait_limit;
+    unsigned* err;
+};
+
+// MN-major shared-memory descriptor, 64-byte swizzle (version 1, sm_100).
+__device__ __forceinline__ uint64_t umma_desc_mn_sw64(uint32_t saddr, uint32_t lbo_bytes) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3fff);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3fff) << 16;   // next 32-channel group
+    d |= (uint64_t)(512 >> 4) << 32;                     // next 8-pixel row group
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)4 << 61;
+    return d;
+}
+
+__host__ __device__ constexpr uint32_t idesc_bf16_mn(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+__global__ void __launch_bounds__(CONV_THREADS, 1) conv_wgrad_tc_kernel(const __grid_constant__ WgradArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + WG_STAGES * WG_A_BYTES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + WG_STAGES * WG_B_MAX);
+    uint64_t* empty = full + WG_STAGES;
+    uint64_t* done = empty + WG_STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    __shared__ int s_fail;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tap = blockIdx.y, off = (tap / 3 - 1) * a.Wp + (tap % 3 - 1);
+    const int pa = blockIdx.x * a.chunk;
+    const int nkb = (min(a.NP, pa + a.chunk) - pa + WG_PIX - 1) / WG_PIX;
+    const int nbx = a.Cin / 32;                              // boxes of x per stage
+    const uint32_t tcols = (uint32_t)a.Cin;                  // 32, 64 or 128 columns
+    const uint32_t bytes = WG_A_BYTES + (uint32_t)nbx * WG_BOX;
+
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        for (int i = 0; i < WG_STAGES; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) tmem_alloc(tmem_slot, tcols);
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {   // ---- TMA producer ----
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int st = kb % WG_STAGES, round = kb / WG_STAGES;
+                if (round > 0 && !mbar_wait(&empty[st], (round - 1) & 1, a.wait_limit)) {
+                    s_fail = 1;
+                    break;
+                }
+                const int p = pa + kb * WG_PIX;
+                mbar_expect_tx(&full[st], bytes);
+                for (int c = 0; c < 4; ++c)   // channels 32c .. 32c + 31 of g (zero past Cout)
+                    tma_load_2d(sA + st * WG_A_BYTES + c * WG_BOX, &a.tg, &full[st], 32 * c, p);
+                for (int c = 0; c < nbx; ++c)
+                    tma_load_2d(sB + st * WG_B_MAX + c * WG_BOX, &a.tx, &full[st], 32 * c, p + off);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {   // ---- MMA issuer ----
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int st = kb % WG_STAGES, round = kb / WG_STAGES;
+                if (!mbar_wait(&full[st], round & 1, a.wait_limit)) {
+                    s_fail = 1;
+                    break;
+                }
+                fence_after();
+                const uint32_t a_base = smem_u32(sA + st * WG_A_BYTES);
+                const uint32_t b_base = smem_u32(sB + st * WG_B_MAX);
+#pragma unroll
+                for (int kk = 0; kk < WG_PIX / 16; ++kk)   // 16 pixels (two 8-row groups) per MMA
+                    umma_bf16(tmem, umma_desc_mn_sw64(a_base + kk * 1024, WG_BOX),
+                              umma_desc_mn_sw64(b_base + kk * 1024, WG_BOX), a.idesc, (kb | kk) ? 1u : 0u);
+                umma_commit(&empty[st]);
+            }
+            umma_commit(done);
+        }
+    } else {   // ---- epilogue: warps 2..5 read TMEM lanes 32 (warp % 4) .. +31 (output channel) ----
+        const int quarter = warp & 3;
+        const int co = quarter * 32 + lane;
+        const bool ok = nkb > 0 && mbar_wait(done, 0, a.wait_limit);
+        if (nkb > 0 && !ok) s_fail = 1;
+        fence_after();
+        if (ok) {
+            const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+            for (int c0 = 0; c0 < a.Cin; c0 += 16) {
+                uint32_t r[16];
+                tmem_ld16(tmem + lane_base + c0, r);
+                tmem_wait_ld();
+                if (co < a.Cout) {
+                    float* d = a.dw + ((size_t)tap * a.Cout + co) * a.Cin + c0;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) atomicAdd(d + j, __uint_as_float(r[j]));
+                }
+            }
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (s_fail && threadIdx.x == 0) atomicOr(a.err, LC3D_FLAG_TIMEOUT);
+    if (warp == 1) {
+        fence_after();
+        tmem_dealloc(tmem, tcols);
+    }
+}
+
+constexpr size_t wgrad_smem_bytes() {
+    return 1024 + WG_STAGES * (WG_A_BYTES + WG_B_MAX) + (2 * WG_STAGES + 1) * 8 + 16;
+}
+
+// ---------------------------------------------------------------------------
 // Element-wise kernels
 // ---------------------------------------------------------------------------
 struct Level {
@@ -732,6 +883,8 @@ struct lc3d_predictor {
     long long wt_off[NLAYERS];
     float* zero_bias = nullptr;
     ConvArgs bconv[NLAYERS];
+    WgradArgs wg[NLAYERS];         // tensor-core weight gradient of each layer
+    int wg_chunks[NLAYERS];
     unsigned* err = nullptr;
     double* scale = nullptr;       // [23] per-sample channel scales (device)
     double* partial = nullptr;     // [STAT_BLOCKS][18]
@@ -798,13 +951,54 @@ int setup_bconv(lc3d_predictor* P, int l) {
     return LC3D_OK;
 }
 
-// dx = dL/d(input of layer l) from g = dL/d(output), zeroed where mask <= 0.
-int bwd_data_tc(lc3d_predictor* P, int l, const float* g, const __nv_bfloat16* mask, float* dx, cudaStream_t s) {
+// Layer l's output gradient g (float32) as bf16 in P->g_bf: the operand of
+// both tensor-core passes of the layer.
+int grad_bf16(lc3d_predictor* P, int l, const float* g, cudaStream_t s) {
     const LayerDef& d = LAYERS[l];
     const Level& L = P->lv[d.level];
     const int CGp = grad_channels(l);
     grad_to_bf16_kernel<<<blocks_for((long long)L.NP * CGp, 256), 256, 0, s>>>(g, d.cout, P->g_bf, CGp, L);
     LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+int setup_wgrad(lc3d_predictor* P, int l, const __nv_bfloat16* x) {
+    const LayerDef& d = LAYERS[l];
+    const Level& L = P->lv[d.level];
+    WgradArgs& a = P->wg[l];
+    memset(&a, 0, sizeof(a));
+    LC3D_TRY(make_map_2d(&a.tg, P->g_bf, L.NP, grad_channels(l), WG_PIX));
+    LC3D_TRY(make_map_2d(&a.tx, x, L.NP, d.cin, WG_PIX));
+    a.dw = P->grad + P->w_off[l];
+    a.Cout = d.cout;
+    a.Cin = d.cin;
+    a.Wp = L.Wp;
+    a.NP = L.NP;
+    // 16 pixel chunks per tap (9 x 16 CTAs), each a multiple of the K block
+    const int chunks = (int)std::min<long long>(16, (L.NP + WG_PIX - 1) / WG_PIX);
+    a.chunk = (int)(((L.NP + chunks - 1) / chunks + WG_PIX - 1) / WG_PIX * WG_PIX);
+    P->wg_chunks[l] = (L.NP + a.chunk - 1) / a.chunk;
+    a.idesc = idesc_bf16_mn(128, d.cin);
+    a.wait_limit = WAIT_LIMIT;
+    a.err = P->err;
+    return LC3D_OK;
+}
+
+// dW of layer l from P->g_bf (grad_bf16 first) and the bias gradient from g.
+int bwd_weights_tc(lc3d_predictor* P, int l, const float* g, cudaStream_t s) {
+    const WgradArgs& a = P->wg[l];
+    conv_wgrad_tc_kernel<<<dim3(P->wg_chunks[l], 9), CONV_THREADS, wgrad_smem_bytes(), s>>>(a);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    const Level& L = P->lv[LAYERS[l].level];
+    const int nchunks = (int)std::min<long long>(128, (L.NP + 1023) / 1024);
+    const int chunk = (L.NP + nchunks - 1) / nchunks;
+    bias_grad_kernel<<<(L.NP + chunk - 1) / chunk, 128, 0, s>>>(g, LAYERS[l].cout, P->grad + P->b_off[l], L.NP, chunk);
+    LC3D_CUDA_TRY(cudaGetLastError());
+    return LC3D_OK;
+}
+
+// dx = dL/d(input of layer l) from P->g_bf (grad_bf16 first), zeroed where mask <= 0.
+int bwd_data_tc(lc3d_predictor* P, int l, const __nv_bfloat16* mask, float* dx, cudaStream_t s) {
     ConvArgs a = P->bconv[l];
     a.out = dx;
     a.mask = mask;
@@ -867,34 +1061,38 @@ int backward(lc3d_predictor* P, float* loss, cudaStream_t s) {
                                                                 grad_channels(l), P->wt + P->wt_off[l]);
     }
     LC3D_CUDA_TRY(cudaGetLastError());
-#define LC3D_BWD_DATA(l, CIN, g, CG, mask, dx, lev) LC3D_TRY(bwd_data_tc(P, l, g, mask, dx, s))
+    // each layer: its output gradient in bf16 once, then the weight and data passes on it
+#define LC3D_BWD_W(l, CG, CIN, g, x) LC3D_TRY(grad_bf16(P, l, g, s)); LC3D_TRY(bwd_weights_tc(P, l, g, s))
+#define LC3D_BWD_DATA(l, CIN, g, CG, mask, dx, lev) LC3D_TRY(bwd_data_tc(P, l, mask, dx, s))
 #else
     const __nv_bfloat16* w = P->wbf;
+#define LC3D_BWD_W(l, CG, CIN, g, x) LC3D_TRY((bwd_weights<CG, CIN>(P, l, g, x, s)))
 #define LC3D_BWD_DATA(l, CIN, g, CG, mask, dx, lev) LC3D_TRY(bwd_data<CIN>(g, CG, w + P->w_off[l], mask, dx, lev, s))
 #endif
     loss_kernel<<<blocks_for(l0.NP, 256), 256, 0, s>>>(P->y, P->target, P->g_out, l0, loss);
     // conv6: d1 -> y
-    LC3D_TRY((bwd_weights<16, 32>(P, 5, P->g_out, P->d1, s)));
+    LC3D_BWD_W(5, 16, 32, P->g_out, P->d1);
     LC3D_BWD_DATA(5, 32, P->g_out, 16, P->d1, P->g_d1, l0);
     downsum_kernel<<<blocks_for((long long)l1.NP * 32, 256), 256, 0, s>>>(P->g_d1, l0, P->g_u2, l1, 32);
     // conv5: d2 -> u2
-    LC3D_TRY((bwd_weights<32, 64>(P, 4, P->g_u2, P->d2, s)));
+    LC3D_BWD_W(4, 32, 64, P->g_u2, P->d2);
     LC3D_BWD_DATA(4, 64, P->g_u2, 32, P->d2, P->g_d2, l1);
     downsum_kernel<<<blocks_for((long long)l2.NP * 64, 256), 256, 0, s>>>(P->g_d2, l1, P->g_u3, l2, 64);
     // conv4: e3 -> u3
-    LC3D_TRY((bwd_weights<64, 128>(P, 3, P->g_u3, P->e3, s)));
+    LC3D_BWD_W(3, 64, 128, P->g_u3, P->e3);
     LC3D_BWD_DATA(3, 128, P->g_u3, 64, P->e3, P->g_e3, l2);
     // conv3: p2 -> e3
-    LC3D_TRY((bwd_weights<128, 64>(P, 2, P->g_e3, P->p2, s)));
+    LC3D_BWD_W(2, 128, 64, P->g_e3, P->p2);
     LC3D_BWD_DATA(2, 64, P->g_e3, 128, nullptr, P->g_p2, l2);
     pool_bwd_mask_kernel<<<blocks_for((long long)l1.NP * 64, 256), 256, 0, s>>>(P->g_d2, P->e2, l1, P->g_p2, l2, 64);
     // conv2: p1 -> e2 (g_d2 now holds dL/d pre-activation of e2)
-    LC3D_TRY((bwd_weights<64, 32>(P, 1, P->g_d2, P->p1, s)));
+    LC3D_BWD_W(1, 64, 32, P->g_d2, P->p1);
     LC3D_BWD_DATA(1, 32, P->g_d2, 64, nullptr, P->g_p1, l1);
-#undef LC3D_BWD_DATA
     pool_bwd_mask_kernel<<<blocks_for((long long)l0.NP * 32, 256), 256, 0, s>>>(P->g_d1, P->e1, l0, P->g_p1, l1, 32);
     // conv1: x0 -> e1
-    LC3D_TRY((bwd_weights<32, 32>(P, 0, P->g_d1, P->x0, s)));
+    LC3D_BWD_W(0, 32, 32, P->g_d1, P->x0);
+#undef LC3D_BWD_W
+#undef LC3D_BWD_DATA
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
@@ -960,11 +1158,17 @@ int lc3d_predictor_create(int grid_steps, int device, lc3d_predictor** out) {
     if (rc == LC3D_OK) rc = setup_conv(P, 4, P->d2, P->u2);
     if (rc == LC3D_OK) rc = setup_conv(P, 5, P->d1, P->y);
     for (int l = 1; l < NLAYERS && rc == LC3D_OK; ++l) rc = setup_bconv(P, l);
+    {   // the input activation of each layer, for its weight gradient
+        const __nv_bfloat16* xin[NLAYERS] = {P->x0, P->p1, P->p2, P->e3, P->d2, P->d1};
+        for (int l = 0; l < NLAYERS && rc == LC3D_OK; ++l) rc = setup_wgrad(P, l, xin[l]);
+    }
     if (rc == LC3D_OK) {
         static bool attrs_set[64] = {};
         bool& attrs = attrs_set[device & 63];
         if (!attrs) {
             cudaFuncSetAttribute(conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem_bytes());
+            cudaFuncSetAttribute(conv_wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)wgrad_smem_bytes());
             cudaFuncSetAttribute(conv_bwd_data_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
             cudaFuncSetAttribute(conv_bwd_data_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
             cudaFuncSetAttribute(conv_bwd_data_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);

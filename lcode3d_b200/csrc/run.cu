@@ -92,6 +92,28 @@ int enqueue_step(lc3d_ctx* c, int par, cudaStream_t s) {
     return LC3D_OK;
 }
 
+// Segment `seg` of one whole xi step (step_schedule_segment): the device
+// beam opens segment 0 and the Ez(0,0) record closes segment 3.
+int enqueue_step_segment(lc3d_ctx* c, int par, cudaStream_t s, int seg, DepositArgs* dep) {
+    const int N = c->N;
+    if (seg == 0) {
+        ProfScope ps(c, LC3D_STAGE_OTHER, s);
+        LC3D_CUDA_TRY(launch_pdl(beam_kernel, dim3((N * N + 255) / 256), dim3(256), 0, s, c->beam_buf, N,
+                                 c->p.grid_step_size, c->p.xi_step_size, c->beam_A, c->beam_sr, c->beam_lf,
+                                 static_cast<const RunCtl*>(c->run_ctl)));
+        LC3D_CUDA_TRY(cudaGetLastError());
+    }
+    LC3D_TRY(step_schedule_segment(c, c->st[par], c->st[par ^ 1], c->beam_buf, s, seg, dep));
+    if (seg == 3) {
+        ProfScope ps(c, LC3D_STAGE_OTHER, s);
+        LC3D_CUDA_TRY(launch_pdl(record_kernel, dim3(1), dim3(32), 0, s,
+                                 static_cast<const double*>(c->st[par ^ 1].Ez), (N / 2) * N + N / 2,
+                                 static_cast<RunCtl*>(c->run_ctl)));
+        LC3D_CUDA_TRY(cudaGetLastError());
+    }
+    return LC3D_OK;
+}
+
 // Capture one xi step from state parity `par` into c->graph[par].
 int capture(lc3d_ctx* c, int par) {
     cudaStream_t cs;
@@ -234,6 +256,13 @@ struct lc3d_batch {
     cudaEvent_t* join;
     cudaGraphExec_t g[2];
     long long launches;        // kernel launches per batch step
+    // multi-deposit mode: every deposition point of a step is one launch
+    // over all simulations (deposit_multi_kernel) between segments of the
+    // simulations' steps
+    int multi;
+    DepositArgs* dargs;        // device [2 phases][3 depositions][n]
+    int* dcta;                 // device [n + 1]: prefix sums of the simulations' tile counts
+    int dctas;
 };
 
 namespace {
@@ -289,9 +318,103 @@ int batch_capture(lc3d_batch* b, int ph) {
     return rc;
 }
 
+// Multi-deposit capture: the step of every simulation in four segments on
+// its branch; after segments 0-2 the branches join, one deposit_multi_kernel
+// launch does all simulations' depositions, and the branches fork again.
+// The depositions' arguments are gathered on the host during the capture and
+// copied to b->dargs after it (the graph holds only their device address).
+int batch_capture_multi(lc3d_batch* b, int ph) {
+    int rc = LC3D_OK;
+    cudaGraph_t g = nullptr;
+    long long count = 0;
+    const int n = b->n;
+    DepositArgs* host = new DepositArgs[3 * n]();
+    // the launch's work list: tile offsets of the simulations (they depend on
+    // the fine lattice only), known before the capture fixes the grid size
+    int* start = new int[n + 1];
+    start[0] = 0;
+    for (int i = 0; i < n; ++i) {
+        lc3d_ctx* c = b->c[i];
+        DepositArgs t{};
+        t.Nf = c->Nf;
+        t.fine_off = deposit_fine_offset(c->p.plasma_fineness);
+        start[i + 1] = start[i] + deposit_multi_tiles(t);
+        memset(c->graph_launches[b->par0[i] ^ ph], 0, sizeof(c->graph_launches[0]));   // gathered over segments
+    }
+    b->dctas = start[n];
+    if (cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        delete[] host;
+        delete[] start;
+        return LC3D_ERR_CUDA;
+    }
+    for (int seg = 0; seg < 4 && rc == LC3D_OK; ++seg) {
+        if (cudaEventRecord(b->fork, b->cap) != cudaSuccess) rc = LC3D_ERR_CUDA;
+        for (int i = 0; i < n && rc == LC3D_OK; ++i) {
+            lc3d_ctx* c = b->c[i];
+            const int par = b->par0[i] ^ ph;
+            if (cudaStreamWaitEvent(b->br[i], b->fork, 0) != cudaSuccess) {
+                rc = LC3D_ERR_CUDA;
+                break;
+            }
+            long long saved[LC3D_NSTAGES];
+            memcpy(saved, c->launches, sizeof(saved));
+            memset(c->launches, 0, sizeof(c->launches));
+            c->capturing = 1;
+            DepositArgs dummy{};
+            rc = enqueue_step_segment(c, par, b->br[i], seg, seg < 3 ? &host[seg * n + i] : &dummy);
+            c->capturing = 0;
+            for (int q = 0; q < LC3D_NSTAGES; ++q) {
+                count += c->launches[q];
+                c->graph_launches[par][q] += c->launches[q];
+            }
+            memcpy(c->launches, saved, sizeof(saved));
+            if (rc == LC3D_OK && (cudaEventRecord(b->join[i], b->br[i]) != cudaSuccess ||
+                                  cudaStreamWaitEvent(b->cap, b->join[i], 0) != cudaSuccess))
+                rc = LC3D_ERR_CUDA;
+        }
+        if (seg < 3 && rc == LC3D_OK) {
+            rc = launch_deposit_multi(b->dargs + ((size_t)ph * 3 + seg) * n, b->dcta, n, b->dctas, b->cap);
+            // the batch's deposition launch is counted on the first simulation's context
+            b->c[0]->graph_launches[b->par0[0] ^ ph][LC3D_STAGE_DEPOSIT] += 1;
+            count += 1;
+        }
+    }
+    const cudaError_t e = cudaStreamEndCapture(b->cap, &g);
+    if (rc == LC3D_OK && e != cudaSuccess) {
+        lc3d_set_last_cuda_error(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+        rc = LC3D_ERR_CUDA;
+    }
+    if (rc == LC3D_OK) {
+        const cudaError_t ei = cudaGraphInstantiate(&b->g[ph], g, 0);
+        if (ei != cudaSuccess) {
+            lc3d_set_last_cuda_error(ei, "cudaGraphInstantiate", __FILE__, __LINE__);
+            b->g[ph] = nullptr;
+            rc = LC3D_ERR_CUDA;
+        }
+    }
+    if (g) cudaGraphDestroy(g);
+    if (rc == LC3D_OK) {
+        // the work list and this phase's deposition arguments, before any replay
+        cudaError_t ec = cudaMemcpy(b->dcta, start, (size_t)(n + 1) * sizeof(int), cudaMemcpyHostToDevice);
+        if (ec == cudaSuccess)
+            ec = cudaMemcpy(b->dargs + (size_t)ph * 3 * n, host, (size_t)3 * n * sizeof(DepositArgs),
+                            cudaMemcpyHostToDevice);
+        if (ec != cudaSuccess) {
+            lc3d_set_last_cuda_error(ec, "cudaMemcpy", __FILE__, __LINE__);
+            rc = LC3D_ERR_CUDA;
+        }
+    }
+    delete[] start;
+    delete[] host;
+    b->launches = count;
+    return rc;
+}
+
 void batch_free(lc3d_batch* b) {
     if (!b) return;
     batch_drop(b);
+    if (b->dargs) cudaFree(b->dargs);
+    if (b->dcta) cudaFree(b->dcta);
     if (b->br)
         for (int i = 0; i < b->n; ++i)
             if (b->br[i]) cudaStreamDestroy(b->br[i]);
@@ -344,6 +467,26 @@ extern "C" int lc3d_batch_create(lc3d_ctx* const* ctxs, int count, lc3d_batch** 
     return LC3D_OK;
 }
 
+extern "C" int lc3d_batch_set_mode(lc3d_batch* b, int multi_deposit) {
+    if (!b || (multi_deposit != 0 && multi_deposit != 1)) return LC3D_ERR_PARAM;
+    int prev = -1;
+    LC3D_CUDA_TRY(cudaGetDevice(&prev));
+    if (prev != b->device) LC3D_CUDA_TRY(cudaSetDevice(b->device));
+    int rc = LC3D_OK;
+    if (cudaDeviceSynchronize() != cudaSuccess) rc = LC3D_ERR_CUDA;   // no replay of the old graphs in flight
+    if (rc == LC3D_OK) {
+        batch_drop(b);   // captured again, in the new form, by the next run
+        b->multi = multi_deposit;
+        if (multi_deposit && !b->dargs) {
+            if (cudaMalloc(&b->dargs, (size_t)6 * b->n * sizeof(DepositArgs)) != cudaSuccess ||
+                cudaMalloc(&b->dcta, (size_t)(b->n + 1) * sizeof(int)) != cudaSuccess)
+                rc = LC3D_ERR_CUDA;
+        }
+    }
+    if (prev != b->device) cudaSetDevice(prev);
+    return rc;
+}
+
 extern "C" int lc3d_batch_destroy(lc3d_batch* b) {
     if (!b) return LC3D_OK;
     cudaDeviceSynchronize();
@@ -378,7 +521,7 @@ extern "C" int lc3d_batch_run(lc3d_batch* b, const int* xi0, int nsteps, double*
             if (!b->c[i]->graph[0] && rc == LC3D_OK) rc = capture(b->c[i], 0);
             if (!b->c[i]->graph[1] && rc == LC3D_OK) rc = capture(b->c[i], 1);
         }
-        for (int ph = 0; ph < 2 && rc == LC3D_OK; ++ph) rc = batch_capture(b, ph);
+        for (int ph = 0; ph < 2 && rc == LC3D_OK; ++ph) rc = b->multi ? batch_capture_multi(b, ph) : batch_capture(b, ph);
     }
     for (int i = 0; i < b->n && rc == LC3D_OK; ++i) {
         set_ctl_kernel<<<1, 32, 0, s>>>(static_cast<RunCtl*>(b->c[i]->run_ctl), xi0[i],

@@ -67,17 +67,17 @@ def conv(x, w, b):
     return y + b
 
 
-def conv_bwd(x, w, g, g_data=None):
-    """(dL/dx, dL/dW, dL/db) of y = conv(x, w, b) given g = dL/dy. dL/dx is
-    computed from ``g_data`` when it is given: the GPU's backward data pass
-    runs on the tensor cores and reads g rounded to bf16 (the weight and
-    bias gradients use g as it is)."""
-    gd = g if g_data is None else g_data
+def conv_bwd(x, w, g, g_bf=None):
+    """(dL/dx, dL/dW, dL/db) of y = conv(x, w, b) given g = dL/dy. dL/dx and
+    dL/dW are computed from ``g_bf`` when it is given: the GPU's backward
+    data and weight passes run on the tensor cores and read g rounded to
+    bf16; the bias gradient uses g as it is."""
+    gd = g if g_bf is None else g_bf
     dw = np.zeros_like(w)
     dx = np.zeros(x.shape)
     for tap in range(9):
         dy_, dx_ = tap // 3 - 1, tap % 3 - 1
-        dw[tap] = np.einsum('hwo,hwi->oi', g, _shift(x, dy_, dx_))
+        dw[tap] = np.einsum('hwo,hwi->oi', gd, _shift(x, dy_, dx_))
         dx += _shift(gd, -dy_, -dx_) @ w[tap]
     return dx, dw, g.sum(axis=(0, 1))
 
@@ -151,7 +151,7 @@ def loss_and_grad(params, x0, target, use_bf16=True):
     loss = float((d ** 2).sum() / (N_OUT * H * W))
     g = 2.0 * d / (N_OUT * H * W)
     L = c['L']
-    # the output gradients the backward data passes read: bf16 on the GPU
+    # the output gradients the backward data and weight passes read: bf16 on the GPU
     RG = (lambda a: bf16(a).astype(np.float64)) if use_bf16 else (lambda a: a)
     grads = [None] * 6
     # conv6
@@ -172,7 +172,7 @@ def loss_and_grad(params, x0, target, use_bf16=True):
     gp1, *grads[1] = conv_bwd(c['p1'], L[1][0], ge2, RG(ge2))
     ge1 = (gd1 + pool_bwd(gp1, c['n1'], c['e1'].shape)) * (c['e1'] > 0)
     # conv1
-    _, *grads[0] = conv_bwd(c['x0'], L[0][0], ge1)
+    _, *grads[0] = conv_bwd(c['x0'], L[0][0], ge1, RG(ge1))
     flat = np.concatenate([np.concatenate([dw.ravel(), db.ravel()]) for dw, db in grads])
     return loss, flat, y
 

@@ -69,15 +69,18 @@ def test_checkpoint_resume(L, tmp_path):
         assert torch.equal(getattr(s2, k), getattr(straight, k)), k
 
 
-def test_batch_matches_individual_runs(L):
+@pytest.mark.parametrize('multi', [False, True])
+def test_batch_matches_individual_runs(L, multi):
     """Four simulations of two grid sizes advanced by one graph launch per
-    step give bit-identical results to running each on its own."""
+    step give bit-identical results to running each on its own, with the
+    depositions on each simulation's branch or as one launch over all
+    simulations per deposition point."""
     from lcode3d_b200 import batch as B
     specs = [dict(grid_steps=N, grid_step_size=16.0 / (N - 1), xi_step_size=0.01, amplitude=A,
                   sigma_r=sr, length_factor=lf)
              for N, A, sr, lf in ((161, 0.3, 1.0, 1.0), (321, 0.05, 0.7, 1.3), (161, 0.8, 1.5, 0.6),
                                   (321, 0.5, 1.0, 1.0))]
-    bt = B.Batch(specs)
+    bt = B.Batch(specs, multi_deposit=multi)
     hist = [h.clone() for h in bt.run(30)]
     hist2 = bt.run(15)
     bt.check_errors()
