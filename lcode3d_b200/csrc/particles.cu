@@ -627,13 +627,19 @@ __device__ __forceinline__ void deposit_tile(const DepositArgs& a, int tile_x, i
 
     // ---- phase 3: split each touched window cell once, add to global ----
     if (s_bb[0] <= s_bb[1]) {
+        // lane = window column (the window is 32 cells wide), warps step over
+        // the rows of each field: consecutive lanes add to consecutive cells
         const int ni = min(s_bb[1] + 2 - oi, DEP2_WR), nj = min(s_bb[3] + 2 - oj, DEP2_WC);
-        const int cells = ni * nj;
-        for (int w = t; w < 4 * cells; w += DEP2_THREADS) {
-            const int q = w / cells, rc = w - q * cells, r = rc / nj, c = rc - r * nj;
-            const double v = s_win[q * DEP2_WIN + r * DEP2_WC + c];
-            if (v != 0.0)
-                fx_add(a.acc + (2 * q) * NN, a.acc + (2 * q + 1) * NN, (size_t)(oi + r) * N + (oj + c), v);
+        static_assert(DEP2_WC == 32, "one lane per window column");
+        if (lane < nj) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                unsigned long long* hi = a.acc + (2 * q) * NN;
+                for (int r = warp; r < ni; r += DEP2_TI) {
+                    const double v = s_win[q * DEP2_WIN + r * DEP2_WC + lane];
+                    if (v != 0.0) fx_add(hi, hi + NN, (size_t)(oi + r) * N + (oj + lane), v);
+                }
+            }
         }
     }
     DEP2_CLK(4);
