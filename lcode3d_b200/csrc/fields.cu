@@ -50,12 +50,16 @@ __device__ __forceinline__ double div_by(double x, double d, double inv_d) {
     return fma(fma(-q0, d, x), inv_d, q0);
 }
 
-__global__ void __launch_bounds__(256) rhs_kernel(const __grid_constant__ RhsArgs a) {
+// One grid row per grid line i (blockIdx.y), 128 cells of it per CTA: the
+// cell's coordinates come without an integer division.
+constexpr int RHS_THREADS = 128;
+
+__global__ void __launch_bounds__(RHS_THREADS) rhs_kernel(const __grid_constant__ RhsArgs a) {
     pdl_wait();
     const int N = a.N;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= N * N) return;
-    const int i = k / N, j = k - i * N;
+    const int i = blockIdx.y, j = blockIdx.x * RHS_THREADS + threadIdx.x;
+    if (j >= N) return;
+    const int k = i * N + j;
     const bool interior = i >= 1 && i <= N - 2 && j >= 1 && j <= N - 2;
     const SolveInputs& in = a.in;
     const double h2 = a.h * 2;
@@ -481,7 +485,8 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
     for (int f = 0; f < 6; ++f) ra.out[f] = on[f] ? c->rhs[f] : nullptr;
     {
         ProfScope ps(c, LC3D_STAGE_RHS, s);
-        LC3D_CUDA_TRY(launch_pdl(rhs_kernel, dim3((n + 255) / 256), dim3(256), 0, s, ra));
+        LC3D_CUDA_TRY(launch_pdl(rhs_kernel, dim3((c->N + RHS_THREADS - 1) / RHS_THREADS, c->N), dim3(RHS_THREADS), 0,
+                                 s, ra));
         LC3D_CUDA_TRY(cudaGetLastError());
     }
 

@@ -38,11 +38,14 @@
 // bounded; on time-out the kernel sets an error flag and exits, and TMEM is
 // always freed.
 //
-// Training (float32 SIMT kernels): backward data (the transposed 3x3
-// convolution), weight and bias gradients (reductions over pixels), the
-// pooling / upsampling / ReLU adjoints, an MSE loss on the 5 fields and
-// Adam. Weights are kept as float32 master copies; the bf16 copies the
-// forward pass reads are refreshed after every update.
+// Training: both gradient passes of every convolution on the tensor cores
+// in bf16 -- the data gradient as the forward convolution of the bf16 output
+// gradient with flipped, transposed weights, the weight gradient as an
+// implicit GEMM over pixels with MN-major operands -- and float32 SIMT
+// kernels for the bias gradients, the pooling / upsampling / ReLU adjoints,
+// an MSE loss on the 5 fields and Adam. Weights are kept as float32 master
+// copies; the bf16 copies the forward pass reads are refreshed after every
+// update.
 
 #include <cuda_bf16.h>
 
@@ -637,119 +640,9 @@ __global__ void flip_weights_kernel(const __nv_bfloat16* __restrict__ w, int CG,
 }
 
 // ---------------------------------------------------------------------------
-// Training kernels (float32)
+// Training kernels (float32): bias gradients, pooling / upsampling / ReLU
+// adjoints and Adam
 // ---------------------------------------------------------------------------
-constexpr int BWD_THREADS = 256;
-constexpr int BWD_PIX = 64;
-
-// dX[p][ci] = sum_tap sum_co g[p - off(tap)][co] W[tap][co][ci], times
-// (mask[p][ci] > 0) when a mask is given; zero in the pad column.
-template <int CIN>
-__global__ void __launch_bounds__(BWD_THREADS) conv_bwd_data_kernel(const float* __restrict__ g, int CG,
-                                                                    const __nv_bfloat16* __restrict__ w,
-                                                                    const __nv_bfloat16* __restrict__ mask,
-                                                                    float* __restrict__ dx, Level L) {
-    extern __shared__ float sm[];
-    const int GP = CG + 1;                         // padded row of gs
-    float* gs = sm;                                // [BWD_PIX][CG + 1]
-    float* ws = sm + BWD_PIX * GP;                 // [CG][CIN]
-    constexpr int CGRP = CIN / 4, PGRP = BWD_THREADS / CGRP, PPT = BWD_PIX / PGRP;
-    const int cg = threadIdx.x % CGRP, pg = threadIdx.x / CGRP;
-    const int p0 = blockIdx.x * BWD_PIX;
-    float acc[PPT][4];
-#pragma unroll
-    for (int i = 0; i < PPT; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
-    for (int tap = 0; tap < 9; ++tap) {
-        const int off = (tap / 3 - 1) * L.Wp + (tap % 3 - 1);
-        __syncthreads();
-        for (int i = threadIdx.x; i < BWD_PIX * CG; i += BWD_THREADS) {
-            const int px = i / CG, co = i - px * CG;
-            const int q = p0 + px - off;
-            gs[px * GP + co] = (q >= 0 && q < L.NP) ? g[(size_t)q * CG + co] : 0.0f;
-        }
-        for (int i = threadIdx.x; i < CG * CIN; i += BWD_THREADS)
-            ws[i] = __bfloat162float(w[(size_t)tap * CG * CIN + i]);
-        __syncthreads();
-        for (int co = 0; co < CG; ++co) {
-            const float4 wv = *reinterpret_cast<const float4*>(ws + co * CIN + 4 * cg);
-#pragma unroll
-            for (int i = 0; i < PPT; ++i) {
-                const float gv = gs[(pg * PPT + i) * GP + co];
-                acc[i][0] += gv * wv.x;
-                acc[i][1] += gv * wv.y;
-                acc[i][2] += gv * wv.z;
-                acc[i][3] += gv * wv.w;
-            }
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < PPT; ++i) {
-        const int p = p0 + pg * PPT + i;
-        if (p >= L.NP) continue;
-        const bool pad = (p % L.Wp) >= L.W;
-        float v[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            v[j] = pad ? 0.0f : acc[i][j];
-            if (mask && !(__bfloat162float(mask[(size_t)p * CIN + 4 * cg + j]) > 0.0f)) v[j] = 0.0f;
-        }
-        *reinterpret_cast<float4*>(dx + (size_t)p * CIN + 4 * cg) = make_float4(v[0], v[1], v[2], v[3]);
-    }
-}
-
-// dW[tap][co][ci] += sum_p g[p][co] x[p + off(tap)][ci] over one chunk of
-// pixels (blockIdx.x) for one tap (blockIdx.y).
-constexpr int WG_SUB = 32;
-template <int CG, int CIN>
-__global__ void __launch_bounds__(BWD_THREADS) conv_bwd_w_kernel(const float* __restrict__ g,
-                                                                 const __nv_bfloat16* __restrict__ x,
-                                                                 float* __restrict__ dw, Level L, int chunk) {
-    __shared__ float gs[WG_SUB][CG];
-    __shared__ __align__(16) float xs[WG_SUB][CIN];
-    constexpr int CGRP = CIN / 4, OGRP = BWD_THREADS / CGRP;
-    constexpr int ROWS = CG >= OGRP ? CG / OGRP : 1;
-    const int cg = threadIdx.x % CGRP, og = threadIdx.x / CGRP;
-    const int tap = blockIdx.y, off = (tap / 3 - 1) * L.Wp + (tap % 3 - 1);
-    const int pa = blockIdx.x * chunk, pb = min(L.NP, pa + chunk);
-    float acc[ROWS][4];
-#pragma unroll
-    for (int r = 0; r < ROWS; ++r)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[r][j] = 0.0f;
-    for (int s0 = pa; s0 < pb; s0 += WG_SUB) {
-        __syncthreads();
-        for (int i = threadIdx.x; i < WG_SUB * CG; i += BWD_THREADS) {
-            const int px = i / CG, co = i - px * CG, p = s0 + px;
-            gs[px][co] = p < pb ? g[(size_t)p * CG + co] : 0.0f;
-        }
-        for (int i = threadIdx.x; i < WG_SUB * CIN; i += BWD_THREADS) {
-            const int px = i / CIN, ci = i - px * CIN, q = s0 + px + off;
-            xs[px][ci] = (s0 + px < pb && q >= 0 && q < L.NP) ? __bfloat162float(x[(size_t)q * CIN + ci]) : 0.0f;
-        }
-        __syncthreads();
-        if (og * ROWS < CG) {
-            for (int px = 0; px < WG_SUB; ++px) {
-                const float4 xv = *reinterpret_cast<const float4*>(&xs[px][4 * cg]);
-#pragma unroll
-                for (int r = 0; r < ROWS; ++r) {
-                    const float gv = gs[px][og * ROWS + r];
-                    acc[r][0] += gv * xv.x;
-                    acc[r][1] += gv * xv.y;
-                    acc[r][2] += gv * xv.z;
-                    acc[r][3] += gv * xv.w;
-                }
-            }
-        }
-    }
-    if (og * ROWS >= CG) return;
-#pragma unroll
-    for (int r = 0; r < ROWS; ++r)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            atomicAdd(dw + ((size_t)tap * CG + og * ROWS + r) * CIN + 4 * cg + j, acc[r][j]);
-}
 
 // db[co] += sum_p g[p][co] over one chunk of pixels.
 __global__ void bias_grad_kernel(const float* __restrict__ g, int CG, float* __restrict__ db, int NP, int chunk) {
@@ -1007,29 +900,6 @@ int bwd_data_tc(lc3d_predictor* P, int l, const __nv_bfloat16* mask, float* dx, 
     return LC3D_OK;
 }
 
-template <int CIN>
-int bwd_data(const float* g, int CG, const __nv_bfloat16* w, const __nv_bfloat16* mask, float* dx, const Level& L,
-             cudaStream_t s) {
-    const size_t smem = ((size_t)BWD_PIX * (CG + 1) + (size_t)CG * CIN) * sizeof(float);
-    conv_bwd_data_kernel<CIN><<<blocks_for(L.NP, BWD_PIX), BWD_THREADS, smem, s>>>(g, CG, w, mask, dx, L);
-    LC3D_CUDA_TRY(cudaGetLastError());
-    return LC3D_OK;
-}
-
-template <int CG, int CIN>
-int bwd_weights(lc3d_predictor* P, int l, const float* g, const __nv_bfloat16* x, cudaStream_t s) {
-    const Level& L = P->lv[LAYERS[l].level];
-    const int nchunks = (int)std::min<long long>(128, (L.NP + 1023) / 1024);
-    int chunk = (L.NP + nchunks - 1) / nchunks;
-    chunk = (chunk + WG_SUB - 1) / WG_SUB * WG_SUB;
-    const int nc = (L.NP + chunk - 1) / chunk;
-    conv_bwd_w_kernel<CG, CIN><<<dim3(nc, 9), BWD_THREADS, 0, s>>>(g, x, P->grad + P->w_off[l], L, chunk);
-    LC3D_CUDA_TRY(cudaGetLastError());
-    bias_grad_kernel<<<nc, 128, 0, s>>>(g, CG, P->grad + P->b_off[l], L.NP, chunk);
-    LC3D_CUDA_TRY(cudaGetLastError());
-    return LC3D_OK;
-}
-
 int forward(lc3d_predictor* P, cudaStream_t s) {
     const Level *l0 = &P->lv[0], *l1 = &P->lv[1], *l2 = &P->lv[2];
     LC3D_TRY(run_conv(P, 0, s));
@@ -1046,14 +916,9 @@ int forward(lc3d_predictor* P, cudaStream_t s) {
     return LC3D_OK;
 }
 
-#ifndef LC3D_PRED_BWD_TC
-#define LC3D_PRED_BWD_TC 1                  // backward data pass on the tensor cores (else float32 SIMT)
-#endif
-
 int backward(lc3d_predictor* P, float* loss, cudaStream_t s) {
     const Level &l0 = P->lv[0], &l1 = P->lv[1], &l2 = P->lv[2];
     LC3D_CUDA_TRY(cudaMemsetAsync(P->grad, 0, (size_t)P->np * sizeof(float), s));
-#if LC3D_PRED_BWD_TC
     // the flipped, transposed bf16 weights of the layers whose input gradient is needed
     for (int l = 1; l < NLAYERS; ++l) {
         const int n = 9 * LAYERS[l].cin * grad_channels(l);
@@ -1064,11 +929,6 @@ int backward(lc3d_predictor* P, float* loss, cudaStream_t s) {
     // each layer: its output gradient in bf16 once, then the weight and data passes on it
 #define LC3D_BWD_W(l, CG, CIN, g, x) LC3D_TRY(grad_bf16(P, l, g, s)); LC3D_TRY(bwd_weights_tc(P, l, g, s))
 #define LC3D_BWD_DATA(l, CIN, g, CG, mask, dx, lev) LC3D_TRY(bwd_data_tc(P, l, mask, dx, s))
-#else
-    const __nv_bfloat16* w = P->wbf;
-#define LC3D_BWD_W(l, CG, CIN, g, x) LC3D_TRY((bwd_weights<CG, CIN>(P, l, g, x, s)))
-#define LC3D_BWD_DATA(l, CIN, g, CG, mask, dx, lev) LC3D_TRY(bwd_data<CIN>(g, CG, w + P->w_off[l], mask, dx, lev, s))
-#endif
     loss_kernel<<<blocks_for(l0.NP, 256), 256, 0, s>>>(P->y, P->target, P->g_out, l0, loss);
     // conv6: d1 -> y
     LC3D_BWD_W(5, 16, 32, P->g_out, P->d1);
@@ -1169,9 +1029,6 @@ int lc3d_predictor_create(int grid_steps, int device, lc3d_predictor** out) {
             cudaFuncSetAttribute(conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem_bytes());
             cudaFuncSetAttribute(conv_wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)wgrad_smem_bytes());
-            cudaFuncSetAttribute(conv_bwd_data_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-            cudaFuncSetAttribute(conv_bwd_data_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-            cudaFuncSetAttribute(conv_bwd_data_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
             attrs = cudaGetLastError() == cudaSuccess;
             if (!attrs) rc = LC3D_ERR_CUDA;
         }
