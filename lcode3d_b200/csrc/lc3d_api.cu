@@ -356,6 +356,7 @@ void destroy(lc3d_ctx* c) {
         if (c->avg[k]) cudaFree(c->avg[k]);
     if (c->acc) cudaFree(c->acc);
     if (c->err) cudaFree(c->err);
+    if (c->err_host) cudaFreeHost(c->err_host);
     if (c->zeros) cudaFree(c->zeros);
     if (c->resid) cudaFree(c->resid);
     if (c->beam_dev) cudaFree(c->beam_dev);
@@ -579,6 +580,9 @@ int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out) {
     c->acc_plane = (ng + 31) / 32 * 32;
     LC3D_STEP(dalloc(&c->acc, c->acc_plane * 8));
     LC3D_STEP(dalloc(&c->err, (size_t)1));
+    // pinned host word the flag is read into (a direct copy, no staging)
+    if (rc == LC3D_OK && cudaHostAlloc(&c->err_host, sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess)
+        rc = LC3D_ERR_CUDA;
     LC3D_STEP(dalloc(&c->zeros, ng));
     LC3D_STEP(dalloc(&c->resid, (size_t)2));
     LC3D_STEP(dalloc(&c->beam_dev, ng));
@@ -959,9 +963,9 @@ int lc3d_set_tiles(lc3d_ctx* c, int deposit_rows, int fft_ctas_per_sm) {
 int lc3d_check_error(lc3d_ctx* c, void* stream) {
     if (!c) return LC3D_ERR_PARAM;
     DeviceGuard g(c->device);
-    unsigned flag = 0;
-    LC3D_CUDA_TRY(cudaMemcpyAsync(&flag, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost, S(stream)));
+    LC3D_CUDA_TRY(cudaMemcpyAsync(c->err_host, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost, S(stream)));
     LC3D_CUDA_TRY(cudaStreamSynchronize(S(stream)));
+    const unsigned flag = *c->err_host;
     if (flag) LC3D_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(unsigned), S(stream)));
     if (flag & LC3D_FLAG_WINDOW) return LC3D_ERR_WINDOW;
     if (flag & LC3D_FLAG_NONFINITE) return LC3D_ERR_NONFINITE;

@@ -240,6 +240,7 @@ struct lc3d_ctx {
     unsigned long long* acc;              // deposit fixed-point accumulators, 8 planes
     size_t acc_plane;                     // plane stride in words
     unsigned* err;                        // device error flag
+    unsigned* err_host;                   // pinned host word lc3d_check_error reads it into
     double* zeros;                        // N x N zeros (absent beam)
     unsigned long long* resid;            // predicted-step residual maxima (2 words, double bits)
     double* diag_w;                       // zn diagnostic: Gaussian weights, then partial sums
