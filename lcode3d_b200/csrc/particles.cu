@@ -231,33 +231,21 @@ struct FineParticle {
     double x, y, dro, djx, djy, djz;
 };
 
-#ifndef LC3D_DEP_ONE_DIVISION
-#define LC3D_DEP_ONE_DIVISION 0
-#endif
-
 // Deposit quantities from the mixed coarse values (lcode.py:651-655).
 __device__ __forceinline__ void particle_values(FineParticle& p, double m, double q, double px, double py,
                                                 double pz) {
     const double gamma_m = sqrt(m * m + px * px + py * py + pz * pz);
-#if LC3D_DEP_ONE_DIVISION
-    // dro = q / (1 - pz / gamma_m) = q gamma_m / (gamma_m - pz) and
-    // dj = p dro / gamma_m = p q / (gamma_m - pz): one division
-    const double qd = q / (gamma_m - pz);
-    p.dro = qd * gamma_m;
-    p.djx = px * qd;
-    p.djy = py * qd;
-    p.djz = pz * qd;
-#else
     // the two quotients by gamma_m from one reciprocal, each corrected by
     // its exact residual (div_h): the reference's divisions, one division
-    // sequence fewer per particle
+    // sequence fewer per particle (the algebraically equal single division
+    // q / (gamma_m - pz) measured only 0.5 % faster and departs from the
+    // reference's rounding)
     const double inv_g = 1.0 / gamma_m;
     p.dro = q / (1 - div_h(pz, gamma_m, inv_g));
     const double dro_g = div_h(p.dro, gamma_m, inv_g);
     p.djx = px * dro_g;
     p.djy = py * dro_g;
     p.djz = pz * dro_g;
-#endif
 }
 
 __device__ __forceinline__ FineParticle fine_particle(const DepositArgs& a, int fi, int fj) {
