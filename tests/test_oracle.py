@@ -193,3 +193,22 @@ def test_run_n641_two_steps():
         scale = float(g['s2_maxabs_' + k])
         assert np.abs(a[320] - g['s2_axis_' + k]).max() <= 1e-12 * scale, k
         assert np.abs(np.diagonal(a) - g['s2_diag_' + k]).max() <= 1e-12 * scale, k
+
+
+def test_golden_floor_of_two_orders(tmp_path):
+    """make_golden's order-sensitivity floor: for each recorded quantity the
+    largest serial-vs-reversed difference relative to the serial values'
+    largest modulus, written beside the serial values."""
+    import make_golden as M
+    ser = {'Ez00': np.array([1.0, -2.0, 4.0]), 's500_axis_ro': np.array([0.5, 0.25]),
+           'steps': np.array(3000), 'snapshots': np.array([500])}
+    rev = {'Ez00': np.array([1.0, -2.0 + 4e-12, 4.0]), 's500_axis_ro': np.array([0.5, 0.25])}
+    a, b = tmp_path / 'ser.npz', tmp_path / 'rev.npz'
+    np.savez(a, **ser)
+    np.savez(b, **rev)
+    M.gen_cfg2_floor(str(a), str(b), str(a))
+    g = np.load(a)
+    assert abs(float(g['floor_Ez00']) - 1e-12) < 1e-15
+    assert g['floor_s500_axis_ro'] == 0.0
+    assert 'floor_steps' not in g.files and 'floor_snapshots' not in g.files
+    assert np.array_equal(g['Ez00'], ser['Ez00'])
