@@ -718,7 +718,7 @@ def run_learned_bench(args):
 def run_reference(args):
     threads = cpu_threads()
     K = max(1, min(args.steps, args.ref_max_steps))
-    W = min(args.warmup, 1)
+    W = max(0, min(args.warmup, 10))   # untimed warm-up steps (CPU steps are slow: at most 10)
     v = time_oracle(args.grid, K, threads, args.pre, W)
     cfg = make_config(args.grid, 'fp64')
     N = cfg.grid_steps

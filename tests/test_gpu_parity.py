@@ -348,3 +348,9 @@ def test_run_n641_full(L):
     worst.sort(reverse=True)
     print('641^2 x 3000 steps vs the reference, largest error/tolerance: ' +
           ', '.join(f'{k} {e:.1e} (tol {t:.1e})' for _, k, e, t in worst[:5]))
+    # the quantities the reference reproduces across deposition orders to 1e-9 or better
+    firm = sorted(((e, k, float(g['floor_' + k])) for _, k, e, t in worst if float(g['floor_' + k]) <= 1e-9),
+                  reverse=True)
+    print(f'{len(firm)} of {len(worst)} quantities have an order floor <= 1e-9; largest errors among them: ' +
+          ', '.join(f'{k} {e:.1e} (floor {f:.1e})' for e, k, f in firm[:5]) +
+          f"; Ez00 history {[e for e, k, f in firm if k == 'Ez00'][0]:.1e}")
