@@ -62,6 +62,23 @@ static_assert(FFT_THREADS % 32 == 0 && FFT_THREADS <= 1024, "whole warps");
 #define LC3D_FFT32_MIN_BLOCKS 5           // ... (float32 transforms)
 #endif
 constexpr int MAX_RADICES = 24;
+#ifndef LC3D_FFT_CLOCKS
+#define LC3D_FFT_CLOCKS 0                 // instrumented builds: per-CTA phase clocks of the last launch
+#endif
+#if LC3D_FFT_CLOCKS
+constexpr int FFT_NCLK = 8;               // wait, extension, four radix passes, readout, partial sums
+__device__ long long g_fft_clocks[4096][FFT_NCLK];
+#define FFT_CLK(k)                                        \
+    do {                                                  \
+        const long long t_ = clock64();                   \
+        clk[(k) < FFT_NCLK ? (k) : FFT_NCLK - 1] += t_ - clk_last; \
+        clk_last = t_;                                    \
+    } while (0)
+#else
+#define FFT_CLK(k) \
+    do {           \
+    } while (0)
+#endif
 constexpr int FFT_PAD = 4;               // complex words between the CTA's two FFTs (bank offset)
 
 struct FftField {
@@ -292,6 +309,10 @@ __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_ker
     Tin* stg = reinterpret_cast<Tin*>(A + FFT_PER_CTA * PS);   // [ROWS_PER_CTA][N]
     const V* tw = reinterpret_cast<const V*>(sizeof(T) == 8 ? static_cast<const void*>(b.tw)
                                                             : static_cast<const void*>(b.tw32));
+#if LC3D_FFT_CLOCKS
+    long long clk[FFT_NCLK] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long clk_last = clock64();
+#endif
     pdl_wait();
     int g = blockIdx.x;
     if (g < b.ngroups) stage_group(b, g, stg);
@@ -302,6 +323,7 @@ __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_ker
     const int n = F.type ? b.N - 2 : b.N;     // input / output length
     cp_async_wait_all();
     __syncthreads();                     // the staging area holds group g
+    FFT_CLK(0);
 
     // symmetric / antisymmetric extensions, rows 2q and 2q + 1 of the group
     // as the real and imaginary parts of FFT q, each staged element written
@@ -327,6 +349,7 @@ __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_ker
     if (F.type == 1 && threadIdx.x < 2 * FFT_PER_CTA)   // DST-I: zeros at m = 0 and m = L
         A[(threadIdx.x >> 1) * PS + (threadIdx.x & 1) * L] = cmk<V>((T)0, (T)0);
     __syncthreads();                     // the staging area is free: start the next group
+    FFT_CLK(1);
     if (g + (int)gridDim.x < b.ngroups) stage_group(b, g + gridDim.x, stg);
     int span = P;
     for (int p = 0; p < b.nrad; ++p) {
@@ -342,6 +365,7 @@ __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_ker
             default: fft_pass<5>(A, span, P, tw); break;
         }
         __syncthreads();
+        FFT_CLK(2 + p);
     }
     // transposed output: out[k][row] for the CTA's rows. The readout list
     // holds (position, k) for the wanted frequencies sorted by position, so
@@ -398,6 +422,7 @@ __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_ker
             }
         }
     }
+    FFT_CLK(6);
     if (F.partial) {   // uniform per CTA: fixed-order sum of everything this CTA wrote
         __syncthreads();   // the FFT buffer is free
         double* red = reinterpret_cast<double*>(fft_smem);
@@ -413,8 +438,13 @@ __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_ker
         }
     }
     __syncthreads();                     // the FFT buffer is free for the next group
+    FFT_CLK(7);
     }
     cp_async_wait_all();                 // nothing left in flight (no group was started past the end)
+#if LC3D_FFT_CLOCKS
+    if (threadIdx.x == 0 && blockIdx.x < 4096)
+        for (int k = 0; k < FFT_NCLK; ++k) g_fft_clocks[blockIdx.x][k] = clk[k];
+#endif
 }
 
 double sin_pi_frac(long long r, long long L) {
@@ -538,6 +568,16 @@ int fft_init(lc3d_ctx* c) {
     LC3D_CUDA_TRY(cudaMemcpy(c->fft_tw, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice));
     return LC3D_OK;
 }
+
+#if LC3D_FFT_CLOCKS
+// Instrumented builds only: phase clocks (summed over the CTA's row groups)
+// of the last fft_rows_kernel launch, [4096][FFT_NCLK] cycles, thread 0.
+extern "C" int lc3d_debug_fft_clocks(long long* host) {
+    LC3D_CUDA_TRY(cudaDeviceSynchronize());
+    LC3D_CUDA_TRY(cudaMemcpyFromSymbol(host, g_fft_clocks, sizeof(g_fft_clocks)));
+    return LC3D_OK;
+}
+#endif
 
 int fft_prepare(int P) {
     // the limit is per kernel, not per context: always the largest size any
