@@ -101,8 +101,12 @@ __global__ void __launch_bounds__(RHS_THREADS) rhs_kernel(const __grid_constant_
 }
 
 // ---------------------------------------------------------------------------
-// Batched float64 GEMM, C = A B (optionally C = Lambda o (A B)), row-major.
-// 64 x 64 tiles, k-step 16, 256 threads with 4 x 4 outputs each.
+// Batched float64 GEMM, C = A B (optionally C = Lambda o (A B)), row-major,
+// on the float64 tensor cores (mma.sync m8n8k4 .f64: each product and sum is
+// an IEEE float64 fused multiply-add). 128 x 64 tiles per 256-thread CTA,
+// eight warps in a 4 x 2 grid of 32 x 32 warp tiles (4 x 4 MMAs per k4
+// step); k-steps of 16 staged by cp.async into two shared-memory buffers,
+// the next k-step copied while the current one is multiplied.
 // ---------------------------------------------------------------------------
 constexpr int MAX_PROBS = 6;
 
@@ -118,11 +122,33 @@ struct GemmBatch {
     int count, total_tiles;
 };
 
-constexpr int GT = 64, GK = 16;
+constexpr int GTM = 128, GTN = 64, GK = 16;
+constexpr int GEMM_THREADS = 256;
+// shared pitches (doubles): the fragment loads of a half-warp (rows g = 0..3
+// or 4..7, columns t = 0..3) fall in distinct banks: 2 (20 g + t) and
+// 2 (68 t + g) mod 32 are distinct over the 16 lanes
+constexpr int AS_LD = GK + 4;    // As[m][k]
+constexpr int BS_LD = GTN + 4;   // Bs[k][n]
+constexpr int AS_SIZE = GTM * AS_LD, BS_SIZE = GK * BS_LD;
+constexpr size_t GEMM_SMEM = 2 * (size_t)(AS_SIZE + BS_SIZE) * sizeof(double);
 
-__global__ void __launch_bounds__(256) dgemm_kernel(const __grid_constant__ GemmBatch b) {
-    __shared__ double As[2][GK][GT + 1];
-    __shared__ double Bs[2][GK][GT];
+// 8-byte global -> shared copy; a source size of 0 writes zeros (the tile
+// edges past M, N or K).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool in) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(in ? 8 : 0) : "memory");
+}
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(GEMM_THREADS, 2) dgemm_kernel(const __grid_constant__ GemmBatch b) {
+    extern __shared__ __align__(16) double gsm[];   // As[2][GTM][AS_LD], Bs[2][GK][BS_LD]
+    double* As = gsm;
+    double* Bs = gsm + 2 * AS_SIZE;
     const int bid = blockIdx.x;
     int pi = 0;
 #pragma unroll 1
@@ -131,63 +157,73 @@ __global__ void __launch_bounds__(256) dgemm_kernel(const __grid_constant__ Gemm
     const GemmProb& P = b.p[pi];
     const int t = bid - P.tile_start;
     const int tm = t / P.tiles_n, tn = t - tm * P.tiles_n;
-    const int row0 = tm * GT, col0 = tn * GT;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int row0 = tm * GTM, col0 = tn * GTN;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, tq = lane & 3;            // fragment row group, thread in group
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
 
-    // load assignments
-    const int a_k = tid & 15, a_r = tid >> 4;        // rows a_r + 16 r
-    const int b_n = tid & 63, b_k = tid >> 6;        // k rows b_k + 4 r
-    double ra[4], rb[4];
-    auto load = [&](int k0) {
+    auto load = [&](int k0, int buf) {
+        double* as = As + buf * AS_SIZE;
+        double* bs = Bs + buf * BS_SIZE;
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int row = row0 + a_r + 16 * r, kk = k0 + a_k;
-            ra[r] = (row < P.M && kk < P.K) ? P.A[(size_t)row * P.lda + kk] : 0.0;
-            const int kb = k0 + b_k + 4 * r, col = col0 + b_n;
-            rb[r] = (kb < P.K && col < P.N) ? P.B[(size_t)kb * P.ldb + col] : 0.0;
+        for (int i = 0; i < GTM * GK / GEMM_THREADS; ++i) {   // 8: rows idx / 16, k idx % 16
+            const int idx = tid + i * GEMM_THREADS, r = idx >> 4, kk = idx & 15;
+            const int row = row0 + r, k = k0 + kk;
+            const bool in = row < P.M && k < P.K;
+            cp_async8(as + r * AS_LD + kk, in ? P.A + (size_t)row * P.lda + k : P.A, in);
         }
+#pragma unroll
+        for (int i = 0; i < GK * GTN / GEMM_THREADS; ++i) {   // 4: k rows idx / 64, columns idx % 64
+            const int idx = tid + i * GEMM_THREADS, kk = idx >> 6, n = idx & 63;
+            const int k = k0 + kk, col = col0 + n;
+            const bool in = k < P.K && col < P.N;
+            cp_async8(bs + kk * BS_LD + n, in ? P.B + (size_t)k * P.ldb + col : P.B, in);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    double acc[4][4];
+
+    double acc[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
     const int nk = (P.K + GK - 1) / GK;
-    load(0);
+    load(0, 0);
     for (int kt = 0; kt < nk; ++kt) {
-        const int buf = kt & 1;
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();   // k-step kt is in; every warp is done with the other buffer
+        if (kt + 1 < nk) load((kt + 1) * GK, (kt + 1) & 1);
+        const double* as = As + (kt & 1) * AS_SIZE + (wm + g) * AS_LD + tq;
+        const double* bs = Bs + (kt & 1) * BS_SIZE + tq * BS_LD + wn + g;
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            As[buf][a_k][a_r + 16 * r] = ra[r];
-            Bs[buf][b_k + 4 * r][b_n] = rb[r];
-        }
-        __syncthreads();
-        if (kt + 1 < nk) load((kt + 1) * GK);
+        for (int ks = 0; ks < GK; ks += 4) {
+            double af[4], bf[4];
 #pragma unroll
-        for (int kk = 0; kk < GK; ++kk) {
-            double av[4], bv[4];
+            for (int i = 0; i < 4; ++i) af[i] = as[i * 8 * AS_LD + ks];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) av[i] = As[buf][kk][ty + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) bv[j] = Bs[buf][kk][tx + 16 * j];
+            for (int j = 0; j < 4; ++j) bf[j] = bs[ks * BS_LD + j * 8];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+                for (int j = 0; j < 4; ++j) dmma(acc[i][j], af[i], bf[j]);
         }
     }
+    // accumulator (i, j, h): row wm + 8 i + g, column wn + 8 j + 2 tq + h
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const int row = row0 + ty + 16 * i;
+        const int row = row0 + wm + 8 * i + g;
         if (row >= P.M) continue;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const int col = col0 + tx + 16 * j;
-            if (col >= P.N) continue;
-            double v = acc[i][j];
-            if (P.L) v *= P.L[(size_t)row * P.ldl + col];
-            P.C[(size_t)row * P.ldc + col] = v;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int col = col0 + wn + 8 * j + 2 * tq + h;
+                if (col >= P.N) continue;
+                double v = acc[i][j][h];
+                if (P.L) v *= P.L[(size_t)row * P.ldl + col];
+                P.C[(size_t)row * P.ldc + col] = v;
+            }
         }
     }
 }
@@ -196,14 +232,14 @@ int launch_gemm(lc3d_ctx* c, GemmBatch& b, cudaStream_t s) {
     int tiles = 0;
     for (int q = 0; q < b.count; ++q) {
         GemmProb& p = b.p[q];
-        p.tiles_n = (p.N + GT - 1) / GT;
+        p.tiles_n = (p.N + GTN - 1) / GTN;
         p.tile_start = tiles;
-        tiles += ((p.M + GT - 1) / GT) * p.tiles_n;
+        tiles += ((p.M + GTM - 1) / GTM) * p.tiles_n;
     }
     b.total_tiles = tiles;
     if (tiles == 0) return LC3D_OK;
     ProfScope ps(c, LC3D_STAGE_TRANSFORM, s);
-    dgemm_kernel<<<tiles, 256, 0, s>>>(b);
+    dgemm_kernel<<<tiles, GEMM_THREADS, GEMM_SMEM, s>>>(b);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
@@ -344,6 +380,7 @@ int upload32(float** dst, const std::vector<double>& v) {
 }  // namespace
 
 int fields_init(lc3d_ctx* c) {
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(dgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
     const int N = c->N, M = c->M;
     const long long L = N - 1;
     const double h = c->p.grid_step_size;

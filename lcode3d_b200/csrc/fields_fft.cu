@@ -133,9 +133,29 @@ __device__ __forceinline__ V mul_mi(V a) { return cmk<V>(a.y, -a.x); }
 template <typename V>
 __device__ __forceinline__ V cscale(V a, typename ReOf<V>::type s) { return cmk<V>(a.x * s, a.y * s); }
 
+// Where a pass's twiddles come from. Float64 passes read a per-CTA shared
+// copy: the small-DFT constants dc[0..2] (exp(-2 pi i / 3), exp(-2 pi i / 5),
+// its square), then one segment per pass, seg[k] = exp(-2 pi i k / (R span)),
+// k < span (transforms 0.327 -> 0.319 ms per step at 641^2). Float32 passes
+// read the constant global table through the read-only cache, which measured
+// faster for them (0.234 against 0.238 ms per step).
+template <typename V, bool SHARED> struct Twiddles;
+template <typename V> struct Twiddles<V, true> {
+    const V* dc;
+    const V* seg;
+    __device__ __forceinline__ V c(int i) const { return dc[i]; }
+    __device__ __forceinline__ V w(int k) const { return seg[k]; }
+};
+template <typename V> struct Twiddles<V, false> {
+    const V* tw;   // tw[m] = exp(-2 pi i m / P)
+    int P, tstep;
+    __device__ __forceinline__ V c(int i) const { return __ldg(tw + (i == 0 ? P / 3 : i * (P / 5))); }
+    __device__ __forceinline__ V w(int k) const { return __ldg(tw + k * tstep); }
+};
+
 // Small DFTs in registers, forward sign, R = 2, 3, 4, 5, 8.
-//  3: W = exp(-2 pi i / 3) = (c, -s) from the twiddle table.
-//  5: W = (c1, -s1), W^2 = (c2, -s2) from the twiddle table;
+//  3: W = exp(-2 pi i / 3) = (c, -s) = tw.c(0) (see Twiddles).
+//  5: W = (c1, -s1) = tw.c(1), W^2 = (c2, -s2) = tw.c(2);
 //     X1,4 = v0 + c1 t1 + c2 t2 -+ i (s1 t3 + s2 t4),
 //     X2,3 = v0 + c2 t1 + c1 t2 -+ i (s2 t3 - s1 t4),
 //     t1 = v1 + v4, t2 = v2 + v3, t3 = v1 - v4, t4 = v2 - v3.
@@ -144,8 +164,8 @@ __device__ __forceinline__ V cscale(V a, typename ReOf<V>::type s) { return cmk<
 //     order (X_0 X_2 X_4 X_6 X_1 X_3 X_5 X_7); dft_out<8> maps register ->
 //     frequency. W8 = sqrt(1/2) (1 - i), W8^2 = -i, W8^3 = -sqrt(1/2) (1 + i):
 //     no table loads, two real products each for j = 1, 3.
-template <int R, typename V>
-__device__ __forceinline__ void dft(V (&v)[R], const V* __restrict__ tw, int P) {
+template <int R, typename V, typename TW>
+__device__ __forceinline__ void dft(V (&v)[R], const TW& tw) {
     using T = typename ReOf<V>::type;
     static_assert(R == 2 || R == 3 || R == 4 || R == 5 || R == 8, "radix 2, 3, 4, 5 or 8");
     if constexpr (R == 2) {
@@ -153,7 +173,7 @@ __device__ __forceinline__ void dft(V (&v)[R], const V* __restrict__ tw, int P) 
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
     } else if constexpr (R == 3) {
-        const V w = __ldg(tw + P / 3);
+        const V w = tw.c(0);
         const V t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
         const V a = cadd(v[0], cscale(t1, w.x));
         const V bb = cscale(t2, -w.y);
@@ -169,7 +189,7 @@ __device__ __forceinline__ void dft(V (&v)[R], const V* __restrict__ tw, int P) 
         v[1] = cadd(a1, a3);
         v[3] = csub(a1, a3);
     } else if constexpr (R == 5) {
-        const V w1 = __ldg(tw + P / 5), w2 = __ldg(tw + 2 * (P / 5));
+        const V w1 = tw.c(1), w2 = tw.c(2);
         const T c1 = w1.x, s1 = -w1.y, c2 = w2.x, s2 = -w2.y;
         const V t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
         const V t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
@@ -194,8 +214,8 @@ __device__ __forceinline__ void dft(V (&v)[R], const V* __restrict__ tw, int P) 
         b[1] = cmk<V>(h * (d[1].x + d[1].y), h * (d[1].y - d[1].x));
         b[2] = mul_mi(d[2]);
         b[3] = cmk<V>(h * (d[3].y - d[3].x), -h * (d[3].x + d[3].y));
-        dft<4>(a, tw, P);
-        dft<4>(b, tw, P);
+        dft<4>(a, tw);
+        dft<4>(b, tw);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             v[j] = a[j];
@@ -216,12 +236,11 @@ __device__ __forceinline__ constexpr int dft_out(int r) {
 // position inside the span, and written back in place. After all passes
 // frequency k = m0 + R0 (m1 + R1 (m2 + ...)) sits at sum_s m_s P / (R0..Rs).
 //
-// The twiddles w^m, w = exp(-2 pi i k / Lr), are one table load and a
-// product tree w^m = w^(m/2) w^(m - m/2) (at most three roundings deep for
-// R <= 8), which keeps the R - 1 scattered table loads off the L1 pipe.
-template <int R, typename V>
-__device__ __forceinline__ void dif_butterfly(V* A, int b, int span, float inv_span, int tstep, int P,
-                                              const V* __restrict__ tw) {
+// The twiddles w^m, w = exp(-2 pi i k / Lr), are one table load (tw.w(k))
+// and a product tree w^m = w^(m/2) w^(m - m/2) (at most three roundings deep
+// for R <= 8), which keeps the R - 1 scattered table loads off the L1 pipe.
+template <int R, typename V, typename TW>
+__device__ __forceinline__ void dif_butterfly(V* A, int b, int span, float inv_span, const TW& tw) {
     // g = b / span: (b + 0.5) / span lies at least 0.5 / span from an
     // integer, far more than the float rounding for b, span < 2^16
     const int g = __float2int_rz(((float)b + 0.5f) * inv_span), k = b - g * span;
@@ -230,10 +249,10 @@ __device__ __forceinline__ void dif_butterfly(V* A, int b, int span, float inv_s
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = A[base + r * span];
     V w[R];
-    w[1] = __ldg(tw + k * tstep);
+    w[1] = tw.w(k);
 #pragma unroll
     for (int m = 2; m < R; ++m) w[m] = cmul(w[m / 2], w[m - m / 2]);
-    dft<R>(v, tw, P);
+    dft<R>(v, tw);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int m = dft_out<R>(r);   // frequency in register r
@@ -241,15 +260,25 @@ __device__ __forceinline__ void dif_butterfly(V* A, int b, int span, float inv_s
     }
 }
 
-template <int R, typename V>
-__device__ __forceinline__ void fft_pass(V* A, int span, int P, const V* tw) {
+template <int R, typename V, typename TW>
+__device__ __forceinline__ void fft_pass(V* A, int span, int P, const TW& tw) {
     const int nb = P / R;
     const float inv_span = 1.0f / (float)span;
-    const int tstep = P / (span * R);   // twiddle stride of this pass
     for (int t = threadIdx.x; t < FFT_PER_CTA * nb; t += FFT_THREADS) {
         const int q = FFT_PER_CTA == 2 && t >= nb, j = t - q * nb;
-        dif_butterfly<R>(A + q * (P + FFT_PAD), j, span, inv_span, tstep, P, tw);
+        dif_butterfly<R>(A + q * (P + FFT_PAD), j, span, inv_span, tw);
     }
+}
+
+// Entries of the CTA's shared twiddle table (float64 passes): the three
+// small-DFT constants, then one segment per pass of span entries.
+__host__ __device__ constexpr int fft_twiddle_entries(int P, const int* rad, int nrad) {
+    int n = 3, span = P;
+    for (int p = 0; p < nrad; ++p) {
+        span /= rad[p];
+        n += span;
+    }
+    return n;
 }
 
 template <int BYTES>
@@ -303,12 +332,29 @@ constexpr int fft_min_blocks() { return sizeof(T) == 8 ? LC3D_FFT_MIN_BLOCKS : L
 template <typename T, typename Tin, typename Tout>
 __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_kernel(const __grid_constant__ FftBatch b) {
     using V = typename CxOf<T>::type;
-    extern __shared__ __align__(16) unsigned char fft_smem[];   // FFT q at q (P + FFT_PAD); then the staging rows
+    // FFT q at q (P + FFT_PAD); the twiddle table; the staging rows
+    extern __shared__ __align__(16) unsigned char fft_smem[];
     const int P = b.P, L = P / 2, PS = P + FFT_PAD;
     V* A = reinterpret_cast<V*>(fft_smem);
-    Tin* stg = reinterpret_cast<Tin*>(A + FFT_PER_CTA * PS);   // [ROWS_PER_CTA][N]
+    constexpr bool SHARED_TW = sizeof(T) == 8;
+    V* tws = A + FFT_PER_CTA * PS;
+    Tin* stg = reinterpret_cast<Tin*>(tws + (SHARED_TW ? fft_twiddle_entries(P, b.rad, b.nrad) : 0));   // [ROWS_PER_CTA][N]
     const V* tw = reinterpret_cast<const V*>(sizeof(T) == 8 ? static_cast<const void*>(b.tw)
                                                             : static_cast<const void*>(b.tw32));
+    if (SHARED_TW) {   // the twiddles of every pass, from the constant table (written at set-up,
+                       // so read before the dependency wait); first used after the next barrier
+        if (threadIdx.x < 3) {
+            const int m = threadIdx.x == 0 ? (P % 3 ? 0 : P / 3) : (P % 5 ? 0 : threadIdx.x * (P / 5));
+            tws[threadIdx.x] = __ldg(tw + m);
+        }
+        int off = 3, span = P;
+        for (int p = 0; p < b.nrad; ++p) {
+            span /= b.rad[p];
+            const int tstep = P / (span * b.rad[p]);
+            for (int k = threadIdx.x; k < span; k += FFT_THREADS) tws[off + k] = __ldg(tw + k * tstep);
+            off += span;
+        }
+    }
 #if LC3D_FFT_CLOCKS
     long long clk[FFT_NCLK] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long clk_last = clock64();
@@ -352,18 +398,29 @@ __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_ker
     FFT_CLK(1);
     if (g + (int)gridDim.x < b.ngroups) stage_group(b, g + gridDim.x, stg);
     int span = P;
+    const V* seg = tws + 3;
     for (int p = 0; p < b.nrad; ++p) {
         const int R = b.rad[p];
         span /= R;
+        Twiddles<V, SHARED_TW> tp;
+        if constexpr (SHARED_TW) {
+            tp.dc = tws;
+            tp.seg = seg;
+        } else {
+            tp.tw = tw;
+            tp.P = P;
+            tp.tstep = P / (span * R);
+        }
         switch (R) {
 #if LC3D_FFT_MAX_RADIX >= 8
-            case 8: fft_pass<8>(A, span, P, tw); break;
+            case 8: fft_pass<8>(A, span, P, tp); break;
 #endif
-            case 4: fft_pass<4>(A, span, P, tw); break;
-            case 2: fft_pass<2>(A, span, P, tw); break;
-            case 3: fft_pass<3>(A, span, P, tw); break;
-            default: fft_pass<5>(A, span, P, tw); break;
+            case 4: fft_pass<4>(A, span, P, tp); break;
+            case 2: fft_pass<2>(A, span, P, tp); break;
+            case 3: fft_pass<3>(A, span, P, tp); break;
+            default: fft_pass<5>(A, span, P, tp); break;
         }
+        seg += span;
         __syncthreads();
         FFT_CLK(2 + p);
     }
@@ -474,12 +531,15 @@ int fft_plan(int P, int* rad) {
 int fft_cta_rows() { return ROWS_PER_CTA; }
 
 // Dynamic shared memory of fft_rows_kernel, the layout the kernel uses: the
-// FFT buffers at a pitch of P + FFT_PAD complex words, then the staging rows
-// (ROWS_PER_CTA x N input elements).
+// FFT buffers at a pitch of P + FFT_PAD complex words, the twiddle table
+// (float64 passes), then the staging rows (ROWS_PER_CTA x N input elements).
 size_t fft_cta_smem_bytes(int P, int N, int types) {
     const size_t cx = types == FFT_F64 ? sizeof(double2) : sizeof(float2);
     const size_t in = (types == FFT_F64 || types == FFT_F64_F32) ? sizeof(double) : sizeof(float);
-    return (size_t)FFT_PER_CTA * (P + FFT_PAD) * cx + (size_t)ROWS_PER_CTA * N * in;
+    int rad[MAX_RADICES];
+    const int nrad = fft_plan(P, rad);
+    return ((size_t)FFT_PER_CTA * (P + FFT_PAD) + (types == FFT_F64 ? fft_twiddle_entries(P, rad, nrad) : 0)) * cx +
+           (size_t)ROWS_PER_CTA * N * in;
 }
 
 // Layout of the twiddle buffer (in doubles): P double2 twiddles, the two

@@ -34,10 +34,11 @@ void lc3d_set_last_cuda_error(cudaError_t e, const char* what, const char* file,
 // with programmatic stream serialization: the launch of a kernel is
 // processed while its predecessor in the stream is still running, and its
 // CTAs start as soon as the predecessor has exited. Every such kernel calls
-// pdl_wait() before its first global-memory access, read or write: the wait
-// returns once the preceding grid has completed and its writes are visible,
-// so stream order holds for all data, and transitively, since every kernel
-// in the chain waits. No kernel triggers its successor early
+// pdl_wait() before its first global-memory access, read or write (reads
+// of tables written once at set-up, which no kernel of the chain writes,
+// may come before it): the wait returns once the preceding grid has
+// completed and its writes are visible, so stream order holds for all data,
+// and transitively, since every kernel in the chain waits. No kernel triggers its successor early
 // (griddepcontrol.launch_dependents): resident, waiting successor CTAs
 // measured slower. pdl_wait() is a no-op for a kernel launched without the
 // attribute. Step loops launched from the host gain 4-7 % from this; CUDA
