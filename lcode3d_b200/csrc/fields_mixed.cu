@@ -17,13 +17,17 @@
 // truncation after S slices, ~2^-7S of the row maxima; the epilogue adds the
 // level sums in float64 and applies 2^(e_a + e_b).
 //
-// GEMM kernel: one 128 x 128 output tile per CTA, K in blocks of 32 (64-byte
-// rows, 64-byte swizzle), all 2S operand slices of a K block per pipeline
-// stage. Warp 0 issues TMA loads, warp 1 owns the TMEM allocation and
-// issues tcgen05.mma (128 x 128 x 16, bf16 -> f32) from one thread, warps
-// 2-5 read the four accumulators with tcgen05.ld and write float64. Every
-// mbarrier wait is bounded: on time-out the kernel raises an error flag and
-// exits its loops, and TMEM is always freed.
+// GEMM kernel: persistent, one CTA per SM looping over 128 x 64 output
+// tiles; K in blocks of 32 (64-byte rows, 64-byte swizzle), all 2S operand
+// slices of a K block per pipeline stage, the stages running on from one
+// tile to the next. Warp 0 issues TMA loads, warp 1 owns the TMEM
+// allocation and issues tcgen05.mma (128 x 64 x 16, bf16 -> f32) from one
+// thread, warps 2-5 read the four accumulators with tcgen05.ld and write
+// float64. TMEM holds two sets of the four accumulators (2 x 4 x 64
+// columns): the MMAs of a tile run into one set while the epilogue drains
+// the other's previous tile. Every mbarrier wait is bounded: on time-out the
+// kernel raises an error flag and every role leaves its loop, and TMEM is
+// always freed.
 //
 // Stages of one solve (rows x cols field, L = axis-0 and R = axis-1
 // transform; S2 and C are symmetric or appear as C^T^T = C, so the two
@@ -47,6 +51,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -56,8 +61,10 @@
 
 namespace {
 
-constexpr int TM = 128, TN = 128;                              // output tile
-constexpr int TILE_BYTES = TM * 64;                              // 8 KiB: 128 rows of 64 bytes (A and B alike)
+constexpr int TM = 128, TN = 64;                               // output tile
+constexpr int TILE_A_BYTES = TM * 64;                            // 8 KiB: 128 rows of 64 bytes
+constexpr int TILE_B_BYTES = TN * 64;                            // 4 KiB
+constexpr int BOX_ROWS = 64;                                     // TMA box height (an A tile is two boxes)
 constexpr int KIND_BF16 = 0, KIND_TF32 = 1;
 
 // Elements of one 64-byte operand row: 32 bf16 or 16 tf32 (float32).
@@ -65,7 +72,9 @@ __host__ __device__ constexpr int k_block(int kind) { return kind == KIND_TF32 ?
 constexpr int MAX_SLICES = 6;
 constexpr int GEMM_THREADS = 192;
 constexpr int NACC = 4;                                          // f32 accumulators, one per digit level
-constexpr int TMEM_COLS = NACC * TN;                             // 512: all of TMEM
+constexpr int ACC_COLS = NACC * TN;                              // 256: one set of accumulators
+constexpr int TMEM_COLS = 2 * ACC_COLS;                          // 512: two sets, all of TMEM
+constexpr int EPI_BYTES = 4 * 32 * 33 * (int)sizeof(double);     // epilogue transposes, one per warp
 constexpr int ROWS_PAD_ALIGN = 128;
 
 struct OzProb {
@@ -83,7 +92,7 @@ struct OzProb {
 
 struct OzBatch {
     OzProb p[6];
-    int count, S, stages, kind;
+    int count, S, stages, kind, total_tiles;
     unsigned* err;
     long long wait_limit;          // bound of every pipeline wait (SM clock cycles)
     int skip_loads;                // timeout test only: the producer issues no loads
@@ -112,29 +121,37 @@ __device__ __forceinline__ double pow2(int e) {
 // ---------------------------------------------------------------------------
 // The GEMM kernel
 // ---------------------------------------------------------------------------
+// Tile t of the batch: its problem and output corner.
+__device__ __forceinline__ const OzProb& oz_tile(const OzBatch& b, int t, int& m0, int& n0) {
+    int pi = 0;
+#pragma unroll 1
+    for (int q = 1; q < b.count; ++q)
+        if (t >= b.p[q].tile_start) pi = q;
+    const OzProb& P = b.p[pi];
+    const int u = t - P.tile_start;
+    m0 = (u / P.tiles_n) * TM;
+    n0 = (u % P.tiles_n) * TN;
+    return P;
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_constant__ OzBatch b) {
     constexpr int KB = k_block(KIND);   // K elements per 64-byte row
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int S = b.S, NS = b.stages;
-    uint8_t* sA = smem;
-    uint8_t* sB = smem + (size_t)NS * S * TILE_BYTES;
-    uint64_t* full = reinterpret_cast<uint64_t*>(sB + (size_t)NS * S * TILE_BYTES);
+    const int STAGE_BYTES = S * (TILE_A_BYTES + TILE_B_BYTES);   // S A tiles, then S B tiles
+    uint8_t* sPipe = smem;
+    double* sEpi = reinterpret_cast<double*>(smem + (size_t)NS * STAGE_BYTES);
+    uint64_t* full = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(sEpi) + EPI_BYTES);
     uint64_t* empty = full + NS;
-    uint64_t* done = empty + NS;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
-    __shared__ int s_fail;
+    uint64_t* tfull = empty + NS;   // [2]: accumulator set complete
+    uint64_t* tempty = tfull + 2;   // [2]: accumulator set drained by the epilogue
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+    __shared__ volatile int s_fail;
 
-    int pi = 0;
-#pragma unroll 1
-    for (int q = 1; q < b.count; ++q)
-        if ((int)blockIdx.x >= b.p[q].tile_start) pi = q;
-    const OzProb& P = b.p[pi];
-    const int t = (int)blockIdx.x - P.tile_start;
-    const int m0 = (t / P.tiles_n) * TM, n0 = (t % P.tiles_n) * TN;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nkb = (P.K + KB - 1) / KB;
+    const int total = b.total_tiles;
 
     if (threadIdx.x == 0) {
         s_fail = 0;
@@ -142,7 +159,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
             mbar_init(&full[i], 1);
             mbar_init(&empty[i], 1);
         }
-        mbar_init(done, 1);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&tfull[i], 1);
+            mbar_init(&tempty[i], 4);   // one arrival per epilogue warp
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -159,97 +179,125 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
         if (lane == 0 && !b.skip_loads) {   // ---- TMA producer ----
             // (skip_loads: nothing is loaded, so no copy is in flight when
             // the MMA issuer's wait for the first stage runs out)
-            for (int kb = 0; kb < nkb; ++kb) {
-                const int st = kb % NS, round = kb / NS;
-                if (round > 0 && !mbar_wait(&empty[st], (round - 1) & 1, b.wait_limit)) {
-                    s_fail = 1;
-                    break;
-                }
-                mbar_expect_tx(&full[st], 2u * S * TILE_BYTES);
-                for (int s = 0; s < S; ++s) {
-                    tma_load_2d(sA + ((size_t)st * S + s) * TILE_BYTES, &P.ta, &full[st], kb * KB,
-                                s * P.a_rows_pad + m0);
-                    tma_load_2d(sB + ((size_t)st * S + s) * TILE_BYTES, &P.tb, &full[st], kb * KB,
-                                s * P.b_rows_pad + n0);
+            int it = 0;   // K blocks issued so far, over all of this CTA's tiles
+            for (int t = blockIdx.x; t < total && !s_fail; t += gridDim.x) {
+                int m0, n0;
+                const OzProb& P = oz_tile(b, t, m0, n0);
+                const int nkb = (P.K + KB - 1) / KB;
+                for (int kb = 0; kb < nkb; ++kb, ++it) {
+                    const int st = it % NS;
+                    if (it >= NS && !mbar_wait(&empty[st], ((it / NS) - 1) & 1, b.wait_limit)) {
+                        s_fail = 1;
+                        break;
+                    }
+                    mbar_expect_tx(&full[st], (uint32_t)STAGE_BYTES);
+                    uint8_t* base = sPipe + (size_t)st * STAGE_BYTES;
+                    for (int s = 0; s < S; ++s) {
+                        uint8_t* a = base + (size_t)s * TILE_A_BYTES;
+                        tma_load_2d(a, &P.ta, &full[st], kb * KB, s * P.a_rows_pad + m0);
+                        tma_load_2d(a + BOX_ROWS * 64, &P.ta, &full[st], kb * KB, s * P.a_rows_pad + m0 + BOX_ROWS);
+                        tma_load_2d(base + (size_t)S * TILE_A_BYTES + (size_t)s * TILE_B_BYTES, &P.tb, &full[st],
+                                    kb * KB, s * P.b_rows_pad + n0);
+                    }
                 }
             }
         }
     } else if (warp == 1) {
         if (lane == 0) {   // ---- MMA issuer ----
             // products of digit level s + u go to accumulator min(s + u, 3)
-            bool ok = true;
-            for (int kb = 0; kb < nkb && ok; ++kb) {
-                const int st = kb % NS, round = kb / NS;
-                if (!mbar_wait(&full[st], round & 1, b.wait_limit)) {
-                    ok = false;
+            int it = 0, j = 0;
+            for (int t = blockIdx.x; t < total && !s_fail; t += gridDim.x, ++j) {
+                const int buf = j & 1;
+                if (j >= 2 && !mbar_wait(&tempty[buf], ((j >> 1) - 1) & 1, b.wait_limit)) {
                     s_fail = 1;
                     break;
                 }
                 fence_after();
-                const uint32_t a_base = smem_u32(sA + (size_t)st * S * TILE_BYTES);
-                const uint32_t b_base = smem_u32(sB + (size_t)st * S * TILE_BYTES);
-                unsigned fresh = (kb == 0) ? 0xfu : 0u;   // accumulators not yet written
-                for (int s = 0; s < S; ++s)
-                    for (int u = 0; s + u < S; ++u) {
-                        const int lvl = min(s + u, NACC - 1);
-                        const uint32_t acc = tmem + lvl * TN;
-#pragma unroll
-                        for (int kk = 0; kk < 2; ++kk) {   // two MMAs per 64-byte row: K = 16 bf16 or 8 tf32
-                            const uint64_t ad = umma_desc_sw64(a_base + s * TILE_BYTES + kk * 32);
-                            const uint64_t bd = umma_desc_sw64(b_base + u * TILE_BYTES + kk * 32);
-                            if constexpr (KIND == KIND_TF32)
-                                umma_tf32(acc, ad, bd, IDESC_TF32, ((fresh >> lvl) & 1u) ? 0u : 1u);
-                            else
-                                umma_bf16(acc, ad, bd, IDESC, ((fresh >> lvl) & 1u) ? 0u : 1u);
-                            fresh &= ~(1u << lvl);
-                        }
+                int m0, n0;
+                const OzProb& P = oz_tile(b, t, m0, n0);
+                const int nkb = (P.K + KB - 1) / KB;
+                const uint32_t accs = tmem + (uint32_t)(buf * ACC_COLS);
+                bool ok = true;
+                for (int kb = 0; kb < nkb; ++kb, ++it) {
+                    const int st = it % NS;
+                    if (!mbar_wait(&full[st], (it / NS) & 1, b.wait_limit)) {
+                        ok = false;
+                        break;
                     }
-                umma_commit(&empty[st]);   // frees the stage once these MMAs have read it
+                    fence_after();
+                    const uint32_t a_base = smem_u32(sPipe + (size_t)st * STAGE_BYTES);
+                    const uint32_t b_base = a_base + (uint32_t)(S * TILE_A_BYTES);
+                    unsigned fresh = (kb == 0) ? 0xfu : 0u;   // accumulators not yet written for this tile
+                    for (int s = 0; s < S; ++s)
+                        for (int u = 0; s + u < S; ++u) {
+                            const int lvl = min(s + u, NACC - 1);
+                            const uint32_t acc = accs + lvl * TN;
+#pragma unroll
+                            for (int kk = 0; kk < 2; ++kk) {   // two MMAs per 64-byte row: K = 16 bf16 or 8 tf32
+                                const uint64_t ad = umma_desc_sw64(a_base + s * TILE_A_BYTES + kk * 32);
+                                const uint64_t bd = umma_desc_sw64(b_base + u * TILE_B_BYTES + kk * 32);
+                                if constexpr (KIND == KIND_TF32)
+                                    umma_tf32(acc, ad, bd, IDESC_TF32, ((fresh >> lvl) & 1u) ? 0u : 1u);
+                                else
+                                    umma_bf16(acc, ad, bd, IDESC, ((fresh >> lvl) & 1u) ? 0u : 1u);
+                                fresh &= ~(1u << lvl);
+                            }
+                        }
+                    umma_commit(&empty[st]);   // frees the stage once these MMAs have read it
+                }
+                if (!ok) {
+                    s_fail = 1;
+                    break;
+                }
+                umma_commit(&tfull[buf]);      // this tile's accumulators complete
             }
-            umma_commit(done);             // accumulators complete
         }
     } else {   // ---- epilogue: warps 2..5 cover TMEM lanes 32 (warp % 4) .. +31 ----
         const int quarter = warp & 3;
         const int row = quarter * 32 + lane;
-        const int m = m0 + row;
-        const bool ok = mbar_wait(done, 0, b.wait_limit);
-        if (!ok) s_fail = 1;
-        fence_after();
-        if (ok) {
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        double* stg = sEpi + (warp - 2) * 32 * 33;
+        const int nacc = min(S, NACC);
+        int j = 0;
+        for (int t = blockIdx.x; t < total && !s_fail; t += gridDim.x, ++j) {
+            const int buf = j & 1;
+            if (!mbar_wait(&tfull[buf], (j >> 1) & 1, b.wait_limit)) {
+                s_fail = 1;
+                break;
+            }
+            fence_after();
+            int m0, n0;
+            const OzProb& P = oz_tile(b, t, m0, n0);
+            const int m = m0 + row;
             const double sa = (m < P.M) ? pow2(P.ea[m]) : 0.0;
-            const int nacc = min(S, NACC);
-            const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
             for (int c0 = 0; c0 < TN; c0 += 32) {
                 double v[32];
 #pragma unroll
-                for (int j = 0; j < 32; ++j) v[j] = 0.0;
+                for (int jj = 0; jj < 32; ++jj) v[jj] = 0.0;
                 for (int d = 0; d < nacc; ++d) {   // exact f32 level sums, added in float64
                     uint32_t r[32];
-                    tmem_ld32(tmem + lane_base + d * TN + c0, r);
+                    tmem_ld32(tmem + lane_base + (uint32_t)(buf * ACC_COLS + d * TN + c0), r);
                     tmem_wait_ld();
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) v[j] += (double)__uint_as_float(r[j]);
+                    for (int jj = 0; jj < 32; ++jj) v[jj] += (double)__uint_as_float(r[jj]);
                 }
                 if (P.transposed) {
                     // out[n][m]: the lanes hold consecutive m, stores coalesce
                     if (m < P.M) {
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const int n = n0 + c0 + j;
+                        for (int jj = 0; jj < 32; ++jj) {
+                            const int n = n0 + c0 + jj;
                             if (n >= P.N) continue;
-                            double x = v[j] * (sa * pow2(__ldg(P.eb + n)));
+                            double x = v[jj] * (sa * pow2(__ldg(P.eb + n)));
                             if (P.lam) x *= P.lam[(size_t)m * P.ldl + n];
                             P.out[(size_t)n * P.ldo + m] = x;
                         }
                     }
                 } else {
                     // out[m][n]: transpose the warp's 32 x 32 block through
-                    // shared memory (the pipeline buffers are free once the
-                    // accumulators are complete) so the lanes write
-                    // consecutive n
-                    double* stg = reinterpret_cast<double*>(smem) + (warp - 2) * 32 * 33;
+                    // shared memory so the lanes write consecutive n
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = v[j];
+                    for (int jj = 0; jj < 32; ++jj) stg[lane * 33 + jj] = v[jj];
                     __syncwarp();
                     const int n = n0 + c0 + lane;
                     const double sb = (n < P.N) ? pow2(__ldg(P.eb + n)) : 0.0;
@@ -263,6 +311,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
                     __syncwarp();
                 }
             }
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[buf]);   // this set may take the tile after next
         }
     }
     fence_before();
@@ -343,7 +394,8 @@ __global__ void __launch_bounds__(256) slice_rows_kernel(const __grid_constant__
 namespace {
 
 struct MixedState {
-    int S, stages, kind;
+    int S, stages, kind, sms;
+    size_t smem_max;               // dynamic shared memory the GEMM kernels may use
     int rows_pad, k_pad;           // common padded shape of every operand buffer
     void* fixed[2];                // sliced S2 (M x M) and C (N x N): bf16 or float32 (tf32)
     int* efixed[2];
@@ -359,7 +411,7 @@ int make_map(CUtensorMap* m, void* base, int S, int rows_pad, int k_pad, int kin
     const int esize = kind == KIND_TF32 ? 4 : 2;
     cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)S * rows_pad};
     cuuint64_t strides[1] = {(cuuint64_t)k_pad * esize};
-    cuuint32_t box[2] = {(cuuint32_t)k_block(kind), TM};   // 64-byte rows
+    cuuint32_t box[2] = {(cuuint32_t)k_block(kind), BOX_ROWS};   // 64-byte rows
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(m, kind == KIND_TF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
                      base, dims, strides, box, estr,
@@ -424,7 +476,19 @@ int mixed_init(lc3d_ctx* c, int slices, int tf32) {
     const int esize = tf32 ? 4 : 2;
     ms->rows_pad = (N + ROWS_PAD_ALIGN - 1) / ROWS_PAD_ALIGN * ROWS_PAD_ALIGN;
     ms->k_pad = (N + 7) / 8 * 8;
-    ms->stages = 200 * 1024 / (2 * slices * TILE_BYTES);
+    {
+        // the opt-in limit of a block less the kernels' static shared memory
+        int dev = 0, optin = 0;
+        LC3D_CUDA_TRY(cudaGetDevice(&dev));
+        LC3D_CUDA_TRY(cudaDeviceGetAttribute(&ms->sms, cudaDevAttrMultiProcessorCount, dev));
+        LC3D_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        cudaFuncAttributes fa16{}, fa32{};
+        LC3D_CUDA_TRY(cudaFuncGetAttributes(&fa16, oz_gemm_kernel<KIND_BF16>));
+        LC3D_CUDA_TRY(cudaFuncGetAttributes(&fa32, oz_gemm_kernel<KIND_TF32>));
+        ms->smem_max = (size_t)optin - std::max(fa16.sharedSizeBytes, fa32.sharedSizeBytes);
+    }
+    // pipeline stages in what the epilogue buffers, barriers and alignment leave
+    ms->stages = (int)((ms->smem_max - EPI_BYTES - 1024 - 256) / ((size_t)slices * (TILE_A_BYTES + TILE_B_BYTES)));
     if (ms->stages > 4) ms->stages = 4;
     if (ms->stages < 2) return LC3D_ERR_PARAM;
     // fixed transform matrices, sliced on the host
@@ -467,13 +531,12 @@ int mixed_init(lc3d_ctx* c, int slices, int tf32) {
         LC3D_CUDA_TRY(cudaMemset(ms->edata[f], 0, ms->rows_pad * sizeof(int)));
         LC3D_TRY(make_map(&ms->map_data[f], ms->data[f], slices, ms->rows_pad, ms->k_pad, ms->kind));
     }
-    // per-kernel limit: the largest pipeline any slice count uses (stages x
-    // 2S tiles <= 200 KiB) plus alignment slack and barriers, so contexts
-    // with different slice counts can coexist
+    // per-kernel limit: the opt-in maximum, which every slice count's
+    // pipeline fits, so contexts with different slice counts can coexist
     LC3D_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<KIND_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       200 * 1024 + 1024 + 256));
+                                       (int)ms->smem_max));
     LC3D_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<KIND_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       200 * 1024 + 1024 + 256));
+                                       (int)ms->smem_max));
     return LC3D_OK;
 }
 
@@ -561,12 +624,16 @@ int mixed_stage(lc3d_ctx* c, const MixedStageDesc* d, int count, cudaStream_t s)
         p.tile_start = tiles;
         tiles += ((p.M + TM - 1) / TM) * p.tiles_n;
     }
-    const size_t smem = (size_t)ms->stages * 2 * ms->S * TILE_BYTES + 1024 + 256;
+    b.total_tiles = tiles;
+    if (!tiles) return LC3D_OK;
+    const size_t smem =
+        (size_t)ms->stages * ms->S * (TILE_A_BYTES + TILE_B_BYTES) + EPI_BYTES + 1024 + 256;
+    const int grid = std::min(tiles, std::max(ms->sms, 1));   // persistent: one CTA per SM
     ProfScope ps(c, LC3D_STAGE_TRANSFORM, s);
     if (ms->kind == KIND_TF32)
-        oz_gemm_kernel<KIND_TF32><<<tiles, GEMM_THREADS, smem, s>>>(b);
+        oz_gemm_kernel<KIND_TF32><<<grid, GEMM_THREADS, smem, s>>>(b);
     else
-        oz_gemm_kernel<KIND_BF16><<<tiles, GEMM_THREADS, smem, s>>>(b);
+        oz_gemm_kernel<KIND_BF16><<<grid, GEMM_THREADS, smem, s>>>(b);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
