@@ -426,10 +426,11 @@ int fields_init(lc3d_ctx* c) {
         LC3D_TRY(upload32(&c->lam32_neu, ln));
     }
     const size_t plane = (size_t)N * N * sizeof(double);
+    const size_t tplane = (size_t)N * fft_pitch(N) * sizeof(double);   // the transform intermediates
     for (int f = 0; f < 6; ++f) {
         LC3D_CUDA_TRY(cudaMalloc(&c->rhs[f], plane));
-        LC3D_CUDA_TRY(cudaMalloc(&c->t1[f], plane));
-        LC3D_CUDA_TRY(cudaMalloc(&c->t2[f], plane));
+        LC3D_CUDA_TRY(cudaMalloc(&c->t1[f], tplane));
+        LC3D_CUDA_TRY(cudaMalloc(&c->t2[f], tplane));
         LC3D_CUDA_TRY(cudaMalloc(&c->raw[f], plane));
         LC3D_CUDA_TRY(cudaMemset(c->rhs[f], 0, plane));
         LC3D_CUDA_TRY(cudaMemset(c->raw[f], 0, plane));
@@ -593,8 +594,11 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
                 const FieldGeom g = geom(c, f);
                 FftRowsDesc& e = d[cnt++];
                 memset(&e, 0, sizeof(e));
-                e.ld_in = N;
-                e.ld_out = N;
+                // the intermediates t1 / t2 at a row pitch of whole 32-byte
+                // sectors, so a CTA's transposed stores fill whole sectors
+                const int Np = fft_pitch(N, f32);
+                e.ld_in = stage == 0 ? N : Np;
+                e.ld_out = stage == 3 ? N : Np;
                 switch (stage) {
                     case 0: e.in = c->rhs[f] + g.off; e.rows = g.rows; e.type = g.type1; e.out = c->t1[f]; break;
                     case 1: e.in = c->t1[f]; e.rows = g.cols; e.type = g.type0; e.out = c->t2[f];
