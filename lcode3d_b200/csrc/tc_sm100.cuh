@@ -49,7 +49,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
     }
 }
 
-// 2-D tiled TMA load into this CTA's shared memory (no multicast). The
+// 2-D tiled TMA load into this CTA's own shared memory (one destination). The
 // innermost coordinate x times the element size must be a multiple of 16
 // bytes; other coordinates may be negative or past the end (zero fill).
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
