@@ -314,7 +314,22 @@ class _StatePool:
 
     @staticmethod
     def _counts(e):
-        return [sys.getrefcount(e[0])] + [sys.getrefcount(t) for t in e[1]] + [_use_count(e[5])]
+        arr = e[1]
+        return [sys.getrefcount(e[0])] + [sys.getrefcount(arr[k]) for k in range(len(arr))] + [_use_count(e[5])]
+
+    @staticmethod
+    def _free(e):
+        """The counts of entry e are back at their baseline e[3], taken the
+        same way as _counts but compared one by one, the object's own count
+        first (an entry in use usually fails there)."""
+        base = e[3]
+        if sys.getrefcount(e[0]) != base[0]:
+            return False
+        arr = e[1]
+        for k in range(len(arr)):
+            if sys.getrefcount(arr[k]) != base[1 + k]:
+                return False
+        return _use_count(e[5]) == base[-1]
 
     def ptrs_of(self, state):
         """The StatePtrs of `state` if it is one of the pool's states with
@@ -329,7 +344,7 @@ class _StatePool:
 
     def take(self, shape_p, g, dev):
         for e in self.entries:
-            if e[4] == (shape_p, g, dev) and self._counts(e) == e[3]:
+            if e[4] == (shape_p, g, dev) and self._free(e):
                 return e
         arrays = tuple(_new_state_arrays(shape_p, g, dev))
         obj = GPUArrays.__new__(GPUArrays)
