@@ -66,6 +66,9 @@ constexpr int TILE_A_BYTES = TM * 64;                            // 8 KiB: 128 r
 constexpr int TILE_B_BYTES = TN * 64;                            // 4 KiB
 constexpr int BOX_ROWS = 64;                                     // TMA box height (an A tile is two boxes)
 constexpr int KIND_BF16 = 0, KIND_TF32 = 1;
+#ifndef LC3D_OZ_MAX_STAGES
+#define LC3D_OZ_MAX_STAGES 4                                     // pipeline stages at most
+#endif
 
 // Elements of one 64-byte operand row: 32 bf16 or 16 tf32 (float32).
 __host__ __device__ constexpr int k_block(int kind) { return kind == KIND_TF32 ? 16 : 32; }
@@ -134,12 +137,15 @@ __device__ __forceinline__ const OzProb& oz_tile(const OzBatch& b, int t, int& m
     return P;
 }
 
-template <int KIND>
+// S (slices per operand) is a template parameter, so that the MMA issuer's
+// product loop unrolls into straight-line issues with every descriptor
+// offset, accumulator and accumulate flag known at compile time.
+template <int KIND, int S>
 __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_constant__ OzBatch b) {
     constexpr int KB = k_block(KIND);   // K elements per 64-byte row
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const int S = b.S, NS = b.stages;
+    const int NS = b.stages;
     const int STAGE_BYTES = S * (TILE_A_BYTES + TILE_B_BYTES);   // S A tiles, then S B tiles
     uint8_t* sPipe = smem;
     double* sEpi = reinterpret_cast<double*>(smem + (size_t)NS * STAGE_BYTES);
@@ -192,6 +198,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
                     }
                     mbar_expect_tx(&full[st], (uint32_t)STAGE_BYTES);
                     uint8_t* base = sPipe + (size_t)st * STAGE_BYTES;
+#pragma unroll
                     for (int s = 0; s < S; ++s) {
                         uint8_t* a = base + (size_t)s * TILE_A_BYTES;
                         tma_load_2d(a, &P.ta, &full[st], kb * KB, s * P.a_rows_pad + m0);
@@ -226,23 +233,34 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
                     }
                     fence_after();
                     const uint32_t a_base = smem_u32(sPipe + (size_t)st * STAGE_BYTES);
-                    const uint32_t b_base = a_base + (uint32_t)(S * TILE_A_BYTES);
-                    unsigned fresh = (kb == 0) ? 0xfu : 0u;   // accumulators not yet written for this tile
-                    for (int s = 0; s < S; ++s)
+                    // descriptors of the stage's first A and B tiles; the
+                    // start-address field counts 16-byte units and stays
+                    // below 2^14 (shared memory < 256 KiB), so the offsets of
+                    // the other tiles and of the second K half add to it
+                    // without a carry into the other fields
+                    const uint64_t da = umma_desc_sw64(a_base);
+                    const uint64_t db = umma_desc_sw64(a_base + (uint32_t)(S * TILE_A_BYTES));
+                    const uint32_t later = kb > 0 ? 1u : 0u;   // accumulators already written for this tile
+#pragma unroll
+                    for (int s = 0; s < S; ++s) {
+                        const uint64_t das = da + (uint64_t)((s * TILE_A_BYTES) >> 4);
+#pragma unroll
                         for (int u = 0; s + u < S; ++u) {
                             const int lvl = min(s + u, NACC - 1);
                             const uint32_t acc = accs + lvl * TN;
-#pragma unroll
-                            for (int kk = 0; kk < 2; ++kk) {   // two MMAs per 64-byte row: K = 16 bf16 or 8 tf32
-                                const uint64_t ad = umma_desc_sw64(a_base + s * TILE_A_BYTES + kk * 32);
-                                const uint64_t bd = umma_desc_sw64(b_base + u * TILE_B_BYTES + kk * 32);
-                                if constexpr (KIND == KIND_TF32)
-                                    umma_tf32(acc, ad, bd, IDESC_TF32, ((fresh >> lvl) & 1u) ? 0u : 1u);
-                                else
-                                    umma_bf16(acc, ad, bd, IDESC, ((fresh >> lvl) & 1u) ? 0u : 1u);
-                                fresh &= ~(1u << lvl);
+                            const uint64_t dbu = db + (uint64_t)((u * TILE_B_BYTES) >> 4);
+                            // the first product of each level in this order is (0, level)
+                            const uint32_t first = (s > 0 || u >= NACC) ? 1u : later;
+                            // two MMAs per 64-byte row (K = 16 bf16 or 8 tf32), the second 32 bytes on
+                            if constexpr (KIND == KIND_TF32) {
+                                umma_tf32(acc, das, dbu, IDESC_TF32, first);
+                                umma_tf32(acc, das + 2, dbu + 2, IDESC_TF32, 1u);
+                            } else {
+                                umma_bf16(acc, das, dbu, IDESC, first);
+                                umma_bf16(acc, das + 2, dbu + 2, IDESC, 1u);
                             }
                         }
+                    }
                     umma_commit(&empty[st]);   // frees the stage once these MMAs have read it
                 }
                 if (!ok) {
@@ -393,6 +411,21 @@ __global__ void __launch_bounds__(256) slice_rows_kernel(const __grid_constant__
 
 namespace {
 
+// The kernel instantiation of a kind and slice count (1 .. MAX_SLICES).
+using OzKernel = void (*)(OzBatch);
+template <int KIND>
+OzKernel oz_kernel_of(int S) {
+    switch (S) {
+        case 1: return oz_gemm_kernel<KIND, 1>;
+        case 2: return oz_gemm_kernel<KIND, 2>;
+        case 3: return oz_gemm_kernel<KIND, 3>;
+        case 4: return oz_gemm_kernel<KIND, 4>;
+        case 5: return oz_gemm_kernel<KIND, 5>;
+        default: return oz_gemm_kernel<KIND, 6>;
+    }
+}
+OzKernel oz_kernel(int kind, int S) { return kind == KIND_TF32 ? oz_kernel_of<KIND_TF32>(S) : oz_kernel_of<KIND_BF16>(S); }
+
 struct MixedState {
     int S, stages, kind, sms;
     size_t smem_max;               // dynamic shared memory the GEMM kernels may use
@@ -483,13 +516,13 @@ int mixed_init(lc3d_ctx* c, int slices, int tf32) {
         LC3D_CUDA_TRY(cudaDeviceGetAttribute(&ms->sms, cudaDevAttrMultiProcessorCount, dev));
         LC3D_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         cudaFuncAttributes fa16{}, fa32{};
-        LC3D_CUDA_TRY(cudaFuncGetAttributes(&fa16, oz_gemm_kernel<KIND_BF16>));
-        LC3D_CUDA_TRY(cudaFuncGetAttributes(&fa32, oz_gemm_kernel<KIND_TF32>));
+        LC3D_CUDA_TRY(cudaFuncGetAttributes(&fa16, oz_kernel(KIND_BF16, slices)));
+        LC3D_CUDA_TRY(cudaFuncGetAttributes(&fa32, oz_kernel(KIND_TF32, slices)));
         ms->smem_max = (size_t)optin - std::max(fa16.sharedSizeBytes, fa32.sharedSizeBytes);
     }
     // pipeline stages in what the epilogue buffers, barriers and alignment leave
     ms->stages = (int)((ms->smem_max - EPI_BYTES - 1024 - 256) / ((size_t)slices * (TILE_A_BYTES + TILE_B_BYTES)));
-    if (ms->stages > 4) ms->stages = 4;
+    if (ms->stages > LC3D_OZ_MAX_STAGES) ms->stages = LC3D_OZ_MAX_STAGES;
     if (ms->stages < 2) return LC3D_ERR_PARAM;
     // fixed transform matrices, sliced on the host
     const long long L = N - 1;
@@ -533,9 +566,7 @@ int mixed_init(lc3d_ctx* c, int slices, int tf32) {
     }
     // per-kernel limit: the opt-in maximum, which every slice count's
     // pipeline fits, so contexts with different slice counts can coexist
-    LC3D_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<KIND_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)ms->smem_max));
-    LC3D_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<KIND_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    LC3D_CUDA_TRY(cudaFuncSetAttribute(oz_kernel(ms->kind, slices), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)ms->smem_max));
     return LC3D_OK;
 }
@@ -630,10 +661,7 @@ int mixed_stage(lc3d_ctx* c, const MixedStageDesc* d, int count, cudaStream_t s)
         (size_t)ms->stages * ms->S * (TILE_A_BYTES + TILE_B_BYTES) + EPI_BYTES + 1024 + 256;
     const int grid = std::min(tiles, std::max(ms->sms, 1));   // persistent: one CTA per SM
     ProfScope ps(c, LC3D_STAGE_TRANSFORM, s);
-    if (ms->kind == KIND_TF32)
-        oz_gemm_kernel<KIND_TF32><<<grid, GEMM_THREADS, smem, s>>>(b);
-    else
-        oz_gemm_kernel<KIND_BF16><<<grid, GEMM_THREADS, smem, s>>>(b);
+    oz_kernel(ms->kind, ms->S)<<<grid, GEMM_THREADS, smem, s>>>(b);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
