@@ -66,6 +66,12 @@ constexpr int TILE_A_BYTES = TM * 64;                            // 8 KiB: 128 r
 constexpr int TILE_B_BYTES = TN * 64;                            // 4 KiB
 constexpr int BOX_ROWS = 64;                                     // TMA box height (an A tile is two boxes)
 constexpr int KIND_BF16 = 0, KIND_TF32 = 1;
+#ifndef LC3D_OZ_CLOCKS
+#define LC3D_OZ_CLOCKS 0   // instrumented builds: per-CTA wait / work cycles of the MMA thread and epilogue
+#endif
+#if LC3D_OZ_CLOCKS
+__device__ long long g_oz_clocks[1024][8];
+#endif
 #ifndef LC3D_OZ_MAX_STAGES
 #define LC3D_OZ_MAX_STAGES 4                                     // pipeline stages at most
 #endif
@@ -213,12 +219,20 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
         if (lane == 0) {   // ---- MMA issuer ----
             // products of digit level s + u go to accumulator min(s + u, 3)
             int it = 0, j = 0;
+#if LC3D_OZ_CLOCKS
+            long long c_tempty = 0, c_full = 0, c_issue = 0, c_t = clock64();
+#define OZ_T(var) do { const long long n_ = clock64(); var += n_ - c_t; c_t = n_; } while (0)
+#else
+#define OZ_T(var) do { } while (0)
+#endif
             for (int t = blockIdx.x; t < total && !s_fail; t += gridDim.x, ++j) {
                 const int buf = j & 1;
+                OZ_T(c_issue);
                 if (j >= 2 && !mbar_wait(&tempty[buf], ((j >> 1) - 1) & 1, b.wait_limit)) {
                     s_fail = 1;
                     break;
                 }
+                OZ_T(c_tempty);
                 fence_after();
                 int m0, n0;
                 const OzProb& P = oz_tile(b, t, m0, n0);
@@ -227,10 +241,12 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
                 bool ok = true;
                 for (int kb = 0; kb < nkb; ++kb, ++it) {
                     const int st = it % NS;
+                    OZ_T(c_issue);
                     if (!mbar_wait(&full[st], (it / NS) & 1, b.wait_limit)) {
                         ok = false;
                         break;
                     }
+                    OZ_T(c_full);
                     fence_after();
                     const uint32_t a_base = smem_u32(sPipe + (size_t)st * STAGE_BYTES);
                     // descriptors of the stage's first A and B tiles; the
@@ -269,20 +285,38 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
                 }
                 umma_commit(&tfull[buf]);      // this tile's accumulators complete
             }
+#if LC3D_OZ_CLOCKS
+            OZ_T(c_issue);
+            if (blockIdx.x < 1024) {
+                g_oz_clocks[blockIdx.x][0] = c_tempty;
+                g_oz_clocks[blockIdx.x][1] = c_full;
+                g_oz_clocks[blockIdx.x][2] = c_issue;
+                g_oz_clocks[blockIdx.x][3] = j;
+            }
+#endif
         }
     } else {   // ---- epilogue: warps 2..5 cover TMEM lanes 32 (warp % 4) .. +31 ----
         const int quarter = warp & 3;
         const int row = quarter * 32 + lane;
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         double* stg = sEpi + (warp - 2) * 32 * 33;
-        const int nacc = min(S, NACC);
+        constexpr int NA = S < NACC ? S : NACC;   // level accumulators in use
         int j = 0;
+#if LC3D_OZ_CLOCKS
+        long long e_wait = 0, e_work = 0, e_t = clock64();
+#endif
         for (int t = blockIdx.x; t < total && !s_fail; t += gridDim.x, ++j) {
             const int buf = j & 1;
+#if LC3D_OZ_CLOCKS
+            { const long long n_ = clock64(); e_work += n_ - e_t; e_t = n_; }
+#endif
             if (!mbar_wait(&tfull[buf], (j >> 1) & 1, b.wait_limit)) {
                 s_fail = 1;
                 break;
             }
+#if LC3D_OZ_CLOCKS
+            { const long long n_ = clock64(); e_wait += n_ - e_t; e_t = n_; }
+#endif
             fence_after();
             int m0, n0;
             const OzProb& P = oz_tile(b, t, m0, n0);
@@ -292,24 +326,35 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
                 double v[32];
 #pragma unroll
                 for (int jj = 0; jj < 32; ++jj) v[jj] = 0.0;
-                for (int d = 0; d < nacc; ++d) {   // exact f32 level sums, added in float64
-                    uint32_t r[32];
-                    tmem_ld32(tmem + lane_base + (uint32_t)(buf * ACC_COLS + d * TN + c0), r);
+                // exact f32 level sums, added in float64 in level order; the
+                // levels' TMEM loads two at a time, one wait per pair
+#pragma unroll
+                for (int d = 0; d < NA; d += 2) {
+                    uint32_t r0[32], r1[32];
+                    tmem_ld32(tmem + lane_base + (uint32_t)(buf * ACC_COLS + d * TN + c0), r0);
+                    if (d + 1 < NA) tmem_ld32(tmem + lane_base + (uint32_t)(buf * ACC_COLS + (d + 1) * TN + c0), r1);
                     tmem_wait_ld();
 #pragma unroll
-                    for (int jj = 0; jj < 32; ++jj) v[jj] += (double)__uint_as_float(r[jj]);
+                    for (int jj = 0; jj < 32; ++jj) v[jj] += (double)__uint_as_float(r0[jj]);
+                    if (d + 1 < NA) {
+#pragma unroll
+                        for (int jj = 0; jj < 32; ++jj) v[jj] += (double)__uint_as_float(r1[jj]);
+                    }
                 }
+                // lane l holds the scale of column n0 + c0 + l; rows' scales
+                // are the lanes' own (sa), handed round by shuffles
+                const int nl = n0 + c0 + lane;
+                const double sbl = (nl < P.N) ? pow2(__ldg(P.eb + nl)) : 0.0;
                 if (P.transposed) {
                     // out[n][m]: the lanes hold consecutive m, stores coalesce
-                    if (m < P.M) {
 #pragma unroll
-                        for (int jj = 0; jj < 32; ++jj) {
-                            const int n = n0 + c0 + jj;
-                            if (n >= P.N) continue;
-                            double x = v[jj] * (sa * pow2(__ldg(P.eb + n)));
-                            if (P.lam) x *= P.lam[(size_t)m * P.ldl + n];
-                            P.out[(size_t)n * P.ldo + m] = x;
-                        }
+                    for (int jj = 0; jj < 32; ++jj) {
+                        const int n = n0 + c0 + jj;
+                        const double sb = __shfl_sync(0xffffffffu, sbl, jj);
+                        if (n >= P.N || m >= P.M) continue;
+                        double x = v[jj] * (sa * sb);
+                        if (P.lam) x *= P.lam[(size_t)m * P.ldl + n];
+                        P.out[(size_t)n * P.ldo + m] = x;
                     }
                 } else {
                     // out[m][n]: transpose the warp's 32 x 32 block through
@@ -317,14 +362,14 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
 #pragma unroll
                     for (int jj = 0; jj < 32; ++jj) stg[lane * 33 + jj] = v[jj];
                     __syncwarp();
-                    const int n = n0 + c0 + lane;
-                    const double sb = (n < P.N) ? pow2(__ldg(P.eb + n)) : 0.0;
+#pragma unroll 4
                     for (int r = 0; r < 32; ++r) {
                         const int mr = m0 + quarter * 32 + r;
-                        if (mr >= P.M || n >= P.N) continue;
-                        double x = stg[r * 33 + lane] * (pow2(__ldg(P.ea + mr)) * sb);
-                        if (P.lam) x *= P.lam[(size_t)mr * P.ldl + n];
-                        P.out[(size_t)mr * P.ldo + n] = x;
+                        const double sar = __shfl_sync(0xffffffffu, sa, r);
+                        if (mr >= P.M || nl >= P.N) continue;
+                        double x = stg[r * 33 + lane] * (sar * sbl);
+                        if (P.lam) x *= P.lam[(size_t)mr * P.ldl + nl];
+                        P.out[(size_t)mr * P.ldo + nl] = x;
                     }
                     __syncwarp();
                 }
@@ -333,6 +378,13 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[buf]);   // this set may take the tile after next
         }
+#if LC3D_OZ_CLOCKS
+        { const long long n_ = clock64(); e_work += n_ - e_t; }
+        if (warp == 2 && lane == 0 && blockIdx.x < 1024) {
+            g_oz_clocks[blockIdx.x][4] = e_wait;
+            g_oz_clocks[blockIdx.x][5] = e_work;
+        }
+#endif
     }
     fence_before();
     __syncthreads();
@@ -665,6 +717,14 @@ int mixed_stage(lc3d_ctx* c, const MixedStageDesc* d, int count, cudaStream_t s)
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
+
+#if LC3D_OZ_CLOCKS
+extern "C" int lc3d_debug_oz_clocks(long long* host) {
+    LC3D_CUDA_TRY(cudaDeviceSynchronize());
+    LC3D_CUDA_TRY(cudaMemcpyFromSymbol(host, g_oz_clocks, sizeof(g_oz_clocks)));
+    return LC3D_OK;
+}
+#endif
 
 PFN_cuTensorMapEncodeTiled_v12000 tc_get_encode() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
