@@ -433,6 +433,13 @@ __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_ker
     const T* lam = static_cast<const T*>(F.lam);
     Tout* out = static_cast<Tout*>(F.out);
     const int total = n * FFT_PER_CTA;
+    // a thread's two rows of out[k] in one 16-byte store where they are
+    // aligned (the padded float64 intermediates: an even pitch, rows from an
+    // even row on): 0.317 -> 0.313 ms of transforms per step; the float32
+    // intermediates are not padded and keep scalar stores
+    using Tout2 = typename CxOf<Tout>::type;
+    const bool vec_out = sizeof(Tout) == 8 && F.ld_out % 2 == 0 &&
+                         (reinterpret_cast<uintptr_t>(F.out) % sizeof(Tout2)) == 0;
     double psum = 0.0;
     constexpr int SU = sizeof(T) == 8 ? 8 : LC3D_FFT32_SU;   // readout entries in flight per thread
     for (int t0 = 0; t0 < total; t0 += SU * FFT_THREADS) {
@@ -470,11 +477,20 @@ __global__ void __launch_bounds__(FFT_THREADS, fft_min_blocks<T>()) fft_rows_ker
                     x1 *= la[u][1];
                 }
                 const Tout y0 = (Tout)x0, y1 = (Tout)x1;
-                o[0] = y0;
                 psum += (double)y0;
                 if (row + 1 < F.rows) {
-                    o[1] = y1;
                     psum += (double)y1;
+                    if (sizeof(Tout) == 8 && vec_out) {
+                        Tout2 y;
+                        y.x = y0;
+                        y.y = y1;
+                        *reinterpret_cast<Tout2*>(o) = y;
+                    } else {
+                        o[0] = y0;
+                        o[1] = y1;
+                    }
+                } else {
+                    o[0] = y0;
                 }
             }
         }
