@@ -397,7 +397,10 @@ def run_ours(args, rank, world, dist):
                 'bound': 'hbm',
                 'achieved': ach, 'peak': hbm, 'unit': 'GB/s', 'frac': ach / hbm,
                 'peak_source': hbm_src, 'algorithmic_per_launch': by, 'avg_launch_ms': avg_ms,
-                'traffic': None}
+                'traffic': None,
+                'note': ('the rows stay in L2 (ncu: L2 throughput ~0.14 of peak); while active the pass is '
+                         'bound by the L1/shared-memory pipe (~0.72 of peak) and by its barrier-separated radix '
+                         'passes: profiles/fft_rows_kernel_641.md')}
     elif dom == 'transform' and stage[dom]['timed']:
         avg_ms = stage[dom]['ms'] / stage[dom]['timed']
         fl = transform_flops_per_launch(N)
