@@ -68,7 +68,11 @@ constexpr int CONV_STAGES = 4;
 constexpr int TILE_PIX = 128;                      // M
 constexpr int KB = 32;                             // channels per K block (64 bytes of bf16)
 constexpr int A_TILE_BYTES = TILE_PIX * KB * 2;     // 8 KiB
-constexpr int B_TILE_MAX = 128 * KB * 2;            // Cout <= 128
+
+// Bytes of a pipeline stage's weight tile: Cout rows of 64 bytes, at least
+// 1 KiB (the 64-byte swizzle's alignment); smaller layers take less shared
+// memory, so more CTAs are resident.
+__host__ __device__ constexpr int conv_b_stride(int cout) { return cout * KB * 2 < 1024 ? 1024 : cout * KB * 2; }
 
 struct ConvArgs {
     CUtensorMap tin;               // [H Wp][Cin] bf16, box (32, 128)
@@ -87,7 +91,8 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) conv3x3_tc_kernel(const __gri
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;
     uint8_t* sB = smem + CONV_STAGES * A_TILE_BYTES;
-    uint64_t* full = reinterpret_cast<uint64_t*>(sB + CONV_STAGES * B_TILE_MAX);
+    const int b_stride = conv_b_stride(a.Cout);   // bytes of a stage's weight tile
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + CONV_STAGES * b_stride);
     uint64_t* empty = full + CONV_STAGES;
     uint64_t* done = empty + CONV_STAGES;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
@@ -126,7 +131,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) conv3x3_tc_kernel(const __gri
                 const int off = (tap / 3 - 1) * a.Wp + (tap % 3 - 1);
                 mbar_expect_tx(&full[st], A_TILE_BYTES + b_bytes);
                 tma_load_2d(sA + st * A_TILE_BYTES, &a.tin, &full[st], cb * KB, p0 + off);
-                tma_load_2d(sB + st * B_TILE_MAX, &a.twt, &full[st], cb * KB, tap * a.Cout);
+                tma_load_2d(sB + st * b_stride, &a.twt, &full[st], cb * KB, tap * a.Cout);
             }
         }
     } else if (warp == 1) {
@@ -139,7 +144,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) conv3x3_tc_kernel(const __gri
                 }
                 fence_after();
                 const uint32_t a_base = smem_u32(sA + st * A_TILE_BYTES);
-                const uint32_t b_base = smem_u32(sB + st * B_TILE_MAX);
+                const uint32_t b_base = smem_u32(sB + st * b_stride);
 #pragma unroll
                 for (int kk = 0; kk < KB / 16; ++kk)
                     umma_bf16(tmem, umma_desc_sw64(a_base + kk * 32), umma_desc_sw64(b_base + kk * 32), a.idesc,
@@ -206,8 +211,8 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) conv3x3_tc_kernel(const __gri
     }
 }
 
-constexpr size_t conv_smem_bytes() {
-    return 1024 + CONV_STAGES * (A_TILE_BYTES + B_TILE_MAX) + (2 * CONV_STAGES + 1) * 8 + 16;
+constexpr size_t conv_smem_bytes(int cout = 128) {
+    return 1024 + CONV_STAGES * (A_TILE_BYTES + conv_b_stride(cout)) + (2 * CONV_STAGES + 1) * 8 + 16;
 }
 
 // ---------------------------------------------------------------------------
@@ -818,7 +823,7 @@ int setup_conv(lc3d_predictor* P, int l, const __nv_bfloat16* in, void* out) {
 
 int run_conv(lc3d_predictor* P, int l, cudaStream_t s) {
     const ConvArgs& a = P->conv[l];
-    conv3x3_tc_kernel<<<blocks_for(a.NP, TILE_PIX), CONV_THREADS, conv_smem_bytes(), s>>>(a);
+    conv3x3_tc_kernel<<<blocks_for(a.NP, TILE_PIX), CONV_THREADS, conv_smem_bytes(a.Cout), s>>>(a);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
@@ -895,7 +900,7 @@ int bwd_data_tc(lc3d_predictor* P, int l, const __nv_bfloat16* mask, float* dx, 
     ConvArgs a = P->bconv[l];
     a.out = dx;
     a.mask = mask;
-    conv3x3_tc_kernel<<<blocks_for(a.NP, TILE_PIX), CONV_THREADS, conv_smem_bytes(), s>>>(a);
+    conv3x3_tc_kernel<<<blocks_for(a.NP, TILE_PIX), CONV_THREADS, conv_smem_bytes(a.Cout), s>>>(a);
     LC3D_CUDA_TRY(cudaGetLastError());
     return LC3D_OK;
 }
