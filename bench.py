@@ -636,7 +636,7 @@ def run_scan(args, rank, world, dist):
         'data': 'synthetic (seeded scan draws, generated plasma and beams)',
         'config': {'workload': f'{len(specs)} independent simulations, grids {counts}, window +-8, dxi 0.01',
                    'seed': args.seed, 'l2': 'no flush (each batch step touches several GB, far more than L2)',
-                   'deposition': ('one launch over all simulations per deposition point (8-row tiles)' if multi
+                   'deposition': ('one launch over all simulations per deposition point (4-row tiles)' if multi
                                   else 'per simulation, on its graph branch (autotuned tile rows)')},
         'autotune': {'choice': {str(k): v for k, v in choice.items()},
                      'ms_per_step': {str(k): v for k, v in timings.items()}},

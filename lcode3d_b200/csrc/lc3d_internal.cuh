@@ -116,10 +116,17 @@ int launch_move_estimate(const EstimateArgs& a, cudaStream_t s);
 int launch_move_smart(const MoveArgs& a, cudaStream_t s);
 int launch_deposit_main(const DepositArgs& a, cudaStream_t s);
 int deposit_fine_offset(int fineness);
+// Default fine rows per deposition CTA (4, 8 or 16; 4 measured fastest at
+// 641^2).
+#ifndef LC3D_DEP2_ROWS
+#define LC3D_DEP2_ROWS 4
+#endif
 // Depositions of several simulations in one launch (batches): tiles of
 // DEP_MULTI_ROWS fine rows, CTA b of the launch takes tile b - cta_start[s]
-// of simulation s.
-constexpr int DEP_MULTI_ROWS = 8;
+// of simulation s. The same height as the default: the window's float64 sums
+// follow the tile, so only the same tiles give results bit-identical to each
+// simulation run alone.
+constexpr int DEP_MULTI_ROWS = LC3D_DEP2_ROWS;
 int deposit_multi_tiles(const DepositArgs& a);
 int launch_deposit_multi(const DepositArgs* args_dev, const int* cta_start_dev, int n, int ctas, cudaStream_t s);
 int launch_deposit_finalize(const DepositFinalizeArgs& f, cudaStream_t s);

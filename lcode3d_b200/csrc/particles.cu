@@ -328,9 +328,6 @@ __device__ __forceinline__ void fx_add(unsigned long long* hi_plane, unsigned lo
 #ifndef LC3D_DEP2_CLOCKS
 #define LC3D_DEP2_CLOCKS 0
 #endif
-#ifndef LC3D_DEP2_ROWS
-#define LC3D_DEP2_ROWS 4                    // default fine rows per CTA (4, 8 or 16; 4 measured fastest at 641^2)
-#endif
 constexpr int DEP2_CMAX = 16;               // coarse columns one row table holds
 constexpr int DEP2_WC = 32;                 // window columns (cells); rows: 2 per fine row of the tile
 
