@@ -17,7 +17,7 @@ from oracle import lcode_oracle as O  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-FIELD_TOL = {2: 1e-2, 3: 1e-4, 4: 3e-6, 5: 1e-7, 6: 1e-8}
+FIELD_TOL = {1: 0.25, 2: 1e-2, 3: 1e-4, 4: 3e-6, 5: 1e-7, 6: 1e-8}
 
 
 def rel(a, b):
@@ -42,8 +42,7 @@ def solve_all(L, cfg, ins):
     return (*F, Ez, Bz)
 
 
-@pytest.mark.parametrize('S', [2, 3, 4, 5])
-@pytest.mark.parametrize('N', [41, 161, 641])
+@pytest.mark.parametrize('S,N', [(S, N) for S in (2, 3, 4, 5) for N in (41, 161, 641)] + [(1, 161), (6, 161), (6, 641)])
 def test_mixed_solvers_vs_fp64(L, N, S):
     rng = np.random.default_rng(100 * N + S)
     h = 16 / (N - 1)
