@@ -25,6 +25,10 @@
 
 #include "lc3d_internal.cuh"
 
+#ifndef LC3D_FFT_STREAMS
+#define LC3D_FFT_STREAMS 2   // FFT passes of a solve on one stream or split over two
+#endif
+
 namespace {
 
 // ---------------------------------------------------------------------------
@@ -586,6 +590,16 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
         const bool f32 = c->p.precision == LC3D_PREC_FFT32;
         const int types[4] = {f32 ? FFT_F64_F32 : FFT_F64, f32 ? FFT_F32 : FFT_F64, f32 ? FFT_F32 : FFT_F64,
                               f32 ? FFT_F32_F64 : FFT_F64};
+        // The E fields and the B fields on two streams (forked after the
+        // right-hand sides, joined before the finalize): the passes of the
+        // two halves are independent, so the tail of one half's pass, when
+        // only part of the SMs still work, is filled by the other half's
+        // row groups. The per-launch timing pass keeps one stream.
+        const bool split = LC3D_FFT_STREAMS == 2 && !c->prof_on && c->fft_stream && on[0] && on[3];
+        if (split) {
+            LC3D_CUDA_TRY(cudaEventRecord(c->ev_fork, s));
+            LC3D_CUDA_TRY(cudaStreamWaitEvent(c->fft_stream, c->ev_fork, 0));
+        }
         for (int stage = 0; stage < 4; ++stage) {
             FftRowsDesc d[6]{};
             int cnt = 0;
@@ -613,7 +627,24 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
                              break;
                 }
             }
-            LC3D_TRY(fft_rows(c, d, cnt, types[stage], s));
+            if (split) {   // Ex Ey Ez on the solve's stream, Bx By Bz on the second
+                FftRowsDesc de[6], db[6];
+                int ne = 0, nb = 0, k = 0;
+                for (int f = 0; f < 6; ++f) {
+                    if (!on[f]) continue;
+                    if (f < 3) de[ne++] = d[k];
+                    else db[nb++] = d[k];
+                    ++k;
+                }
+                LC3D_TRY(fft_rows(c, de, ne, types[stage], s));
+                LC3D_TRY(fft_rows(c, db, nb, types[stage], c->fft_stream));
+            } else {
+                LC3D_TRY(fft_rows(c, d, cnt, types[stage], s));
+            }
+        }
+        if (split) {
+            LC3D_CUDA_TRY(cudaEventRecord(c->ev_join, c->fft_stream));
+            LC3D_CUDA_TRY(cudaStreamWaitEvent(s, c->ev_join, 0));
         }
     } else {
         // the four GEMM stages
