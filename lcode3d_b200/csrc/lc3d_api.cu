@@ -365,8 +365,10 @@ void destroy(lc3d_ctx* c) {
     if (c->ev_copy) cudaEventDestroy(c->ev_copy);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
-    if (c->ev_join) cudaEventDestroy(c->ev_join);
-    if (c->fft_stream) cudaStreamDestroy(c->fft_stream);
+    for (int q = 0; q < 2; ++q) {
+        if (c->ev_join[q]) cudaEventDestroy(c->ev_join[q]);
+        if (c->fft_stream[q]) cudaStreamDestroy(c->fft_stream[q]);
+    }
     diag_free(c);
     if (c->fft_tw) cudaFree(c->fft_tw);
     mixed_free(c);
@@ -593,9 +595,13 @@ int lc3d_create(const lc3d_params* p, int device, lc3d_ctx** out) {
     if (rc == LC3D_OK && cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = LC3D_ERR_CUDA;
     if (rc == LC3D_OK && cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming) != cudaSuccess) rc = LC3D_ERR_CUDA;
     if (rc == LC3D_OK && cudaEventCreateWithFlags(&c->ev_copy, cudaEventDisableTiming) != cudaSuccess) rc = LC3D_ERR_CUDA;
-    if (rc == LC3D_OK && cudaStreamCreateWithFlags(&c->fft_stream, cudaStreamNonBlocking) != cudaSuccess) rc = LC3D_ERR_CUDA;
+    for (int q = 0; q < 2; ++q) {
+        if (rc == LC3D_OK && cudaStreamCreateWithFlags(&c->fft_stream[q], cudaStreamNonBlocking) != cudaSuccess)
+            rc = LC3D_ERR_CUDA;
+        if (rc == LC3D_OK && cudaEventCreateWithFlags(&c->ev_join[q], cudaEventDisableTiming) != cudaSuccess)
+            rc = LC3D_ERR_CUDA;
+    }
     if (rc == LC3D_OK && cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess) rc = LC3D_ERR_CUDA;
-    if (rc == LC3D_OK && cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) rc = LC3D_ERR_CUDA;
     LC3D_STEP(particles_prepare());
     LC3D_STEP(fields_init(c));
     LC3D_STEP(fft_init(c));

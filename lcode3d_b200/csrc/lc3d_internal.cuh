@@ -266,8 +266,8 @@ struct lc3d_ctx {
     double* packed;                       // coarse particles of the last move, [Nc*Nc][8] (x y m q px py pz -)
     cudaStream_t copy_stream;             // its host-to-device copies
     cudaEvent_t ev_main, ev_copy;         // ordering of those copies with the step's stream
-    cudaStream_t fft_stream;              // second stream of the FFT passes (half the fields)
-    cudaEvent_t ev_fork, ev_join;         // its fork from and join to the solve's stream
+    cudaStream_t fft_stream[2];           // further streams of the FFT passes (groups of fields)
+    cudaEvent_t ev_fork, ev_join[2];      // their fork from and joins to the solve's stream
     // field-solver workspaces (fields.cu)
     double *S2, *C, *CT;                  // 2*DST-I (M x M), DCT-I (N x N), its transpose
     double *lam_dir, *lam_mix, *lam_mixT, *lam_neu;
