@@ -31,6 +31,9 @@
 #ifndef LC3D_FFT32_STREAMS
 #define LC3D_FFT32_STREAMS 3   // ... float32 FFT passes
 #endif
+#ifndef LC3D_FIN_PER_GROUP
+#define LC3D_FIN_PER_GROUP 1
+#endif
 
 namespace {
 
@@ -548,6 +551,11 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
         }
     }
     int bz_partials = 0;   // > 0: the FFT pass left this many Bz partial sums in c->red
+    // FFT passes on several streams whose join waits until each group's
+    // finalize has run on its own stream (step finalisation only)
+    int fin_groups = 0;
+    int fin_group_of[6] = {0, 0, 0, 0, 0, 0};
+    cudaStream_t fin_stream[3] = {s, s, s};
     if (c->p.precision == LC3D_PREC_MIXED || c->p.precision == LC3D_PREC_TF32) {
         // four split-BF16 tensor-core GEMM stages (fields_mixed.cu)
         for (int stage = 0; stage < 4; ++stage) {
@@ -659,10 +667,16 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
                 LC3D_TRY(fft_rows(c, d, cnt, types[stage], s));
             }
         }
-        for (int q = 1; q < nstreams; ++q) {
-            if (!used[q]) continue;
-            LC3D_CUDA_TRY(cudaEventRecord(c->ev_join[q - 1], c->fft_stream[q - 1]));
-            LC3D_CUDA_TRY(cudaStreamWaitEvent(s, c->ev_join[q - 1], 0));
+        if (LC3D_FIN_PER_GROUP && o.mode == 1 && nstreams > 1) {   // each group finalised on its own stream, then joined
+            fin_groups = nstreams;
+            for (int f = 0; f < 6; ++f) fin_group_of[f] = group_of(f);
+            for (int q = 1; q < nstreams; ++q) fin_stream[q] = used[q] ? c->fft_stream[q - 1] : s;
+        } else {
+            for (int q = 1; q < nstreams; ++q) {
+                if (!used[q]) continue;
+                LC3D_CUDA_TRY(cudaEventRecord(c->ev_join[q - 1], c->fft_stream[q - 1]));
+                LC3D_CUDA_TRY(cudaStreamWaitEvent(s, c->ev_join[q - 1], 0));
+            }
         }
     } else {
         // the four GEMM stages
@@ -722,30 +736,43 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
         }
         return LC3D_OK;
     }
-    FinalizeArgs fa{};
-    memset(&fa, 0, sizeof(fa));
-    for (int f = 0; f < 6; ++f) {
-        if (!on[f]) continue;
-        fa.raw[f] = c->raw[f];
-        fa.prev[f] = o.prev[f];
-        fa.out[f] = o.out[f];
-        fa.avg[f] = o.avg[f];
+    // one finalize over all fields, or one per group of fields on that
+    // group's stream (the groups' FFT passes ran on several streams)
+    for (int q = 0; q < (fin_groups ? fin_groups : 1); ++q) {
+        FinalizeArgs fa{};
+        memset(&fa, 0, sizeof(fa));
+        for (int f = 0; f < 6; ++f) {
+            if (!on[f] || (fin_groups && fin_group_of[f] != q)) continue;
+            fa.raw[f] = c->raw[f];
+            fa.prev[f] = o.prev[f];
+            fa.out[f] = o.out[f];
+            fa.avg[f] = o.avg[f];
+        }
+        bool any = false;
+        for (int f = 0; f < 6; ++f) any = any || fa.raw[f];
+        if (!any) continue;
+        fa.partial = c->red;
+        fa.nblocks = nred;
+        fa.n = n;
+        fa.variant_A = c->p.field_solver_variant_A;
+        fa.has_bz = fa.raw[5] != nullptr;
+        fa.inv_n = inv_n;
+        uintptr_t al = 0;
+        for (int f = 0; f < 6; ++f)
+            al |= reinterpret_cast<uintptr_t>(fa.raw[f]) | reinterpret_cast<uintptr_t>(fa.prev[f]) |
+                  reinterpret_cast<uintptr_t>(fa.out[f]) | reinterpret_cast<uintptr_t>(fa.avg[f]);
+        fa.vec = (al & 15) == 0;
+        const int threads = fa.vec ? (n + 1) / 2 : n;
+        cudaStream_t sq = fin_groups ? fin_stream[q] : s;
+        ProfScope ps(c, LC3D_STAGE_FIELD_FIN, sq);
+        LC3D_CUDA_TRY(launch_pdl(finalize_step_kernel, dim3((threads + RED_THREADS - 1) / RED_THREADS),
+                                 dim3(RED_THREADS), 0, sq, fa));
+        LC3D_CUDA_TRY(cudaGetLastError());
     }
-    fa.partial = c->red;
-    fa.nblocks = nred;
-    fa.n = n;
-    fa.variant_A = c->p.field_solver_variant_A;
-    fa.has_bz = on[5];
-    fa.inv_n = inv_n;
-    uintptr_t al = 0;
-    for (int f = 0; f < 6; ++f)
-        al |= reinterpret_cast<uintptr_t>(fa.raw[f]) | reinterpret_cast<uintptr_t>(fa.prev[f]) |
-              reinterpret_cast<uintptr_t>(fa.out[f]) | reinterpret_cast<uintptr_t>(fa.avg[f]);
-    fa.vec = (al & 15) == 0;
-    const int threads = fa.vec ? (n + 1) / 2 : n;
-    ProfScope ps(c, LC3D_STAGE_FIELD_FIN, s);
-    LC3D_CUDA_TRY(launch_pdl(finalize_step_kernel, dim3((threads + RED_THREADS - 1) / RED_THREADS),
-                             dim3(RED_THREADS), 0, s, fa));
-    LC3D_CUDA_TRY(cudaGetLastError());
+    for (int q = 1; q < fin_groups; ++q) {
+        if (fin_stream[q] == s) continue;
+        LC3D_CUDA_TRY(cudaEventRecord(c->ev_join[q - 1], fin_stream[q]));
+        LC3D_CUDA_TRY(cudaStreamWaitEvent(s, c->ev_join[q - 1], 0));
+    }
     return LC3D_OK;
 }
