@@ -73,6 +73,9 @@ __global__ void __launch_bounds__(RHS_THREADS) rhs_kernel(const __grid_constant_
     const bool interior = i >= 1 && i <= N - 2 && j >= 1 && j <= N - 2;
     const SolveInputs& in = a.in;
     const double h2 = a.h * 2;
+    // every result first, then the stores: the stores could alias the
+    // inputs for the compiler, so loads after a store would wait for it
+    double o[6] = {};
     if (a.out[0]) {   // the four transverse fields
         double dro_dx = 0, dro_dy = 0, djz_dx = 0, djz_dy = 0;
         if (interior) {
@@ -90,10 +93,10 @@ __global__ void __launch_bounds__(RHS_THREADS) rhs_kernel(const __grid_constant_
         const double djx_dxi = div_by(in.jx_prev[k] - in.jx[k], a.dxi, a.inv_dxi);
         const double djy_dxi = div_by(in.jy_prev[k] - in.jy[k], a.dxi, a.inv_dxi);
         const double st = a.st;
-        a.out[0][k] = -((dro_dx - djx_dxi) - in.Ex_sub[k] * st);
-        a.out[1][k] = -((dro_dy - djy_dxi) - in.Ey_sub[k] * st);
-        a.out[3][k] = +((djz_dy - djy_dxi) + in.Bx_sub[k] * st);
-        a.out[4][k] = -((djz_dx - djx_dxi) - in.By_sub[k] * st);
+        o[0] = -((dro_dx - djx_dxi) - in.Ex_sub[k] * st);
+        o[1] = -((dro_dy - djy_dxi) - in.Ey_sub[k] * st);
+        o[3] = +((djz_dy - djy_dxi) + in.Bx_sub[k] * st);
+        o[4] = -((djz_dx - djx_dxi) - in.By_sub[k] * st);
     }
     if (a.out[2] || a.out[5]) {
         double ez = 0, bz = 0;
@@ -105,9 +108,12 @@ __global__ void __launch_bounds__(RHS_THREADS) rhs_kernel(const __grid_constant_
             ez = -div_by(djx_dx + djy_dy, h2, a.inv_h2);
             bz = -div_by(djx_dy - djy_dx, h2, a.inv_h2);
         }
-        if (a.out[2]) a.out[2][k] = ez;
-        if (a.out[5]) a.out[5][k] = bz;
+        o[2] = ez;
+        o[5] = bz;
     }
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+        if (a.out[f]) a.out[f][k] = o[f];
 }
 
 // ---------------------------------------------------------------------------
