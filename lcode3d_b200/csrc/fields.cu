@@ -314,20 +314,25 @@ __device__ __forceinline__ double2 finalize_value(const FinalizeArgs& a, int f, 
 __global__ void __launch_bounds__(RED_THREADS) finalize_step_kernel(const __grid_constant__ FinalizeArgs a) {
     pdl_wait();
     __shared__ double sh[RED_THREADS];
-    const double mean = a.has_bz ? mean_from_partials(a.partial, a.nblocks, a.inv_n, sh) : 0.0;
     int k = blockIdx.x * RED_THREADS + threadIdx.x;
     if (a.vec) {
-        // two cells per thread: all twelve 16-byte loads issued before the stores
+        // two cells per thread: all twelve 16-byte loads issued before the
+        // stores, and before the Bz mean's reduction (which they overlap)
         k *= 2;
-        if (k >= a.n) return;
-        if (k + 1 < a.n) {
-            double2 r[6], p[6];
+        const bool pair = k + 1 < a.n;
+        double2 r[6], p[6];
+        if (pair) {
 #pragma unroll
             for (int f = 0; f < 6; ++f)
                 if (a.raw[f]) {
                     r[f] = __ldcg(reinterpret_cast<const double2*>(a.raw[f] + k));
                     p[f] = __ldcg(reinterpret_cast<const double2*>(a.prev[f] + k));
                 }
+        }
+        // every thread of the CTA takes part in the reduction's barriers
+        const double mean = a.has_bz ? mean_from_partials(a.partial, a.nblocks, a.inv_n, sh) : 0.0;
+        if (k >= a.n) return;
+        if (pair) {
 #pragma unroll
             for (int f = 0; f < 6; ++f) {
                 if (!a.raw[f]) continue;
@@ -338,8 +343,17 @@ __global__ void __launch_bounds__(RED_THREADS) finalize_step_kernel(const __grid
             }
             return;
         }
-        // an odd cell count leaves the last cell to one thread, below
+        // an odd cell count leaves the last cell to one thread
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            if (!a.raw[f]) continue;
+            const double2 v = finalize_value(a, f, a.raw[f][k], a.prev[f][k], mean);
+            if (a.out[f]) a.out[f][k] = v.x;
+            a.avg[f][k] = v.y;
+        }
+        return;
     }
+    const double mean = a.has_bz ? mean_from_partials(a.partial, a.nblocks, a.inv_n, sh) : 0.0;
     if (k >= a.n) return;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
