@@ -629,8 +629,10 @@ int solve_fields(lc3d_ctx* c, int which, const SolveInputs& in, const SolveOutpu
         // by the other groups' row groups. Measured at 641^2: float64 1802 ->
         // 1864 xi-steps/s with two streams (1835 with three); float32
         // transforms 2109 -> 2145 with two, 2176 with three. The per-launch
-        // timing pass keeps one stream.
-        const int nstreams = c->prof_on ? 1 : f32 ? LC3D_FFT32_STREAMS : LC3D_FFT_STREAMS;
+        // timing pass keeps one stream, and so do the steps of a batch graph
+        // (its branches overlap the simulations already: a 32-simulation scan
+        // measured 3772 aggregate xi-steps/s on one stream, 3600 on several).
+        const int nstreams = (c->prof_on || c->one_stream) ? 1 : f32 ? LC3D_FFT32_STREAMS : LC3D_FFT_STREAMS;
         auto group_of = [&](int f) {
             if (nstreams == 3) return f == 2 || f == 5 ? 2 : (f < 2 ? 0 : 1);
             if (nstreams == 2) return f < 3 ? 0 : 1;

@@ -292,6 +292,8 @@ struct lc3d_ctx {
     long long prof_count[LC3D_NSTAGES];
     // device-side beam and graph-replayed runs (run.cu)
     int capturing;                        // a step is being captured into a graph
+    int one_stream;                       // solves on the caller's stream alone: a batch graph's
+                                          // branches already overlap the simulations
     double* beam_buf;                     // N x N beam evaluated on the device
     void* run_ctl;                        // device RunCtl: xi counter, history
     double beam_A, beam_sr, beam_lf;      // amplitude, sigma_r, length factor

@@ -291,8 +291,10 @@ int batch_capture(lc3d_batch* b, int ph) {
         memcpy(saved, c->launches, sizeof(saved));
         memset(c->launches, 0, sizeof(c->launches));
         c->capturing = 1;
+        c->one_stream = 1;
         rc = enqueue_step(c, b->par0[i] ^ ph, b->br[i]);
         c->capturing = 0;
+        c->one_stream = 0;
         for (int q = 0; q < LC3D_NSTAGES; ++q) count += c->launches[q];
         memcpy(c->graph_launches[b->par0[i] ^ ph], c->launches, sizeof(c->launches));
         memcpy(c->launches, saved, sizeof(saved));
@@ -360,9 +362,11 @@ int batch_capture_multi(lc3d_batch* b, int ph) {
             memcpy(saved, c->launches, sizeof(saved));
             memset(c->launches, 0, sizeof(c->launches));
             c->capturing = 1;
+            c->one_stream = 1;
             DepositArgs dummy{};
             rc = enqueue_step_segment(c, par, b->br[i], seg, seg < 3 ? &host[seg * n + i] : &dummy);
             c->capturing = 0;
+            c->one_stream = 0;
             for (int q = 0; q < LC3D_NSTAGES; ++q) {
                 count += c->launches[q];
                 c->graph_launches[par][q] += c->launches[q];
