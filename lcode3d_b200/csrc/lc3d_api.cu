@@ -266,19 +266,21 @@ int run_step(lc3d_ctx* c, const lc3d_state_ptrs& prev, const lc3d_state_ptrs& ou
         mv.est_y = pass ? c->pw[0][1] : nullptr;
         for (int f = 0; f < 6; ++f) mv.F[f] = pass ? c->avg[f] : prevF[f];
         mv.out_x = pw[0]; mv.out_y = pw[1]; mv.out_px = pw[2]; mv.out_py = pw[3]; mv.out_pz = pw[4];
-        {
-            ProfScope ps(c, LC3D_STAGE_MOVE, s);
-            LC3D_TRY(launch_move_smart(mv, s));
-        }
         if (pass == 0 && x && x->beam_host) {
-            // the host beam crosses on the copy stream while the first
-            // deposition runs; the first field solve waits for it
+            // the host beam crosses on the copy stream while the first push
+            // and deposition run (it waits only for the work queued before
+            // this step, the previous step's reads of the buffer); the first
+            // field solve waits for it
             LC3D_CUDA_TRY(cudaEventRecord(c->ev_main, s));
             LC3D_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, c->ev_main, 0));
             LC3D_CUDA_TRY(cudaMemcpyAsync(c->beam_dev, x->beam_host, (size_t)c->N * c->N * sizeof(double),
                                           cudaMemcpyHostToDevice, c->copy_stream));
             LC3D_CUDA_TRY(cudaEventRecord(c->ev_copy, c->copy_stream));
             in.beam = c->beam_dev;
+        }
+        {
+            ProfScope ps(c, LC3D_STAGE_MOVE, s);
+            LC3D_TRY(launch_move_smart(mv, s));
         }
         if (pass == 0 && predicted) {
             // the prediction stands in for the first-pass fields: only the
