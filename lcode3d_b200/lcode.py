@@ -25,6 +25,7 @@ float64);
 (1..6; default 4 for 'mixed', 3 for 'tf32').
 """
 import ctypes
+import operator
 import sys
 
 import numpy as np
@@ -186,16 +187,17 @@ class Solver:
         """The same array objects as last time, none written since (torch
         counts every in-place write of a tensor or of a view of it in
         ``_version``): nothing to copy. The solver holds the arrays, so their
-        storage cannot have been freed and reused meanwhile."""
-        return seen is not None and all(a is b and getattr(a, '_version', None) == v
-                                        for a, (b, v) in zip(arrays, seen))
+        storage cannot have been freed and reused meanwhile. (map / attrgetter
+        keep the per-step check in C: it runs on every step() call.)"""
+        return (seen is not None and all(map(operator.is_, arrays, seen[0]))
+                and list(map(_VERSION, arrays)) == seen[1])
 
     @staticmethod
     def _seen(arrays):
-        return tuple((a, getattr(a, '_version', None)) for a in arrays)
+        return arrays, list(map(_VERSION, arrays))
 
     def set_virt(self, virt):
-        arrays = tuple(getattr(virt, n) for n in _lib.VIRT_NAMES)
+        arrays = _GET_VIRT(virt)
         if self._unchanged(arrays, self._virt_arrays):
             return
         ip = getattr(virt, 'indices_prev').to(torch.int32).contiguous()
@@ -208,7 +210,7 @@ class Solver:
         self._virt_arrays = self._seen(arrays)
 
     def set_const(self, const):
-        arrays = tuple(getattr(const, n) for n in _lib.CONST_NAMES)
+        arrays = _GET_CONST(const)
         if self._unchanged(arrays, self._const_arrays):
             return
         c = _lib.ConstPtrs(*[getattr(const, n).data_ptr() for n in _lib.CONST_NAMES])
@@ -219,6 +221,11 @@ class Solver:
         if check_errors:
             check(lib.lc3d_check_error(self.ctx, _stream()), where)
 
+
+_GET_VIRT = operator.attrgetter(*_lib.VIRT_NAMES)
+_GET_CONST = operator.attrgetter(*_lib.CONST_NAMES)
+_GET_STATE = operator.attrgetter(*_lib.STATE_NAMES)
+_VERSION = operator.attrgetter('_version')   # const / virt_params arrays are torch tensors
 
 _solvers = {}
 _solvers_raw = {}   # (raw config attribute values, device) -> Solver: skips params_of per call
@@ -314,32 +321,23 @@ class _StatePool:
 
     @staticmethod
     def _counts(e):
-        arr = e[1]
-        return [sys.getrefcount(e[0])] + [sys.getrefcount(arr[k]) for k in range(len(arr))] + [_use_count(e[5])]
+        return sys.getrefcount(e[0]), list(map(sys.getrefcount, e[1])), _use_count(e[5])
 
     @staticmethod
     def _free(e):
         """The counts of entry e are back at their baseline e[3], taken the
-        same way as _counts but compared one by one, the object's own count
-        first (an entry in use usually fails there)."""
+        same way as _counts, the object's own count first (an entry in use
+        usually fails there)."""
         base = e[3]
-        if sys.getrefcount(e[0]) != base[0]:
-            return False
-        arr = e[1]
-        for k in range(len(arr)):
-            if sys.getrefcount(arr[k]) != base[1 + k]:
-                return False
-        return _use_count(e[5]) == base[-1]
+        return (sys.getrefcount(e[0]) == base[0] and list(map(sys.getrefcount, e[1])) == base[1]
+                and _use_count(e[5]) == base[2])
 
     def ptrs_of(self, state):
         """The StatePtrs of `state` if it is one of the pool's states with
         all 15 arrays still its own (else None)."""
         for e in self.entries:
             if e[0] is state:
-                for n, t in zip(_lib.STATE_NAMES, e[1]):
-                    if getattr(state, n) is not t:
-                        return None
-                return e[2]
+                return e[2] if all(map(operator.is_, _GET_STATE(state), e[1])) else None
         return None
 
     def take(self, shape_p, g, dev):
